@@ -1,0 +1,247 @@
+"""bksp_b200 -- Python host binding of libbksp.so, the B200 (sm_100a) build
+of the bksp Krylov-solver C API.
+
+The functions below mirror ``bksp.h`` one to one (same names, argument
+order and meaning, same return codes), taking NumPy arrays where the C API
+takes host pointers:
+
+* ``bksp_dcg, dcr, dbicg, dbicgstab, dbicgstabl`` -- single right-hand side;
+  ``x`` is updated in place and the bksp return code is returned;
+* ``dblcg, dblbicgstab, dblbicgstabl`` -- ``B``/``X`` are n-by-s arrays
+  (passed to C column-major, as ``dmat``);
+* ``dshbicg, dshbicgstabl`` -- ``x`` has ``n * (len(sigma) + 1)`` entries,
+  seed first.
+
+There is no CPU fallback: importing this module loads the CUDA library and
+raises if it has not been built (``python -c "import __graft_entry__ as g;
+g.build()"`` or ``make -C bksp_b200/csrc``).
+"""
+import contextlib
+import ctypes as C
+import os
+
+import numpy as np
+
+NOT_CONVERGED = -1
+DIVERGENCE = -2
+INVALID_PARAMETERS = -3
+INVALID_MATRIX_TYPE = -4
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libbksp.so")
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+
+
+class DSpMat(C.Structure):
+    """``dspmat``: 0-based CSR with pointer-to-int size fields."""
+    _fields_ = [("row", _ip), ("col", _ip), ("nnz", _ip),
+                ("row_size", _ip), ("col_size", _ip), ("value", _dp),
+                ("format", C.c_char_p), ("type", C.c_char_p)]
+
+
+class DMat(C.Structure):
+    """``dmat``: column-major dense block."""
+    _fields_ = [("row_size", C.c_int), ("col_size", C.c_int), ("value", _dp)]
+
+
+class Stats(C.Structure):
+    """``bksp_gpu_stats`` (bksp_gpu.h)."""
+    _fields_ = [("hist", _dp), ("hist_cap", C.c_int), ("hist_len", C.c_int),
+                ("ret", C.c_int), ("solve_ms", C.c_double),
+                ("total_ms", C.c_double), ("true_res", C.c_double)]
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(
+            f"bksp_b200: CUDA library {LIB_PATH} is not built; run "
+            "`make -C bksp_b200/csrc` (there is no CPU fallback)")
+    L = C.CDLL(LIB_PATH)
+    sp, mp = C.POINTER(DSpMat), C.POINTER(DMat)
+    d, i = C.c_double, C.c_int
+    sig = {
+        "bksp_dcg": [sp, _dp, d, i, _dp],
+        "dcr": [sp, _dp, d, i, _dp],
+        "dbicg": [sp, _dp, d, i, _dp],
+        "dbicgstab": [sp, _dp, d, i, _dp],
+        "dbicgstabl": [sp, _dp, i, d, i, _dp],
+        "dblcg": [sp, mp, d, i, mp],
+        "dblbicgstab": [sp, mp, d, i, mp],
+        "dblbicgstabl": [sp, mp, i, d, i, mp],
+        "dshbicg": [sp, _dp, _dp, i, d, i, _dp],
+        "dshbicgstabl": [sp, _dp, i, _dp, i, d, i, _dp],
+        "myqr": [i, i, _dp, _dp],
+    }
+    for name, argt in sig.items():
+        f = getattr(L, name)
+        f.argtypes = argt
+        f.restype = C.c_int
+    L.read_matrix_market.argtypes = [C.c_char_p]
+    L.read_matrix_market.restype = sp
+    L.bksp_gpu_record.argtypes = [C.POINTER(Stats)]
+    L.bksp_gpu_record.restype = None
+    L.bksp_gpu_version.restype = C.c_char_p
+    return L
+
+
+lib = _load()
+
+
+class CsrMatrix:
+    """A ``dspmat`` over NumPy buffers (kept alive by this object).
+
+    ``symmetric=True`` sets type "symmetric": the arrays then hold one
+    triangle and the operator mirrors the off-diagonal entries.
+    """
+
+    def __init__(self, rowptr, col, val, n=None, symmetric=False):
+        self.rowptr = np.ascontiguousarray(rowptr, dtype=np.int32)
+        self.col = np.ascontiguousarray(col, dtype=np.int32)
+        self.val = np.ascontiguousarray(val, dtype=np.float64)
+        n = self.rowptr.size - 1 if n is None else int(n)
+        self.n = n
+        self.symmetric = bool(symmetric)
+        self._nnz = C.c_int(int(self.col.size))
+        self._n = C.c_int(n)
+        self._m = C.c_int(n)
+        self.s = DSpMat(self.rowptr.ctypes.data_as(_ip),
+                        self.col.ctypes.data_as(_ip), C.pointer(self._nnz),
+                        C.pointer(self._n), C.pointer(self._m),
+                        self.val.ctypes.data_as(_dp), b"csr",
+                        b"symmetric" if symmetric else b"unsymmetric")
+
+    @property
+    def ptr(self):
+        return C.byref(self.s)
+
+
+def _vec(a):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    return a
+
+
+def _dmat(a):
+    buf = np.asfortranarray(a, dtype=np.float64)
+    return buf, DMat(buf.shape[0], buf.shape[1], buf.ctypes.data_as(_dp))
+
+
+def _inplace(x):
+    if not (isinstance(x, np.ndarray) and x.dtype == np.float64
+            and x.flags.c_contiguous):
+        raise TypeError("x must be a C-contiguous float64 array (updated in place)")
+    return x.ctypes.data_as(_dp)
+
+
+def bksp_dcg(A, b, tol, max_iter, x):
+    b = _vec(b)
+    return lib.bksp_dcg(A.ptr, b.ctypes.data_as(_dp), tol, max_iter, _inplace(x))
+
+
+def dcr(A, b, tol, max_iter, x):
+    b = _vec(b)
+    return lib.dcr(A.ptr, b.ctypes.data_as(_dp), tol, max_iter, _inplace(x))
+
+
+def dbicg(A, b, tol, max_iter, x):
+    b = _vec(b)
+    return lib.dbicg(A.ptr, b.ctypes.data_as(_dp), tol, max_iter, _inplace(x))
+
+
+def dbicgstab(A, b, tol, max_iter, x):
+    b = _vec(b)
+    return lib.dbicgstab(A.ptr, b.ctypes.data_as(_dp), tol, max_iter,
+                         _inplace(x))
+
+
+def dbicgstabl(A, b, l, tol, max_iter, x):
+    b = _vec(b)
+    return lib.dbicgstabl(A.ptr, b.ctypes.data_as(_dp), l, tol, max_iter,
+                          _inplace(x))
+
+
+def _block(fn, A, B, args, X):
+    Bf, Bm = _dmat(B)
+    Xf, Xm = _dmat(X)
+    ret = fn(A.ptr, C.byref(Bm), *args, C.byref(Xm))
+    X[...] = Xf
+    return ret
+
+
+def dblcg(A, B, tol, max_iter, X):
+    """X (n-by-s NumPy array) is updated in place."""
+    return _block(lib.dblcg, A, B, (tol, max_iter), X)
+
+
+def dblbicgstab(A, B, tol, max_iter, X):
+    return _block(lib.dblbicgstab, A, B, (tol, max_iter), X)
+
+
+def dblbicgstabl(A, B, l, tol, max_iter, X):
+    return _block(lib.dblbicgstabl, A, B, (l, tol, max_iter), X)
+
+
+def dshbicg(A, b, sigma, tol, max_iter, x):
+    b = _vec(b)
+    s = _vec(sigma)
+    return lib.dshbicg(A.ptr, b.ctypes.data_as(_dp), s.ctypes.data_as(_dp),
+                       int(s.size), tol, max_iter, _inplace(x))
+
+
+def dshbicgstabl(A, b, l, sigma, tol, max_iter, x):
+    b = _vec(b)
+    s = _vec(sigma)
+    return lib.dshbicgstabl(A.ptr, b.ctypes.data_as(_dp), l,
+                            s.ctypes.data_as(_dp), int(s.size), tol,
+                            max_iter, _inplace(x))
+
+
+def myqr(V):
+    """Thin QR of an m-by-n array; returns (Q, R, info)."""
+    Vf = np.asfortranarray(V, dtype=np.float64).copy(order="F")
+    m, n = Vf.shape
+    R = np.zeros((n, n), order="F")
+    info = lib.myqr(m, n, Vf.ctypes.data_as(_dp), R.ctypes.data_as(_dp))
+    return Vf, R, info
+
+
+def read_matrix_market(path):
+    """Returns (rowptr, col, val, n, type) from the library's reader."""
+    p = lib.read_matrix_market(os.fsencode(path))
+    if not p:
+        raise OSError(f"cannot read Matrix Market file {path}")
+    m = p.contents
+    n = m.row_size[0]
+    nnz = m.nnz[0]
+    rowptr = np.ctypeslib.as_array(m.row, shape=(n + 1,)).copy()
+    col = np.ctypeslib.as_array(m.col, shape=(nnz,)).copy() if nnz else np.zeros(0, np.int32)
+    val = np.ctypeslib.as_array(m.value, shape=(nnz,)).copy() if nnz else np.zeros(0)
+    return rowptr, col, val, n, m.type.decode()
+
+
+@contextlib.contextmanager
+def record(hist_cap=0):
+    """Collect ``bksp_gpu_stats`` of the bksp calls made inside the block.
+
+    Yields a dict filled on exit: ``ret``, ``hist`` (convergence-test values,
+    one per iteration), ``solve_ms``, ``total_ms``.
+    """
+    buf = np.zeros(max(int(hist_cap), 1))
+    st = Stats(buf.ctypes.data_as(_dp), int(hist_cap), 0, 0, 0.0, 0.0, 0.0)
+    out = {}
+    lib.bksp_gpu_record(C.byref(st))
+    try:
+        yield out
+    finally:
+        lib.bksp_gpu_record(None)
+        out["ret"] = st.ret
+        out["hist_len"] = st.hist_len
+        out["hist"] = buf[:min(st.hist_len, int(hist_cap))].copy()
+        out["solve_ms"] = st.solve_ms
+        out["total_ms"] = st.total_ms
+        out["true_res"] = st.true_res
+
+
+def version():
+    return lib.bksp_gpu_version().decode()

@@ -1,0 +1,119 @@
+// K3: fused level-1 kernels -- one pass computing up to kLcMaxOut linear
+// combinations of up to kLcMaxIn vectors with scalar-slot coefficients, and
+// up to kMaxDots dot products of the results, reduced in FP64 (the
+// reference's cblas_daxpy / dscal / dcopy / ddot / dnrm2 sequences, e.g.
+// src/bicgstabl.c:60-122, fused per recurrence step).
+//
+// Terms are applied in input order: the first present term is a rounded
+// product, every further term a fused multiply-add -- the rounding of a
+// dscal / dcopy followed by FMA-based daxpy calls on the reference's CPU.
+// Inputs stream through one at a time, so register use grows with the
+// number of outputs and dots, not with the number of inputs.
+// Operands are streamed as 16-byte packets (double2 / float4); lengths are
+// padded to a multiple of 64 and padding entries are zero in every vector.
+#pragma once
+#include "dev_common.cuh"
+
+namespace bk {
+
+template <typename T, int MI, int MO, int ND>
+__global__ void __launch_bounds__(kThreads)
+k_lincomb(const LcH<T> d, Red rd) {
+  if (finished(rd.ctl)) return;
+  using PV = typename Pack<T>::V;
+  constexpr int P = Pack<T>::N;
+  __shared__ T cs[MO][MI];
+  __shared__ unsigned pres[MO];
+  if (threadIdx.x < MO) {
+    unsigned m = 0;
+    for (int i = 0; i < MI; ++i)
+      if (threadIdx.x < d.nout && i < d.nin && d.c[threadIdx.x][i].op) m |= 1u << i;
+    pres[threadIdx.x] = m;
+  }
+  for (int t = threadIdx.x; t < MO * MI; t += kThreads) {
+    const int o = t / MI, i = t % MI;
+    cs[o][i] = (o < d.nout && i < d.nin) ? (T)eval_cf(d.c[o][i], rd.S) : T(0);
+  }
+  __syncthreads();
+  unsigned pm[MO];
+#pragma unroll
+  for (int o = 0; o < MO; ++o) pm[o] = pres[o];
+
+  double acc[ND > 0 ? ND : 1];
+#pragma unroll
+  for (int k = 0; k < ND; ++k) acc[k] = 0.0;
+
+  const long long npk = d.n / P;
+  const long long gstride = (long long)gridDim.x * kThreads;
+  for (int rep = 0; rep < d.reps; ++rep) {
+    const long long off = (long long)rep * d.stride;
+    for (long long q = (long long)blockIdx.x * kThreads + threadIdx.x; q < npk;
+         q += gstride) {
+      // Inputs are streamed one at a time into the output accumulators, so
+      // only the outputs and the dot operands stay live.
+      T r[MO][P], da[ND > 0 ? ND : 1][P], db[ND > 0 ? ND : 1][P];
+      bool first[MO];
+#pragma unroll
+      for (int o = 0; o < MO; ++o) first[o] = true;
+#pragma unroll
+      for (int i = 0; i < MI; ++i) {
+        if (i < d.nin) {
+          const T* p = d.in[i] + ((d.in_rep_mask >> i) & 1u ? off : 0);
+          T v[P];
+          unpack<T>(reinterpret_cast<const PV*>(p)[q], v);
+#pragma unroll
+          for (int o = 0; o < MO; ++o) {
+            if ((pm[o] >> i) & 1u) {
+              const T c = cs[o][i];
+#pragma unroll
+              for (int e = 0; e < P; ++e)
+                r[o][e] = first[o] ? mul_rn(c, v[e]) : fma_rn(c, v[e], r[o][e]);
+              first[o] = false;
+            }
+          }
+#pragma unroll
+          for (int k = 0; k < ND; ++k) {
+            if (d.dot[k][0] == i) {
+#pragma unroll
+              for (int e = 0; e < P; ++e) da[k][e] = v[e];
+            }
+            if (d.dot[k][1] == i) {
+#pragma unroll
+              for (int e = 0; e < P; ++e) db[k][e] = v[e];
+            }
+          }
+        }
+      }
+#pragma unroll
+      for (int o = 0; o < MO; ++o) {
+        if (o < d.nout) {
+          if (first[o]) {
+#pragma unroll
+            for (int e = 0; e < P; ++e) r[o][e] = T(0);
+          }
+          T* p = d.out[o] + ((d.out_rep_mask >> o) & 1u ? off : 0);
+          reinterpret_cast<PV*>(p)[q] = repack<T>(r[o]);
+#pragma unroll
+          for (int k = 0; k < ND; ++k) {
+            if (d.dot[k][0] == d.nin + o) {
+#pragma unroll
+              for (int e = 0; e < P; ++e) da[k][e] = r[o][e];
+            }
+            if (d.dot[k][1] == d.nin + o) {
+#pragma unroll
+              for (int e = 0; e < P; ++e) db[k][e] = r[o][e];
+            }
+          }
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < ND; ++k) {
+#pragma unroll
+        for (int e = 0; e < P; ++e) acc[k] += (double)da[k][e] * (double)db[k][e];
+      }
+    }
+  }
+  if (ND > 0 || rd.epi) finish_reduction<ND>(acc, rd);
+}
+
+}  // namespace bk

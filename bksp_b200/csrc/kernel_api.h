@@ -1,0 +1,113 @@
+// Host-visible kernel interface: plain structs shared by the CUDA kernels
+// (kernels.cu) and the host solver drivers (*.cpp), plus the launch entry
+// points.  Nothing here depends on device code.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace bk {
+
+constexpr int kScalars = 512;     // FP64 scalar slots per solve
+constexpr int kGridCap = 148 * 8; // reduction grid cap (= kMaxBlocks)
+constexpr int kNotConverged = -1;
+constexpr int kDivergence = -2;
+constexpr int kLcMaxIn = 24;   // widest linear combination (inputs)
+constexpr int kLcMaxOut = 4;   // widest linear combination (outputs)
+constexpr int kMaxDotsApi = 8;
+constexpr int kTileNnz = 2048;  // SpMV row block: max stored entries
+constexpr int kTileRows = 256;  // SpMV row block: max rows (= threads)
+
+// Coefficient of one linear-combination term (mirrors Cf in dev_common.cuh).
+struct CfH {
+  signed char op;   // 0 absent, 1 k, 2 k*S[s], 3 k/S[s], 4 k*S[s]/S[s2],
+                    // 5 k*S[s]*S[s2]
+  unsigned char pad;
+  short s, s2;
+  short pad2;
+  double k;
+};
+static inline CfH cf_const(double k) { CfH c{}; c.op = 1; c.k = k; return c; }
+static inline CfH cf_slot(short s, double k = 1.0) { CfH c{}; c.op = 2; c.s = s; c.k = k; return c; }
+static inline CfH cf_inv(short s, double k = 1.0) { CfH c{}; c.op = 3; c.s = s; c.k = k; return c; }
+static inline CfH cf_ratio(short s, short s2, double k = 1.0) {
+  CfH c{}; c.op = 4; c.s = s; c.s2 = s2; c.k = k; return c;
+}
+static inline CfH cf_prod(short s, short s2, double k = 1.0) {
+  CfH c{}; c.op = 5; c.s = s; c.s2 = s2; c.k = k; return c;
+}
+
+struct CtlH {
+  int done, iter, ret, max_iter, hist_cap, trips, trip_cap, hist_len;
+  double tol;
+  double* hist;
+};
+
+struct RedH {
+  double* part;
+  unsigned int* ticket;
+  double* S;
+  CtlH* ctl;
+  short out, epi, a0, a1;
+};
+
+// Device CSR matrix (one value precision).
+struct CsrH {
+  const int* rowptr;
+  const int* col;
+  const void* val;
+  const int* rb;
+  int n;
+  int nrb;
+};
+
+// One linear-combination launch: out[o] = sum_i c[o][i] * in[i], terms
+// evaluated in input order (first term a product, the rest fused
+// multiply-adds), repeated `reps` times with operands flagged in the rep
+// masks advanced by `stride` elements per repetition.  `nd` dot products
+// between any two of [in..., out...] (post-update values) are reduced into
+// the scalar slots.  Lengths are padded lengths (multiple of 64).
+template <typename T>
+struct LcH {
+  const T* in[kLcMaxIn];
+  T* out[kLcMaxOut];
+  CfH c[kLcMaxOut][kLcMaxIn];
+  long long n;
+  long long stride;
+  int nin, nout, reps;
+  unsigned in_rep_mask, out_rep_mask;
+  int nd;
+  unsigned char dot[kMaxDotsApi][2];
+};
+
+template <typename T>
+struct SpmvH {
+  const T* x;
+  T* y;
+  T* y2;
+  const T* b;
+  const T* w0;
+  const T* w1;
+  int mode;   // 0: y = A x   1: y = b - A x
+  int nd;
+  unsigned char dot[kMaxDotsApi][2];   // 0 = y, 1 = b, 2 = w0, 3 = w1
+};
+
+// ---- launches (kernels.cu) ----
+// SpMV: VT = matrix value type, T = vector/accumulation type.
+void launch_spmv_d(const CsrH& A, const SpmvH<double>& io, const RedH& rd,
+                   cudaStream_t st);
+void launch_spmv_f(const CsrH& A, const SpmvH<float>& io, const RedH& rd,
+                   cudaStream_t st);
+void launch_lincomb_d(const LcH<double>& d, const RedH& rd, cudaStream_t st);
+void launch_lincomb_f(const LcH<float>& d, const RedH& rd, cudaStream_t st);
+// Run only a scalar epilogue (one thread).
+void launch_epilogue(const RedH& rd, cudaStream_t st);
+// Element-wise precision conversions / mixed-precision updates.
+void launch_convert_d2f(const double* a, float* b, long long n, cudaStream_t st);
+void launch_convert_f2d(const float* a, double* b, long long n, cudaStream_t st);
+// Graph while-loop control: keep looping while !done and trips < trip_cap.
+void launch_loop_control(CtlH* ctl, unsigned long long handle, int use_handle,
+                         cudaStream_t st);
+
+}  // namespace bk

@@ -1,0 +1,125 @@
+// Single translation unit holding every device kernel of the library (the
+// scalar epilogues are one device function shared by all reductions) and
+// the host-callable launch wrappers declared in kernel_api.h.
+#include <cstdio>
+
+#include "dev_common.cuh"
+#include "epilogues.cuh"
+#include "k_spmv.cuh"
+#include "k_vec.cuh"
+#include "kernel_api.h"
+
+namespace bk {
+
+static inline int grid_for(long long work_items) {
+  long long g = (work_items + kThreads - 1) / kThreads;
+  if (g < 1) g = 1;
+  if (g > kMaxBlocks) g = kMaxBlocks;
+  return (int)g;
+}
+
+// ------------------------------------------------------------------ SpMV
+
+template <typename VT, typename XT>
+static void spmv_dispatch(const CsrH& A, const SpmvH<XT>& io, const RedH& rd,
+                          cudaStream_t st) {
+  const int g = A.nrb < kMaxBlocks ? (A.nrb > 0 ? A.nrb : 1) : kMaxBlocks;
+  switch (io.nd) {
+    case 0: k_spmv<VT, XT, 0><<<g, kThreads, 0, st>>>(A, io, rd); break;
+    case 1: k_spmv<VT, XT, 1><<<g, kThreads, 0, st>>>(A, io, rd); break;
+    case 2: k_spmv<VT, XT, 2><<<g, kThreads, 0, st>>>(A, io, rd); break;
+    default: k_spmv<VT, XT, 3><<<g, kThreads, 0, st>>>(A, io, rd); break;
+  }
+}
+
+void launch_spmv_d(const CsrH& A, const SpmvH<double>& io, const RedH& rd,
+                   cudaStream_t st) {
+  spmv_dispatch<double, double>(A, io, rd, st);
+}
+void launch_spmv_f(const CsrH& A, const SpmvH<float>& io, const RedH& rd,
+                   cudaStream_t st) {
+  spmv_dispatch<float, float>(A, io, rd, st);
+}
+
+// ------------------------------------------------------ linear combination
+
+template <typename T, int MI, int MO>
+static void lc_nd(const LcH<T>& d, const RedH& rd, cudaStream_t st) {
+  const int g = grid_for(d.n / Pack<T>::N);
+  switch (d.nd) {
+    case 0: k_lincomb<T, MI, MO, 0><<<g, kThreads, 0, st>>>(d, rd); break;
+    case 1: k_lincomb<T, MI, MO, 1><<<g, kThreads, 0, st>>>(d, rd); break;
+    case 2: k_lincomb<T, MI, MO, 2><<<g, kThreads, 0, st>>>(d, rd); break;
+    default: k_lincomb<T, MI, MO, 3><<<g, kThreads, 0, st>>>(d, rd); break;
+  }
+}
+
+template <typename T>
+static void lc_dispatch(const LcH<T>& d, const RedH& rd, cudaStream_t st) {
+  if (d.nin <= 4 && d.nout <= 2) lc_nd<T, 4, 2>(d, rd, st);
+  else if (d.nin <= 8 && d.nout <= 4) lc_nd<T, 8, 4>(d, rd, st);
+  else lc_nd<T, 24, 4>(d, rd, st);
+}
+
+void launch_lincomb_d(const LcH<double>& d, const RedH& rd, cudaStream_t st) {
+  lc_dispatch<double>(d, rd, st);
+}
+void launch_lincomb_f(const LcH<float>& d, const RedH& rd, cudaStream_t st) {
+  lc_dispatch<float>(d, rd, st);
+}
+
+// ----------------------------------------------------------- conversions
+
+__global__ void k_convert_d2f(const double* __restrict__ a, float* __restrict__ b,
+                              long long n) {
+  for (long long i = (long long)blockIdx.x * kThreads + threadIdx.x; i < n;
+       i += (long long)gridDim.x * kThreads)
+    b[i] = (float)a[i];
+}
+__global__ void k_convert_f2d(const float* __restrict__ a, double* __restrict__ b,
+                              long long n) {
+  for (long long i = (long long)blockIdx.x * kThreads + threadIdx.x; i < n;
+       i += (long long)gridDim.x * kThreads)
+    b[i] = (double)a[i];
+}
+void launch_convert_d2f(const double* a, float* b, long long n, cudaStream_t st) {
+  k_convert_d2f<<<grid_for(n), kThreads, 0, st>>>(a, b, n);
+}
+void launch_convert_f2d(const float* a, double* b, long long n, cudaStream_t st) {
+  k_convert_f2d<<<grid_for(n), kThreads, 0, st>>>(a, b, n);
+}
+
+// ------------------------------------------------------- scalar / control
+
+__global__ void k_epilogue(Red rd) {
+  if (finished(rd.ctl)) return;
+  run_epilogue(rd);
+}
+
+void launch_epilogue(const RedH& rd, cudaStream_t st) {
+  k_epilogue<<<1, 1, 0, st>>>(rd);
+}
+
+// Body-final node of a solve's CUDA-graph while loop.  The loop ends when a
+// convergence test has finished the solve, and in any case after trip_cap
+// trips: the cap is checked here, independently of the method's epilogues,
+// so a device-side loop can never outlive its iteration budget.
+__global__ void k_loop_control(Ctl* c, cudaGraphConditionalHandle h,
+                               int use_handle) {
+  const int trips = ++c->trips;
+  bool keep = !c->done;
+  if (keep && trips >= c->trip_cap) {
+    c->done = 1;
+    c->ret = kNotConverged;
+    keep = false;
+  }
+  if (use_handle) cudaGraphSetConditional(h, keep ? 1u : 0u);
+}
+
+void launch_loop_control(CtlH* ctl, unsigned long long handle, int use_handle,
+                         cudaStream_t st) {
+  k_loop_control<<<1, 1, 0, st>>>(ctl, (cudaGraphConditionalHandle)handle,
+                                  use_handle);
+}
+
+}  // namespace bk

@@ -1,0 +1,345 @@
+#include "runtime.h"
+
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+
+namespace bk {
+
+void check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) {
+    std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+    throw CudaError(m);
+  }
+}
+
+Ctx& Ctx::get() {
+  thread_local Ctx cx;
+  thread_local bool ready = false;
+  if (!ready) {
+    BK_CHECK(cudaGetDevice(&cx.device));
+    BK_CHECK(cudaStreamCreateWithFlags(&cx.st, cudaStreamNonBlocking));
+    const char* loop = std::getenv("BKSP_GPU_LOOP");
+    cx.use_cond_graph = !(loop && std::string(loop) == "poll");
+    // Keep freed solve buffers cached in the device pool between calls.
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, cx.device) == cudaSuccess) {
+      uint64_t thr = UINT64_MAX;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+    ready = true;
+  }
+  return cx;
+}
+
+void* dalloc(size_t bytes, cudaStream_t st) {
+  void* p = nullptr;
+  BK_CHECK(cudaMallocAsync(&p, bytes, st));
+  return p;
+}
+
+void dfree(void* p, cudaStream_t st) {
+  if (p) cudaFreeAsync(p, st);
+}
+
+void DevCsr::release(cudaStream_t st) {
+  dfree(rowptr, st);
+  dfree(col, st);
+  dfree(v64, st);
+  dfree(v32, st);
+  dfree(rb, st);
+  rowptr = col = rb = nullptr;
+  v64 = nullptr;
+  v32 = nullptr;
+}
+
+HostCsr expand_symmetric(int n, const int* rowptr, const int* col,
+                         const double* val) {
+  HostCsr h;
+  h.n = n;
+  std::vector<int> cnt(n + 1, 0);
+  for (int i = 0; i < n; ++i)
+    for (int k = rowptr[i]; k < rowptr[i + 1]; ++k) {
+      const int j = col[k];
+      if (j < 0 || j >= n) throw CudaError("matrix: column index out of range");
+      cnt[i]++;
+      if (j != i) cnt[j]++;
+    }
+  h.rowptr.assign(n + 1, 0);
+  for (int i = 0; i < n; ++i) h.rowptr[i + 1] = h.rowptr[i] + cnt[i];
+  const int nnz = h.rowptr[n];
+  h.col.resize(nnz);
+  h.val.resize(nnz);
+  std::vector<int> pos(h.rowptr.begin(), h.rowptr.end() - 1);
+  for (int i = 0; i < n; ++i)
+    for (int k = rowptr[i]; k < rowptr[i + 1]; ++k) {
+      const int j = col[k];
+      h.col[pos[i]] = j;
+      h.val[pos[i]++] = val[k];
+      if (j != i) {
+        h.col[pos[j]] = i;
+        h.val[pos[j]++] = val[k];
+      }
+    }
+  // Sort each row by column.
+  std::vector<std::pair<int, double>> tmp;
+  for (int i = 0; i < n; ++i) {
+    const int a = h.rowptr[i], b = h.rowptr[i + 1];
+    bool sorted = true;
+    for (int k = a + 1; k < b; ++k)
+      if (h.col[k] < h.col[k - 1]) { sorted = false; break; }
+    if (sorted) continue;
+    tmp.clear();
+    for (int k = a; k < b; ++k) tmp.push_back({h.col[k], h.val[k]});
+    std::stable_sort(tmp.begin(), tmp.end(),
+                     [](const std::pair<int, double>& x,
+                        const std::pair<int, double>& y) { return x.first < y.first; });
+    for (int k = a; k < b; ++k) {
+      h.col[k] = tmp[k - a].first;
+      h.val[k] = tmp[k - a].second;
+    }
+  }
+  return h;
+}
+
+HostCsr transpose(int n, const int* rowptr, const int* col, const double* val) {
+  HostCsr h;
+  h.n = n;
+  h.rowptr.assign(n + 1, 0);
+  const int nnz = rowptr[n];
+  for (int k = 0; k < nnz; ++k) {
+    if (col[k] < 0 || col[k] >= n) throw CudaError("matrix: column index out of range");
+    h.rowptr[col[k] + 1]++;
+  }
+  for (int i = 0; i < n; ++i) h.rowptr[i + 1] += h.rowptr[i];
+  h.col.resize(nnz);
+  h.val.resize(nnz);
+  std::vector<int> pos(h.rowptr.begin(), h.rowptr.end() - 1);
+  for (int i = 0; i < n; ++i)
+    for (int k = rowptr[i]; k < rowptr[i + 1]; ++k) {
+      const int p = pos[col[k]]++;
+      h.col[p] = i;
+      h.val[p] = val[k];
+    }
+  return h;
+}
+
+std::vector<int> make_row_blocks(int n, const int* rowptr) {
+  std::vector<int> rb;
+  rb.reserve(n / 64 + 2);
+  rb.push_back(0);
+  int rows = 0;
+  long long nz = 0;
+  for (int i = 0; i < n; ++i) {
+    const long long len = rowptr[i + 1] - rowptr[i];
+    if (rows > 0 && (rows == kTileRows || nz + len > kTileNnz)) {
+      rb.push_back(i);
+      rows = 0;
+      nz = 0;
+    }
+    rows++;
+    nz += len;
+    if (len > kTileNnz) {   // a long row is a block by itself
+      rb.push_back(i + 1);
+      rows = 0;
+      nz = 0;
+    }
+  }
+  if (rows > 0) rb.push_back(n);
+  return rb;
+}
+
+void upload_csr(int n, const int* rowptr, const int* col, const double* val,
+                bool want_fp32, DevCsr& out, cudaStream_t st) {
+  if (n <= 0) throw CudaError("matrix: empty");
+  const int nnz = rowptr[n];
+  if (rowptr[0] != 0 || nnz < 0) throw CudaError("matrix: bad row pointer");
+  for (int i = 0; i < n; ++i)
+    if (rowptr[i + 1] < rowptr[i]) throw CudaError("matrix: bad row pointer");
+  std::vector<int> rb = make_row_blocks(n, rowptr);
+  const long long padn = (long long)(nnz + 3) / 4 * 4 + 4;
+  out.n = n;
+  out.nnz = nnz;
+  out.nrb = (int)rb.size() - 1;
+  out.rowptr = dalloc_n<int>(n + 1, st);
+  out.col = dalloc_n<int>(padn, st);
+  out.v64 = dalloc_n<double>(padn, st);
+  out.rb = dalloc_n<int>((long long)rb.size(), st);
+  BK_CHECK(cudaMemsetAsync(out.col, 0, sizeof(int) * padn, st));
+  BK_CHECK(cudaMemsetAsync(out.v64, 0, sizeof(double) * padn, st));
+  BK_CHECK(cudaMemcpyAsync(out.rowptr, rowptr, sizeof(int) * (n + 1),
+                           cudaMemcpyHostToDevice, st));
+  if (nnz > 0) {
+    BK_CHECK(cudaMemcpyAsync(out.col, col, sizeof(int) * nnz,
+                             cudaMemcpyHostToDevice, st));
+    BK_CHECK(cudaMemcpyAsync(out.v64, val, sizeof(double) * nnz,
+                             cudaMemcpyHostToDevice, st));
+  }
+  BK_CHECK(cudaMemcpyAsync(out.rb, rb.data(), sizeof(int) * rb.size(),
+                           cudaMemcpyHostToDevice, st));
+  if (want_fp32) {
+    out.v32 = dalloc_n<float>(padn, st);
+    launch_convert_d2f(out.v64, out.v32, padn, st);
+    BK_CHECK(cudaGetLastError());
+  }
+}
+
+void SolveState::create(int cap, cudaStream_t st) {
+  S = dalloc_n<double>(kScalars, st);
+  ctl = dalloc_n<CtlH>(1, st);
+  part = dalloc_n<double>((long long)kMaxDotsApi * kGridCap, st);
+  ticket = dalloc_n<unsigned>(4, st);
+  hist_cap = cap;
+  hist = cap > 0 ? dalloc_n<double>(cap, st) : nullptr;
+  BK_CHECK(cudaMemsetAsync(S, 0, sizeof(double) * kScalars, st));
+  BK_CHECK(cudaMemsetAsync(ticket, 0, sizeof(unsigned) * 4, st));
+  BK_CHECK(cudaMemsetAsync(ctl, 0, sizeof(CtlH), st));
+}
+
+void SolveState::release(cudaStream_t st) {
+  dfree(S, st);
+  dfree(ctl, st);
+  dfree(part, st);
+  dfree(ticket, st);
+  dfree(hist, st);
+  S = nullptr;
+  ctl = nullptr;
+  part = nullptr;
+  ticket = nullptr;
+  hist = nullptr;
+}
+
+void SolveState::start(int iter0, int max_iter, double tol, cudaStream_t st) {
+  CtlH c;
+  std::memset(&c, 0, sizeof(c));
+  c.iter = iter0;
+  c.max_iter = max_iter;
+  c.tol = tol;
+  c.hist = hist;
+  c.hist_cap = hist_cap;
+  c.trip_cap = std::max(1, max_iter - iter0 + 2);
+  c.ret = kNotConverged;
+  BK_CHECK(cudaMemcpyAsync(ctl, &c, sizeof(c), cudaMemcpyHostToDevice, st));
+  BK_CHECK(cudaStreamSynchronize(st));
+}
+
+CtlH SolveState::read(cudaStream_t st) const {
+  CtlH c;
+  BK_CHECK(cudaMemcpyAsync(&c, ctl, sizeof(c), cudaMemcpyDeviceToHost, st));
+  BK_CHECK(cudaStreamSynchronize(st));
+  return c;
+}
+
+void SolveState::set_scalar(short slot, double v, cudaStream_t st) {
+  BK_CHECK(cudaMemcpyAsync(S + slot, &v, sizeof(double),
+                           cudaMemcpyHostToDevice, st));
+  BK_CHECK(cudaStreamSynchronize(st));
+}
+
+double SolveState::get_scalar(short slot, cudaStream_t st) const {
+  double v = 0.0;
+  BK_CHECK(cudaMemcpyAsync(&v, S + slot, sizeof(double),
+                           cudaMemcpyDeviceToHost, st));
+  BK_CHECK(cudaStreamSynchronize(st));
+  return v;
+}
+
+template <typename T>
+void Lc<T>::launch(const RedH& rd, cudaStream_t st) {
+  for (size_t k = 0; k < dots_.size(); ++k) {
+    int a = dots_[k].first, b = dots_[k].second;
+    if (a >= OUT) a = d.nin + (a - OUT);
+    if (b >= OUT) b = d.nin + (b - OUT);
+    d.dot[k][0] = (unsigned char)a;
+    d.dot[k][1] = (unsigned char)b;
+  }
+  if constexpr (sizeof(T) == 8)
+    launch_lincomb_d(d, rd, st);
+  else
+    launch_lincomb_f(d, rd, st);
+}
+template struct Lc<double>;
+template struct Lc<float>;
+
+void spmv(const DevCsr& A, const SpmvH<double>& io, const RedH& rd,
+          cudaStream_t st) {
+  launch_spmv_d(A.h64(), io, rd, st);
+}
+void spmv(const DevCsr& A, const SpmvH<float>& io, const RedH& rd,
+          cudaStream_t st) {
+  launch_spmv_f(A.h32(), io, rd, st);
+}
+
+static bool run_graph_while(SolveState& ss,
+                            const std::function<void(cudaStream_t)>& body,
+                            cudaStream_t st) {
+  cudaGraph_t g = nullptr;
+  cudaGraphExec_t ex = nullptr;
+  if (cudaGraphCreate(&g, 0) != cudaSuccess) return false;
+  bool ok = false;
+  do {
+    cudaGraphConditionalHandle h;
+    if (cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault) !=
+        cudaSuccess)
+      break;
+    alignas(cudaGraphNodeParams) unsigned char raw[sizeof(cudaGraphNodeParams)];
+    std::memset(raw, 0, sizeof(raw));
+    cudaGraphNodeParams& cp = *reinterpret_cast<cudaGraphNodeParams*>(raw);
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    if (cudaGraphAddNode(&node, g, nullptr, 0, &cp) != cudaSuccess) break;
+    cudaGraph_t bodyg = cp.conditional.phGraph_out[0];
+    if (cudaStreamBeginCaptureToGraph(st, bodyg, nullptr, nullptr, 0,
+                                      cudaStreamCaptureModeThreadLocal) !=
+        cudaSuccess)
+      break;
+    body(st);
+    launch_loop_control(ss.ctl, (unsigned long long)h, 1, st);
+    cudaGraph_t captured = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(st, &captured);
+    if (ce != cudaSuccess) {
+      cudaGetLastError();
+      break;
+    }
+    if (cudaGraphInstantiate(&ex, g, 0) != cudaSuccess) {
+      cudaGetLastError();
+      ex = nullptr;
+      break;
+    }
+    ok = true;
+  } while (false);
+  if (ok) {
+    BK_CHECK(cudaGraphLaunch(ex, st));
+    BK_CHECK(cudaStreamSynchronize(st));
+  }
+  if (ex) cudaGraphExecDestroy(ex);
+  cudaGraphDestroy(g);
+  return ok;
+}
+
+CtlH run_loop(SolveState& ss, const std::function<void(cudaStream_t)>& body,
+              cudaStream_t st) {
+  CtlH c = ss.read(st);
+  if (c.done) return c;
+  Ctx& cx = Ctx::get();
+  if (cx.use_cond_graph) {
+    if (run_graph_while(ss, body, st)) return ss.read(st);
+    cx.use_cond_graph = false;   // not supported here: poll from now on
+  }
+  int chunk = 1;
+  for (;;) {
+    for (int k = 0; k < chunk; ++k) {
+      body(st);
+      launch_loop_control(ss.ctl, 0ull, 0, st);
+    }
+    BK_CHECK(cudaGetLastError());
+    c = ss.read(st);
+    if (c.done) return c;
+    chunk = std::min(chunk * 2, 32);
+  }
+}
+
+}  // namespace bk

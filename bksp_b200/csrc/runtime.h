@@ -1,0 +1,174 @@
+// Host runtime of the solver library: per-thread device context, stream-
+// ordered device allocation, CSR upload, per-solve scalar/control state,
+// linear-combination builder and the CUDA-graph iteration loop.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstring>
+#include <functional>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "kernel_api.h"
+#include "solver_defs.h"
+
+namespace bk {
+
+// Any CUDA failure inside the library becomes this exception; the C entry
+// points catch it and return INVALID_PARAMETERS.
+struct CudaError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+void check(cudaError_t e, const char* what);
+#define BK_CHECK(call) ::bk::check((call), #call)
+
+inline long long pad64(long long n) { return (n + 63) / 64 * 64; }
+
+// Per-host-thread library context: device, stream, pinned staging.
+struct Ctx {
+  int device = 0;
+  cudaStream_t st = nullptr;
+  bool use_cond_graph = true;   // CUDA-graph while loop (else host polling)
+  static Ctx& get();
+};
+
+// Stream-ordered device allocation from the device's memory pool (freed
+// blocks stay cached in the pool for the next solve).
+void* dalloc(size_t bytes, cudaStream_t st);
+void dfree(void* p, cudaStream_t st);
+template <typename T>
+T* dalloc_n(long long n, cudaStream_t st) {
+  return static_cast<T*>(dalloc(sizeof(T) * (size_t)(n > 0 ? n : 1), st));
+}
+
+// Device CSR operator.  Values are kept in FP64 (parity solves, true
+// residuals) and, on request, FP32 (mixed-precision inner solves), sharing
+// one index structure.
+struct DevCsr {
+  int n = 0, nnz = 0, nrb = 0;
+  int* rowptr = nullptr;
+  int* col = nullptr;
+  double* v64 = nullptr;
+  float* v32 = nullptr;
+  int* rb = nullptr;
+  CsrH h64() const { return CsrH{rowptr, col, v64, rb, n, nrb}; }
+  CsrH h32() const { return CsrH{rowptr, col, v32, rb, n, nrb}; }
+  void release(cudaStream_t st);
+};
+
+// Host-side CSR (0-based, int32).
+struct HostCsr {
+  int n = 0;
+  std::vector<int> rowptr, col;
+  std::vector<double> val;
+};
+
+// Mirror every stored off-diagonal entry (a "symmetric" bksp matrix stores
+// one triangle; reference src/matvec.c:100-127).  Rows come out sorted by
+// column.
+HostCsr expand_symmetric(int n, const int* rowptr, const int* col,
+                         const double* val);
+// A^T in CSR; entries of each row ordered by the original row index, which
+// reproduces the summation order of the reference's scatter A^T x
+// (src/matvec.c:29-45).
+HostCsr transpose(int n, const int* rowptr, const int* col, const double* val);
+
+// Upload a host CSR (rows in the caller's order) and build its row blocks.
+void upload_csr(int n, const int* rowptr, const int* col, const double* val,
+                bool want_fp32, DevCsr& out, cudaStream_t st);
+
+// Row-block partition used by the SpMV tile kernel.
+std::vector<int> make_row_blocks(int n, const int* rowptr);
+
+// Per-solve device state: scalar slots, control block, reduction scratch,
+// optional residual history.
+struct SolveState {
+  double* S = nullptr;
+  CtlH* ctl = nullptr;
+  double* part = nullptr;
+  unsigned* ticket = nullptr;
+  double* hist = nullptr;
+  int hist_cap = 0;
+  void create(int hist_cap, cudaStream_t st);
+  void release(cudaStream_t st);
+  // Reset control: iteration index starts at iter0, budget max_iter.
+  void start(int iter0, int max_iter, double tol, cudaStream_t st);
+  RedH red(short out, short epi, short a0 = 0, short a1 = 0) const {
+    return RedH{part, ticket, S, ctl, out, epi, a0, a1};
+  }
+  CtlH read(cudaStream_t st) const;
+  void set_scalar(short slot, double v, cudaStream_t st);
+  double get_scalar(short slot, cudaStream_t st) const;
+};
+
+// Builder for one fused linear-combination launch (LcH).
+template <typename T>
+struct Lc {
+  LcH<T> d;
+  explicit Lc(long long n) {
+    std::memset(&d, 0, sizeof(d));
+    d.n = n;
+    d.reps = 1;
+  }
+  static constexpr int OUT = 100;   // dot operand code base for outputs
+  int in(const T* p, bool rep = false) {
+    if (d.nin >= kLcMaxIn) throw CudaError("lincomb: too many inputs");
+    const int i = d.nin++;
+    d.in[i] = p;
+    if (rep) d.in_rep_mask |= 1u << i;
+    return i;
+  }
+  int out(T* p, bool rep = false) {
+    if (d.nout >= kLcMaxOut) throw CudaError("lincomb: too many outputs");
+    const int o = d.nout++;
+    d.out[o] = p;
+    if (rep) d.out_rep_mask |= 1u << o;
+    return o;
+  }
+  Lc& term(int o, int i, CfH c) {
+    d.c[o][i] = c;
+    return *this;
+  }
+  // Operands: input index, or OUT + output index.
+  Lc& dot(int a, int b) {
+    if (d.nd >= 3) throw CudaError("lincomb: too many dots");
+    dots_.push_back({a, b});
+    d.nd++;
+    return *this;
+  }
+  Lc& batch(int reps, long long stride) {
+    d.reps = reps;
+    d.stride = stride;
+    return *this;
+  }
+  void launch(const RedH& rd, cudaStream_t st);
+ private:
+  std::vector<std::pair<int, int>> dots_;
+};
+
+// Runs `body` (one iteration's launches) until the solve is done, as a
+// CUDA-graph while loop (one graph launch per solve) or, as fallback, by
+// host polling.  Returns the final control block.
+CtlH run_loop(SolveState& ss, const std::function<void(cudaStream_t)>& body,
+              cudaStream_t st);
+
+// Convenience for SpMV launches.
+template <typename T>
+SpmvH<T> spmv_io(const T* x, T* y) {
+  SpmvH<T> io;
+  std::memset(&io, 0, sizeof(io));
+  io.x = x;
+  io.y = y;
+  return io;
+}
+
+void spmv(const DevCsr& A, const SpmvH<double>& io, const RedH& rd,
+          cudaStream_t st);
+void spmv(const DevCsr& A, const SpmvH<float>& io, const RedH& rd,
+          cudaStream_t st);
+
+}  // namespace bk

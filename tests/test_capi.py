@@ -1,0 +1,95 @@
+"""Host-side checks of libbksp.so that need no GPU: every function the
+public headers declare is exported, argument validation, the Matrix Market
+reader and the dense helpers."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+import bksp_b200 as B
+from conftest import ROOT
+
+HEADERS = ["include/bksp.h", "include/bksp_gpu.h"]
+
+
+def _declared():
+    names = set()
+    for h in HEADERS:
+        src = open(os.path.join(ROOT, h)).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        src = re.sub(r"static inline[^{]*\{[^}]*\}", "", src, flags=re.S)
+        for m in re.finditer(r"^\s*[A-Za-z_][\w\s\*]*?\b([a-z_][\w]*)\s*\(", src, re.M):
+            name = m.group(1)
+            if name not in ("if", "return", "sizeof", "defined"):
+                names.add(name)
+    return names
+
+
+def test_headers_declare_the_bksp_api():
+    names = _declared()
+    for f in ["bksp_dcg", "dcr", "dbicg", "dbicgstab", "dbicgstabl", "dblcg",
+              "dblbicgstab", "dblbicgstabl", "dshbicg", "dshbicgstabl",
+              "read_matrix_market", "myqr", "dmat_create", "darray2dmat",
+              "dmat_free", "dvec2mat"]:
+        assert f in names, f
+
+
+def test_library_exports_every_declared_symbol():
+    lib = C.CDLL(B.LIB_PATH)
+    missing = [n for n in sorted(_declared()) if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_invalid_arguments_are_rejected_without_gpu_work():
+    # Matrix type checks happen before any device call.
+    rp = np.array([0, 1, 2], np.int32)
+    A = B.CsrMatrix(rp, np.array([0, 1], np.int32), np.array([1.0, 1.0]))
+    x = np.zeros(2)
+    assert B.bksp_dcg(A, np.ones(2), 1e-8, 10, x) == B.INVALID_MATRIX_TYPE
+    assert B.dcr(A, np.ones(2), 1e-8, 10, x) == B.INVALID_MATRIX_TYPE
+    assert B.dbicgstabl(A, np.ones(2), 0, 1e-8, 10, x) == B.INVALID_PARAMETERS
+    assert B.dbicgstabl(A, np.ones(2), 99, 1e-8, 10, x) == B.INVALID_PARAMETERS
+    # Row pointer inconsistent with nnz.
+    bad = B.CsrMatrix(np.array([0, 1, 3], np.int32), np.array([0, 1], np.int32),
+                      np.array([1.0, 1.0]))
+    assert B.dbicg(bad, np.ones(2), 1e-8, 10, x) == B.INVALID_PARAMETERS
+
+
+def test_read_matrix_market_matches_reference_reader(tmp_path, testmats):
+    # Write pde2961 back out (general) and bfwb398 (symmetric triangle) and
+    # read them with the library: same CSR, entries in file order.
+    for name, sym in (("pde", False), ("bfwb", True)):
+        rp, c, v = (testmats[f"{name}_rowptr"], testmats[f"{name}_col"],
+                    testmats[f"{name}_val"])
+        n = rp.size - 1
+        rows = np.repeat(np.arange(n), np.diff(rp))
+        p = tmp_path / f"{name}.mtx"
+        with open(p, "w") as f:
+            f.write("%%MatrixMarket matrix coordinate real "
+                    + ("symmetric" if sym else "general") + "\n% comment\n")
+            f.write(f"{n} {n} {rp[-1]}\n")
+            for i, j, a in zip(rows, c, v):
+                f.write(f"{i + 1} {j + 1} {float(a)!r}\n")
+        r2, c2, v2, n2, t2 = B.read_matrix_market(str(p))
+        assert n2 == n and t2 == ("symmetric" if sym else "unsymmetric")
+        assert np.array_equal(r2, rp) and np.array_equal(c2, c)
+        assert np.array_equal(v2, v)
+    with pytest.raises(OSError):
+        B.read_matrix_market(str(tmp_path / "missing.mtx"))
+
+
+def test_dense_helpers():
+    d = B.lib.dmat_create
+    d.restype = C.POINTER(B.DMat)
+    d.argtypes = [C.c_int, C.c_int]
+    m = d(5, 3).contents
+    assert (m.row_size, m.col_size) == (5, 3)
+    vals = np.ctypeslib.as_array(m.value, shape=(15,))
+    assert np.all(vals == 0.0)
+    x = np.arange(5, dtype=np.float64)
+    B.lib.dvec2mat.argtypes = [C.POINTER(C.c_double), C.c_int, C.POINTER(B.DMat)]
+    B.lib.dvec2mat(x.ctypes.data_as(C.POINTER(C.c_double)), 1, C.byref(m))
+    # reference src/util.c:57-67 writes value[i * col_size + m]
+    assert [vals[i * 3 + 1] for i in range(5)] == list(x)

@@ -1,0 +1,185 @@
+"""GPU parity of the single-right-hand-side methods (through the C-ABI)
+against the compiled reference's golden outputs and the CPU oracle."""
+import ctypes as C
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+from conftest import hist_close, iters_close
+from bksp_b200 import problems as P
+from oracle import solvers as S
+
+pytestmark = pytest.mark.gpu
+
+_dp = C.POINTER(C.c_double)
+
+
+def _spmv(B, A, trans, x):
+    B.lib.bksp_gpu_dcsrmv.argtypes = [C.c_void_p, C.c_char, _dp, _dp]
+    y = np.zeros(A.n)
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    rc = B.lib.bksp_gpu_dcsrmv(C.addressof(A.s), trans, x.ctypes.data_as(_dp),
+                               y.ctypes.data_as(_dp))
+    assert rc == 0
+    return y
+
+
+def _row_sums_sequential(rp, c, v, x):
+    """y_i = ((0 + a_0 x_0) + a_1 x_1) + ... with FP64 rounding per step,
+    the reference's dcsrgemm0 order (src/matvec.c:19-27)."""
+    n = rp.size - 1
+    y = np.zeros(n)
+    L = np.diff(rp)
+    prod = v * x[c]
+    acc = np.zeros(n)
+    for k in range(L.max()):
+        m = L > k
+        acc[m] = acc[m] + prod[rp[:-1][m] + k]
+    return acc
+
+
+def test_spmv_bit_exact_vs_reference_order(gpu, testmats):
+    rp, c, v = testmats["pde_rowptr"], testmats["pde_col"], testmats["pde_val"]
+    A = gpu.CsrMatrix(rp, c, v)
+    x = np.random.default_rng(5).uniform(-1, 1, A.n)
+    y = _spmv(gpu, A, b"n", x)
+    assert np.array_equal(y, _row_sums_sequential(rp, c, v, x))
+    # A^T: rows of the transpose in original row order (scatter order).
+    At = sp.csr_matrix((v, c, rp), shape=(A.n, A.n)).T.tocsr()
+    yt = _spmv(gpu, A, b"t", x)
+    np.testing.assert_allclose(yt, At @ x, rtol=1e-13, atol=1e-13)
+    # Mirrored one-triangle operator.
+    Ls = gpu.CsrMatrix(testmats["bfwb_rowptr"], testmats["bfwb_col"],
+                       testmats["bfwb_val"], symmetric=True)
+    Lf = S.full_symmetric(sp.csr_matrix(
+        (testmats["bfwb_val"], testmats["bfwb_col"], testmats["bfwb_rowptr"]),
+        shape=(Ls.n, Ls.n)))
+    xs = np.random.default_rng(6).uniform(-1, 1, Ls.n)
+    np.testing.assert_allclose(_spmv(gpu, Ls, b"s", xs), Lf @ xs, rtol=1e-12,
+                               atol=1e-20)
+
+
+@pytest.mark.parametrize("nrows,rowlen", [(1, 5000), (3, 2049), (700, 0), (1000, 1)])
+def test_spmv_ragged_and_long_rows(gpu, nrows, rowlen):
+    rng = np.random.default_rng(nrows)
+    n = max(nrows, 64)
+    lens = rng.integers(0, 12, n)
+    lens[:nrows] = rowlen
+    rp = np.zeros(n + 1, np.int64)
+    np.cumsum(lens, out=rp[1:])
+    c = rng.integers(0, n, rp[-1]).astype(np.int32)
+    v = rng.uniform(-1, 1, rp[-1])
+    A = gpu.CsrMatrix(rp.astype(np.int32), c, v)
+    x = rng.uniform(-1, 1, n)
+    y = _spmv(gpu, A, b"n", x)
+    ref = sp.csr_matrix((v, c, rp), shape=(n, n)) @ x
+    np.testing.assert_allclose(y, ref, rtol=1e-12, atol=1e-12)
+    short = lens <= 2048
+    assert np.array_equal(y[short], _row_sums_sequential(rp, c, v, x)[short])
+
+
+def _pde(gpu, tm):
+    A = gpu.CsrMatrix(tm["pde_rowptr"], tm["pde_col"], tm["pde_val"])
+    As = sp.csr_matrix((tm["pde_val"], tm["pde_col"], tm["pde_rowptr"]),
+                       shape=(A.n, A.n))
+    return A, As
+
+
+def test_cg_cr_known_answers(gpu, testmats, golden):
+    Ls = gpu.CsrMatrix(testmats["bfwb_rowptr"], testmats["bfwb_col"],
+                       testmats["bfwb_val"], symmetric=True)
+    Af = S.full_symmetric(sp.csr_matrix(
+        (testmats["bfwb_val"], testmats["bfwb_col"], testmats["bfwb_rowptr"]),
+        shape=(Ls.n, Ls.n)))
+    b = np.zeros(Ls.n); b[0] = 1.0
+    for key, fn in (("testc/cg", gpu.bksp_dcg), ("testc/cr", gpu.dcr)):
+        g = golden[key]
+        x = np.zeros(Ls.n)
+        with gpu.record(hist_cap=1000) as st:
+            ret = fn(Ls, b, 1e-14, 500, x)
+        assert iters_close(ret, g["ret"]), (key, ret, g["ret"])
+        assert abs(np.linalg.norm(x) - g["xnorm"]) < 1e-6 * g["xnorm"]
+        assert S.true_residual(Af, b, x) < 10 * max(g["true_res"], 1e-15)
+        hist_close(st["hist"], g["hist"], floor=1e-6)
+
+
+@pytest.mark.parametrize("key,call", [
+    ("testc/bicg", lambda B, A, b, x: B.dbicg(A, b, 1e-14, 500, x)),
+    ("testc/bicgstab", lambda B, A, b, x: B.dbicgstab(A, b, 1e-14, 500, x)),
+    ("testc/bicgstabl4", lambda B, A, b, x: B.dbicgstabl(A, b, 4, 1e-14, 500, x)),
+])
+def test_nonsymmetric_known_answers(gpu, testmats, golden, key, call):
+    A, As = _pde(gpu, testmats)
+    b = np.zeros(A.n); b[0] = 1.0
+    x = np.zeros(A.n)
+    with gpu.record(hist_cap=1000) as st:
+        ret = call(gpu, A, b, x)
+    g = golden[key]
+    # tol 1e-14 sits at the rounding floor of this problem: the reference
+    # itself moves by several iterations with its BLAS thread count.
+    assert iters_close(ret, g["ret"], rel=0.08), (key, ret, g["ret"])
+    assert S.true_residual(As, b, x) < 1e-12
+    hist_close(st["hist"], g["hist"], floor=1e-6)
+
+
+def test_seeded_configs_match_reference(gpu, golden):
+    rp, c, v, n = P.poisson2d(64)
+    lrp, lc, lv, _ = P.lower_triangle(rp, c, v, n)
+    Af = sp.csr_matrix((v, c, rp), shape=(n, n))
+    b = P.uniform(n, 0)
+    for key, fn in (("cfg1/cg_poisson64", gpu.bksp_dcg), ("cfg1/cr_poisson64", gpu.dcr)):
+        x = np.zeros(n)
+        with gpu.record(hist_cap=20000) as st:
+            ret = fn(gpu.CsrMatrix(lrp, lc, lv, symmetric=True), b, 1e-10, 10000, x)
+        g = golden[key]
+        assert iters_close(ret, g["ret"]), (key, ret, g["ret"])
+        hist_close(st["hist"], g["hist"], floor=1e-8)
+        assert S.true_residual(Af, b, x) < 1e-9
+    rp, c, v, n = P.convdiff3d(24)
+    Af = sp.csr_matrix((v, c, rp), shape=(n, n))
+    b = Af @ P.uniform(n, 1)
+    A = gpu.CsrMatrix(rp, c, v)
+    runs = [(f"cfg2/bicgstabl{l}_cd24",
+             (lambda l: lambda x: gpu.dbicgstabl(A, b, l, 1e-10, 2000, x))(l))
+            for l in (1, 2, 4)]
+    runs += [("cfg2/bicgstab_cd24", lambda x: gpu.dbicgstab(A, b, 1e-10, 2000, x)),
+             ("cfg2/bicg_cd24", lambda x: gpu.dbicg(A, b, 1e-10, 2000, x))]
+    for key, run in runs:
+        x = np.zeros(n)
+        with gpu.record(hist_cap=5000) as st:
+            ret = run(x)
+        g = golden[key]
+        assert iters_close(ret, g["ret"]), (key, ret, g["ret"])
+        hist_close(st["hist"], g["hist"], floor=1e-8)
+        assert S.true_residual(Af, b, x) < 1e-9
+
+
+def test_initial_guess_and_budget(gpu):
+    rp, c, v, n = P.convdiff3d(10)
+    Af = sp.csr_matrix((v, c, rp), shape=(n, n))
+    b = Af @ P.uniform(n, 1)
+    A = gpu.CsrMatrix(rp, c, v)
+    x0 = P.uniform(n, 7)
+    ret_o, x_o, _ = S.bicgstabl(Af, b, 2, 1e-10, 500, x0=x0)
+    x = x0.copy()
+    ret = gpu.dbicgstabl(A, b, 2, 1e-10, 500, x)
+    assert iters_close(ret, ret_o)
+    np.testing.assert_allclose(x, x_o, atol=1e-8)
+    # Budget exhausted -> NOT_CONVERGED; no iteration -> first index.
+    x = np.zeros(n)
+    assert gpu.dbicgstabl(A, b, 2, 1e-10, 2, x) == gpu.NOT_CONVERGED
+    x = np.zeros(n)
+    assert gpu.dbicgstab(A, b, 1e-10, 0, x) == 0
+    assert np.all(x == 0)
+    Ls = gpu.CsrMatrix(*P.lower_triangle(*P.poisson2d(8))[:3], symmetric=True)
+    assert gpu.dcr(Ls, np.ones(64), 1e-10, 1, np.zeros(64)) == 1
+
+
+def test_nan_breakdown_is_divergence(gpu):
+    # A zero matrix gives alpha = 0/0 in the first iteration.
+    n = 64
+    rp = np.arange(n + 1, dtype=np.int32)
+    A = gpu.CsrMatrix(rp, np.arange(n, dtype=np.int32), np.zeros(n))
+    x = np.zeros(n)
+    assert gpu.dbicgstab(A, np.ones(n), 1e-10, 50, x) == gpu.DIVERGENCE
