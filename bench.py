@@ -1,0 +1,373 @@
+#!/usr/bin/env python
+"""Benchmark: time to an FP64 true relative residual ||b - A x|| / ||b|| <=
+1e-8 on one B200, BiCGSTAB(4) on the 3D convection-diffusion 7-point upwind
+stencil, 128^3 grid (n = 2,097,152, nnz = 14,581,760), b = A x_true with
+x_true ~ U[-1, 1] (seed 1).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Our arm prints one JSON line:
+  value        time-to-solution (s) of the headline solve with A, b, x
+               resident in HBM (CUDA events on the launching stream, max over
+               ranks); the headline solve is the best available GPU mode,
+               named in config.mode, and the plain FP64 GPU solve is reported
+               beside it (plain_fp64_s);
+  e2e          the same solve through the public bksp.h call with host
+               arrays (upload of the CSR operator, b and x0 from pinned host
+               memory and download of x inside the timed region);
+  roofline     the SpMV kernel (dominant kernel) timed alone with CUDA events
+               over the same operator, algorithmic bytes / duration vs the
+               measured HBM copy bandwidth;
+  cpu_baseline the reference (aldente39/bksp compiled from source with gcc +
+               OpenBLAS, oracle/_ref) on this host's cores, one full solve.
+With --gpus N > 1 each rank solves its own replica (the method does not
+shard): value is the max over ranks.
+
+--impl reference times the reference CPU implementation instead: each step
+runs a bounded number of outer iterations; value = measured time per outer
+iteration x the iteration count of one full reference solve (run once,
+untimed, in warm-up).
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "time to 1e-8 FP64 true residual: learned-precond mixed vs plain FP64, same B200"
+TOL_TRUE = 1e-8
+L_DEG = 4
+NX = 128
+
+
+def args_():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--nx", type=int, default=NX)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def problem(nx):
+    from bksp_b200 import problems as P
+    rp, c, v, n = P.convdiff3d(nx)
+    xt = P.uniform(n, 1)
+    b = P.csr_matvec(rp, c, v, xt)
+    return rp, c, v, n, b
+
+
+def workload_config(nx, n, nnz):
+    return {"workload": f"bicgstabl{L_DEG}_convdiff3d_{nx}^3",
+            "n": n, "nnz": nnz, "l": L_DEG, "tol_true_residual": TOL_TRUE,
+            "rhs": "b = A x_true, x_true ~ U[-1,1] seed 1",
+            "l2": "inputs larger than L2 (FP64 CSR %.0f MB)" % ((nnz * 12 + 4 * n) / 1e6),
+            "parallelism": "replicas"}
+
+
+# ----------------------------------------------------------- reference arm
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    cores = os.cpu_count() or 1
+    os.environ["OPENBLAS_NUM_THREADS"] = str(cores)
+    os.environ["OMP_NUM_THREADS"] = str(cores)
+    from oracle import ref as R
+    rp, c, v, n, b = problem(a.nx)
+    A = R.Matrix(rp, c, v, n)
+    # Full solve once (warm-up, untimed): the reference's iteration count.
+    t0 = time.perf_counter()
+    ret_full, outs, _ = R.call("dbicgstabl", A, b, L_DEG, TOL_TRUE, 10000, np.zeros(n))
+    full_s = time.perf_counter() - t0
+    iters_full = ret_full + 1 if ret_full >= 0 else 10000
+    sample = 8
+    for _ in range(max(a.warmup - 1, 0)):
+        R.call("dbicgstabl", A, b, L_DEG, 1e-300, sample, np.zeros(n))
+    times = []
+    for _ in range(a.steps):
+        t0 = time.perf_counter()
+        R.call("dbicgstabl", A, b, L_DEG, 1e-300, sample, np.zeros(n))
+        times.append(time.perf_counter() - t0)
+    per_iter = float(np.mean(times)) / sample
+    value = per_iter * iters_full
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "s",
+        "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": 1e3 * float(np.mean(times)), "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": workload_config(a.nx, n, int(rp[-1])),
+        "cpu_baseline": {"value": value, "unit": "s", "cores": cores,
+                         "kind": "reference",
+                         "sample": f"{sample} outer iterations per step; "
+                                   f"x {iters_full} iterations of one full "
+                                   f"solve ({full_s:.1f} s wall, ret {ret_full})"},
+        "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "reference_full_solve_s": full_s,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------ our arm
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.p = None
+        return self
+
+    def __exit__(self, *exc):
+        self.rows = []
+        if self.p is None:
+            return
+        time.sleep(0.25)
+        self.p.terminate()
+        try:
+            out, _ = self.p.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+            out, _ = self.p.communicate()
+        for line in out.strip().splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9:
+                self.rows.append(f)
+
+    def summary(self):
+        if not getattr(self, "rows", None):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4)
+                          if r[5 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def run_ours(a):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    import bksp_b200 as B
+
+    rp, c, v, n, b_h = problem(a.nx)
+    nnz = int(rp[-1])
+    Ah = B.CsrMatrix(rp, c, v)
+    G = B.GpuMatrix(Ah, B.FP32)
+    dev = torch.device("cuda", local)
+    b = torch.from_numpy(b_h).to(dev)
+    x = torch.zeros(n, dtype=torch.float64, device=dev)
+    # A dedicated (non-default) stream: the library orders its work on it and
+    # the CUDA events below are recorded on it.
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    sp = stream.cuda_stream
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def plain_step():
+        x.zero_()
+        ret, st = G.solve(B.BICGSTABL, b.data_ptr(), x.data_ptr(), TOL_TRUE,
+                          10000, l=L_DEG, stream=sp)
+        return ret, st
+
+    def timed(step, k):
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ms, last = [], None
+        for _ in range(k):
+            ev0.record(stream)
+            last = step()
+            ev1.record(stream)
+            ev1.synchronize()
+            ms.append(ev0.elapsed_time(ev1))
+        return ms, last
+
+    def max_over_ranks(val):
+        if world == 1:
+            return val
+        t = torch.tensor([val], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # Headline mode (until the mixed solve lands: plain FP64 BiCGSTAB(l)).
+    mode, step = "plain_fp64", plain_step
+    for _ in range(a.warmup):
+        step()
+    barrier()
+    with Clocks(local) as clk:
+        ms, (ret, st) = timed(step, a.steps)
+    barrier()
+    step_ms = max_over_ranks(float(np.mean(ms)))
+    true_res = G.true_residual(b.data_ptr(), x.data_ptr(), sp)
+    plain_ms = step_ms
+    launches = int(st["launches"]) * a.steps
+
+    # Dominant kernel alone: SpMV over the same operator, FP64 and FP32.
+    xs64 = torch.rand(n, dtype=torch.float64, device=dev)
+    ys64 = torch.empty(n, dtype=torch.float64, device=dev)
+    xs32 = xs64.float()
+    ys32 = torch.empty(n, dtype=torch.float32, device=dev)
+    reps = 50
+    kern = {}
+    for name, xx, yy, f32 in (("spmv_fp64", xs64, ys64, False),
+                              ("spmv_fp32", xs32, ys32, True)):
+        for _ in range(5):
+            G.spmv(xx.data_ptr(), yy.data_ptr(), f32, sp)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            G.spmv(xx.data_ptr(), yy.data_ptr(), f32, sp)
+        e1.record(stream)
+        e1.synchronize()
+        kern[name] = e0.elapsed_time(e1) / reps
+    wv = 8 if mode == "plain_fp64" else 4
+    kname = "spmv_fp64" if wv == 8 else "spmv_fp32"
+    alg_bytes = nnz * (wv + 4) + 4 * (n + 1) + 2 * wv * n
+    peak, peak_kind = peaks()
+    achieved = alg_bytes / (kern[kname] * 1e-3) / 1e9
+    traffic = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            traffic = json.load(f).get(kname)
+    except (OSError, ValueError):
+        traffic = None
+
+    # End to end through bksp.h with host arrays (pinned).
+    def pinned(arr):
+        t = torch.from_numpy(np.ascontiguousarray(arr)).pin_memory()
+        return t, t.numpy()
+    _, rp_p = pinned(rp)
+    _, c_p = pinned(c)
+    _, v_p = pinned(v)
+    _, b_p = pinned(b_h)
+    xt_, x_p = pinned(np.zeros(n))
+    Ap = B.CsrMatrix(rp_p, c_p, v_p)
+    e2e_ms = []
+    for i in range(a.warmup + a.steps):
+        x_p[:] = 0.0
+        if world > 1:
+            dist.barrier()
+        t0 = time.perf_counter()
+        r_e2e = B.dbicgstabl(Ap, b_p, L_DEG, TOL_TRUE, 10000, x_p)
+        dt = time.perf_counter() - t0
+        if i >= a.warmup:
+            e2e_ms.append(dt * 1e3)
+    e2e_s = max_over_ranks(float(np.mean(e2e_ms))) / 1e3
+    h2d = 4 * (n + 1) + 12 * nnz + 16 * n
+    d2h = 8 * n
+
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        cpu = cpu_baseline(rp, c, v, n, b_h)
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": step_ms / 1e3, "unit": "s",
+            "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": step_ms, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if mode == "plain_fp64" else "f32+f64",
+            "data": "synthetic",
+            "config": dict(workload_config(a.nx, n, nnz), mode=mode),
+            "ret": ret, "true_residual": true_res,
+            "plain_fp64_s": plain_ms / 1e3,
+            "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "ret": r_e2e},
+            "roofline": {"bound": "hbm", "kernel": kname,
+                         "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind,
+                         "traffic": traffic, "alg_bytes": alg_bytes,
+                         "launch_ms": kern[kname],
+                         "spmv_ms": kern},
+            "cpu_baseline": cpu,
+            "clocks": clk.summary(),
+            "gpu_launches": launches,
+        }
+        print(json.dumps(line), flush=True)
+    G.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def cpu_baseline(rp, c, v, n, b):
+    """One full reference solve on this host (oracle/_ref), all cores."""
+    cores = os.cpu_count() or 1
+    os.environ["OPENBLAS_NUM_THREADS"] = str(cores)
+    os.environ["OMP_NUM_THREADS"] = str(cores)
+    try:
+        from oracle import ref as R
+        if not R.available():
+            return {"value": None, "unit": "s", "cores": cores,
+                    "kind": "reference", "sample": "oracle/_ref not built"}
+        A = R.Matrix(rp, c, v, n)
+        t0 = time.perf_counter()
+        ret, outs, _ = R.call("dbicgstabl", A, b, L_DEG, TOL_TRUE, 10000, np.zeros(n))
+        dt = time.perf_counter() - t0
+        return {"value": dt, "unit": "s", "cores": cores, "kind": "reference",
+                "sample": f"one full dbicgstabl(l={L_DEG}) solve to tol "
+                          f"{TOL_TRUE} (ret {ret})"}
+    except Exception as e:  # the baseline is reported, never required
+        return {"value": None, "unit": "s", "cores": cores, "kind": "reference",
+                "sample": f"failed: {e}"}
+
+
+def main():
+    a = args_()
+    if a.impl == "reference":
+        return run_reference(a)
+    return run_ours(a)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -50,7 +50,9 @@ class Stats(C.Structure):
     """``bksp_gpu_stats`` (bksp_gpu.h)."""
     _fields_ = [("hist", _dp), ("hist_cap", C.c_int), ("hist_len", C.c_int),
                 ("ret", C.c_int), ("solve_ms", C.c_double),
-                ("total_ms", C.c_double), ("true_res", C.c_double)]
+                ("total_ms", C.c_double), ("true_res", C.c_double),
+                ("launches", C.c_longlong), ("inner_iters", C.c_int),
+                ("sweeps", C.c_int)]
 
 
 def _load():
@@ -83,6 +85,15 @@ def _load():
     L.bksp_gpu_record.argtypes = [C.POINTER(Stats)]
     L.bksp_gpu_record.restype = None
     L.bksp_gpu_version.restype = C.c_char_p
+    vp = C.c_void_p
+    L.bksp_gpu_matrix_create.argtypes = [sp, i, C.POINTER(vp)]
+    L.bksp_gpu_matrix_destroy.argtypes = [vp]
+    L.bksp_gpu_matrix_info.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    L.bksp_gpu_solve.argtypes = [vp, i, i, vp, vp, d, i, vp, C.POINTER(Stats)]
+    L.bksp_gpu_spmv.argtypes = [vp, i, vp, vp, vp]
+    L.bksp_gpu_true_residual.argtypes = [vp, vp, vp, vp]
+    L.bksp_gpu_true_residual.restype = d
+    L.bksp_gpu_device_count.restype = i
     return L
 
 
@@ -228,7 +239,8 @@ def record(hist_cap=0):
     one per iteration), ``solve_ms``, ``total_ms``.
     """
     buf = np.zeros(max(int(hist_cap), 1))
-    st = Stats(buf.ctypes.data_as(_dp), int(hist_cap), 0, 0, 0.0, 0.0, 0.0)
+    st = Stats(buf.ctypes.data_as(_dp), int(hist_cap), 0, 0, 0.0, 0.0, 0.0,
+               0, 0, 0)
     out = {}
     lib.bksp_gpu_record(C.byref(st))
     try:
@@ -245,3 +257,55 @@ def record(hist_cap=0):
 
 def version():
     return lib.bksp_gpu_version().decode()
+
+
+# ------------------------------------------------------ device-resident API
+
+MIRROR, FP32, TRANSPOSE = 1, 2, 4
+CG, CR, BICG, BICGSTAB, BICGSTABL = 1, 2, 3, 4, 5
+
+
+class GpuMatrix:
+    """``bksp_gpu_matrix``: an operator uploaded once and kept in HBM."""
+
+    def __init__(self, A, flags=0):
+        h = C.c_void_p()
+        rc = lib.bksp_gpu_matrix_create(A.ptr, int(flags), C.byref(h))
+        if rc != 0:
+            raise RuntimeError(f"bksp_gpu_matrix_create failed ({rc})")
+        self.h = h
+        n, nnz = C.c_int(), C.c_int()
+        lib.bksp_gpu_matrix_info(h, C.byref(n), C.byref(nnz))
+        self.n, self.nnz = n.value, nnz.value
+
+    def close(self):
+        if self.h:
+            lib.bksp_gpu_matrix_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def solve(self, method, b_ptr, x_ptr, tol, max_iter, l=0, stream=None,
+              hist_cap=0):
+        """Device pointers b, x (n doubles).  Returns (ret, stats dict)."""
+        buf = np.zeros(max(int(hist_cap), 1))
+        st = Stats(buf.ctypes.data_as(_dp), int(hist_cap), 0, 0, 0.0, 0.0,
+                   0.0, 0, 0, 0)
+        ret = lib.bksp_gpu_solve(self.h, method, l, b_ptr, x_ptr, tol,
+                                 max_iter, stream, C.byref(st))
+        return ret, {"ret": st.ret, "hist": buf[:min(st.hist_len, hist_cap)].copy(),
+                     "hist_len": st.hist_len, "solve_ms": st.solve_ms,
+                     "true_res": st.true_res, "launches": st.launches,
+                     "inner_iters": st.inner_iters, "sweeps": st.sweeps}
+
+    def spmv(self, x_ptr, y_ptr, fp32=False, stream=None):
+        rc = lib.bksp_gpu_spmv(self.h, int(bool(fp32)), x_ptr, y_ptr, stream)
+        if rc != 0:
+            raise RuntimeError("bksp_gpu_spmv failed")
+
+    def true_residual(self, b_ptr, x_ptr, stream=None):
+        return lib.bksp_gpu_true_residual(self.h, b_ptr, x_ptr, stream)

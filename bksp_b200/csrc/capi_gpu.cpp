@@ -1,0 +1,213 @@
+// bksp_gpu.h device-resident entry points: operator handles, solves on
+// device vectors, single SpMV launches and FP64 true residuals.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <new>
+
+#include "capi_internal.h"
+#include "solvers.h"
+
+using namespace bk;
+
+struct bksp_gpu_matrix {
+  DevCsr A;
+  DevCsr At;
+  bool has_t = false;
+  int flags = 0;
+  int device = 0;
+};
+
+namespace {
+
+cudaStream_t pick(void* stream) {
+  return stream ? static_cast<cudaStream_t>(stream) : Ctx::get().st;
+}
+
+int fail(const std::exception& e) {
+  if (std::getenv("BKSP_GPU_VERBOSE")) std::fprintf(stderr, "bksp: %s\n", e.what());
+  cudaGetLastError();
+  return INVALID_PARAMETERS;
+}
+
+}  // namespace
+
+namespace bk {
+
+// FP64 true residual ||b - A x|| / ||b|| of padded device vectors.
+double true_residual_dev(const DevCsr& A, const double* b, const double* x,
+                         cudaStream_t st) {
+  const long long np = pad64(A.n);
+  double* r = dalloc_n<double>(np, st);
+  BK_CHECK(cudaMemsetAsync(r, 0, sizeof(double) * np, st));
+  SolveState ss;
+  ss.create(0, st);
+  ss.start(0, 1, 0.0, st);
+  SpmvH<double> io = spmv_io<double>(x, r);
+  io.b = b;
+  io.mode = 1;
+  io.nd = 2;
+  io.dot[0][0] = 0; io.dot[0][1] = 0;   // (r, r)
+  io.dot[1][0] = 1; io.dot[1][1] = 1;   // (b, b)
+  spmv(A, io, ss.red(kD, E_NONE), st);
+  const double rr = ss.get_scalar(kD, st), bb = ss.get_scalar(kD + 1, st);
+  ss.release(st);
+  dfree(r, st);
+  return std::sqrt(rr) / std::sqrt(bb);
+}
+
+}  // namespace bk
+
+extern "C" {
+
+int bksp_gpu_matrix_create(dspmat* A, int flags, bksp_gpu_matrix** out) {
+  if (!out || check_matrix(A) != 0) return INVALID_PARAMETERS;
+  *out = nullptr;
+  bksp_gpu_matrix* m = new (std::nothrow) bksp_gpu_matrix();
+  if (!m) return INVALID_PARAMETERS;
+  try {
+    Ctx& cx = Ctx::get();
+    cudaStream_t st = cx.st;
+    m->flags = flags;
+    m->device = cx.device;
+    const int n = *A->row_size;
+    upload_operator(A, (flags & BKSP_GPU_MIRROR) != 0, (flags & BKSP_GPU_FP32) != 0,
+                    m->A, st);
+    if (flags & BKSP_GPU_TRANSPOSE) {
+      HostCsr t = transpose(n, A->row, A->col, A->value);
+      upload_csr(n, t.rowptr.data(), t.col.data(), t.val.data(),
+                 (flags & BKSP_GPU_FP32) != 0, m->At, st);
+      m->has_t = true;
+    }
+    BK_CHECK(cudaStreamSynchronize(st));
+    *out = m;
+    return 0;
+  } catch (const std::exception& e) {
+    delete m;
+    return fail(e);
+  }
+}
+
+int bksp_gpu_matrix_destroy(bksp_gpu_matrix* m) {
+  if (!m) return 0;
+  cudaStream_t st = Ctx::get().st;
+  m->A.release(st);
+  m->At.release(st);
+  cudaStreamSynchronize(st);
+  delete m;
+  return 0;
+}
+
+int bksp_gpu_matrix_info(const bksp_gpu_matrix* m, int* n, int* nnz) {
+  if (!m) return INVALID_PARAMETERS;
+  if (n) *n = m->A.n;
+  if (nnz) *nnz = m->A.nnz;
+  return 0;
+}
+
+int bksp_gpu_solve(bksp_gpu_matrix* m, int method, int l, const double* b,
+                   double* x, double tol, int max_iter, void* stream,
+                   bksp_gpu_stats* stats) {
+  if (!m || !b || !x) return INVALID_PARAMETERS;
+  if (method == BKSP_GPU_BICG && !m->has_t) return INVALID_PARAMETERS;
+  if (method == BKSP_GPU_BICGSTABL && (l < 1 || l > kBlMaxL)) return INVALID_PARAMETERS;
+  bksp_gpu_stats* saved = g_stats;
+  g_stats = stats;
+  int ret = INVALID_PARAMETERS;
+  try {
+    cudaStream_t st = pick(stream);
+    Timer tm(st);
+    const long long l0 = launch_count();
+    const int n = m->A.n;
+    const long long np = pad64(n);
+    double* db = dalloc_n<double>(np, st);
+    double* dx = dalloc_n<double>(np, st);
+    BK_CHECK(cudaMemsetAsync(db, 0, sizeof(double) * np, st));
+    BK_CHECK(cudaMemsetAsync(dx, 0, sizeof(double) * np, st));
+    tm.begin_solve();
+    BK_CHECK(cudaMemcpyAsync(db, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+    BK_CHECK(cudaMemcpyAsync(dx, x, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+    SolveState ss;
+    ss.create(hist_cap_for(max_iter), st);
+    SolveOut o;
+    switch (method) {
+      case BKSP_GPU_CG: o = bk::cg(m->A, db, dx, tol, max_iter, ss, st); break;
+      case BKSP_GPU_CR: o = bk::cr(m->A, db, dx, tol, max_iter, ss, st); break;
+      case BKSP_GPU_BICG: o = bk::bicg(m->A, m->At, db, dx, tol, max_iter, ss, st); break;
+      case BKSP_GPU_BICGSTAB: o = bk::bicgstab(m->A, db, dx, tol, max_iter, ss, st); break;
+      case BKSP_GPU_BICGSTABL: o = bk::bicgstabl(m->A, db, l, dx, tol, max_iter, ss, st); break;
+      default: throw CudaError("unknown method");
+    }
+    BK_CHECK(cudaMemcpyAsync(x, dx, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+    tm.end_solve();
+    BK_CHECK(cudaStreamSynchronize(st));
+    tm.report(o.ret, &ss, o.iters);
+    if (stats) {
+      stats->launches = launch_count() - l0;
+      stats->true_res = true_residual_dev(m->A, db, dx, st);
+    }
+    ss.release(st);
+    dfree(db, st);
+    dfree(dx, st);
+    BK_CHECK(cudaStreamSynchronize(st));
+    ret = o.ret;
+  } catch (const std::exception& e) {
+    ret = fail(e);
+  }
+  g_stats = saved;
+  return ret;
+}
+
+int bksp_gpu_spmv(bksp_gpu_matrix* m, int fp32, const void* x, void* y,
+                  void* stream) {
+  if (!m || !x || !y) return INVALID_PARAMETERS;
+  if (fp32 && !m->A.v32) return INVALID_PARAMETERS;
+  try {
+    cudaStream_t st = pick(stream);
+    thread_local SolveState ss;
+    thread_local bool ready = false;
+    if (!ready) {
+      ss.create(0, st);
+      ss.start(0, 1, 0.0, st);
+      ready = true;
+    }
+    if (fp32)
+      spmv(m->A, spmv_io<float>(static_cast<const float*>(x), static_cast<float*>(y)),
+           ss.red(kD, E_NONE), st);
+    else
+      spmv(m->A, spmv_io<double>(static_cast<const double*>(x), static_cast<double*>(y)),
+           ss.red(kD, E_NONE), st);
+    BK_CHECK(cudaGetLastError());
+    return 0;
+  } catch (const std::exception& e) {
+    return fail(e);
+  }
+}
+
+double bksp_gpu_true_residual(bksp_gpu_matrix* m, const double* b,
+                              const double* x, void* stream) {
+  if (!m || !b || !x) return NAN;
+  try {
+    cudaStream_t st = pick(stream);
+    const int n = m->A.n;
+    const long long np = pad64(n);
+    double* db = dalloc_n<double>(np, st);
+    double* dx = dalloc_n<double>(np, st);
+    BK_CHECK(cudaMemsetAsync(db, 0, sizeof(double) * np, st));
+    BK_CHECK(cudaMemsetAsync(dx, 0, sizeof(double) * np, st));
+    BK_CHECK(cudaMemcpyAsync(db, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+    BK_CHECK(cudaMemcpyAsync(dx, x, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));
+    const double r = true_residual_dev(m->A, db, dx, st);
+    dfree(db, st);
+    dfree(dx, st);
+    BK_CHECK(cudaStreamSynchronize(st));
+    return r;
+  } catch (const std::exception& e) {
+    fail(e);
+    return NAN;
+  }
+}
+
+}  // extern "C"

@@ -94,6 +94,9 @@ struct SpmvH {
 };
 
 // ---- launches (kernels.cu) ----
+// Kernel launches issued by this thread (graph replays are added by the
+// loop runner: captured body kernels x trips).
+long long& launch_count();
 // SpMV: VT = matrix value type, T = vector/accumulation type.
 void launch_spmv_d(const CsrH& A, const SpmvH<double>& io, const RedH& rd,
                    cudaStream_t st);
@@ -106,6 +109,12 @@ void launch_epilogue(const RedH& rd, cudaStream_t st);
 // Element-wise precision conversions / mixed-precision updates.
 void launch_convert_d2f(const double* a, float* b, long long n, cudaStream_t st);
 void launch_convert_f2d(const float* a, double* b, long long n, cudaStream_t st);
+// Solve start: reset control + ticket, optionally preset S[slot] (slot < 0:
+// none).  Scalar preset without host synchronisation.
+void launch_ctl_init(CtlH* c, unsigned* ticket, double* S, int iter0,
+                     int max_iter, double tol, double* hist, int hist_cap,
+                     short slot, double value, cudaStream_t st);
+void launch_set_scalar(double* S, short slot, double v, cudaStream_t st);
 // Graph while-loop control: keep looping while !done and trips < trip_cap.
 void launch_loop_control(CtlH* ctl, unsigned long long handle, int use_handle,
                          cudaStream_t st);

@@ -11,6 +11,11 @@
 
 namespace bk {
 
+long long& launch_count() {
+  thread_local long long n = 0;
+  return n;
+}
+
 static inline int grid_for(long long work_items) {
   long long g = (work_items + kThreads - 1) / kThreads;
   if (g < 1) g = 1;
@@ -34,10 +39,12 @@ static void spmv_dispatch(const CsrH& A, const SpmvH<XT>& io, const RedH& rd,
 
 void launch_spmv_d(const CsrH& A, const SpmvH<double>& io, const RedH& rd,
                    cudaStream_t st) {
+  ++launch_count();
   spmv_dispatch<double, double>(A, io, rd, st);
 }
 void launch_spmv_f(const CsrH& A, const SpmvH<float>& io, const RedH& rd,
                    cudaStream_t st) {
+  ++launch_count();
   spmv_dispatch<float, float>(A, io, rd, st);
 }
 
@@ -62,9 +69,11 @@ static void lc_dispatch(const LcH<T>& d, const RedH& rd, cudaStream_t st) {
 }
 
 void launch_lincomb_d(const LcH<double>& d, const RedH& rd, cudaStream_t st) {
+  ++launch_count();
   lc_dispatch<double>(d, rd, st);
 }
 void launch_lincomb_f(const LcH<float>& d, const RedH& rd, cudaStream_t st) {
+  ++launch_count();
   lc_dispatch<float>(d, rd, st);
 }
 
@@ -83,13 +92,49 @@ __global__ void k_convert_f2d(const float* __restrict__ a, double* __restrict__ 
     b[i] = (double)a[i];
 }
 void launch_convert_d2f(const double* a, float* b, long long n, cudaStream_t st) {
+  ++launch_count();
   k_convert_d2f<<<grid_for(n), kThreads, 0, st>>>(a, b, n);
 }
 void launch_convert_f2d(const float* a, double* b, long long n, cudaStream_t st) {
+  ++launch_count();
   k_convert_f2d<<<grid_for(n), kThreads, 0, st>>>(a, b, n);
 }
 
 // ------------------------------------------------------- scalar / control
+
+// Start of a solve: control block and arrival ticket reset on the device
+// (no host synchronisation), optional scalar preset.
+__global__ void k_ctl_init(Ctl* c, unsigned* ticket, double* S, int iter0,
+                           int max_iter, double tol, double* hist, int hist_cap,
+                           short slot, double value) {
+  c->done = 0;
+  c->iter = iter0;
+  c->ret = kNotConverged;
+  c->max_iter = max_iter;
+  c->hist_cap = hist_cap;
+  c->trips = 0;
+  c->trip_cap = max_iter - iter0 + 2 > 1 ? max_iter - iter0 + 2 : 1;
+  c->hist_len = 0;
+  c->tol = tol;
+  c->hist = hist;
+  ticket[0] = 0u;
+  if (slot >= 0) S[slot] = value;
+}
+
+void launch_ctl_init(CtlH* c, unsigned* ticket, double* S, int iter0,
+                     int max_iter, double tol, double* hist, int hist_cap,
+                     short slot, double value, cudaStream_t st) {
+  ++launch_count();
+  k_ctl_init<<<1, 1, 0, st>>>(c, ticket, S, iter0, max_iter, tol, hist,
+                              hist_cap, slot, value);
+}
+
+__global__ void k_set_scalar(double* S, short slot, double v) { S[slot] = v; }
+
+void launch_set_scalar(double* S, short slot, double v, cudaStream_t st) {
+  ++launch_count();
+  k_set_scalar<<<1, 1, 0, st>>>(S, slot, v);
+}
 
 __global__ void k_epilogue(Red rd) {
   if (finished(rd.ctl)) return;
@@ -97,6 +142,7 @@ __global__ void k_epilogue(Red rd) {
 }
 
 void launch_epilogue(const RedH& rd, cudaStream_t st) {
+  ++launch_count();
   k_epilogue<<<1, 1, 0, st>>>(rd);
 }
 
@@ -118,6 +164,7 @@ __global__ void k_loop_control(Ctl* c, cudaGraphConditionalHandle h,
 
 void launch_loop_control(CtlH* ctl, unsigned long long handle, int use_handle,
                          cudaStream_t st) {
+  ++launch_count();
   k_loop_control<<<1, 1, 0, st>>>(ctl, (cudaGraphConditionalHandle)handle,
                                   use_handle);
 }

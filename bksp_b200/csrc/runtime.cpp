@@ -210,17 +210,9 @@ void SolveState::release(cudaStream_t st) {
 }
 
 void SolveState::start(int iter0, int max_iter, double tol, cudaStream_t st) {
-  CtlH c;
-  std::memset(&c, 0, sizeof(c));
-  c.iter = iter0;
-  c.max_iter = max_iter;
-  c.tol = tol;
-  c.hist = hist;
-  c.hist_cap = hist_cap;
-  c.trip_cap = std::max(1, max_iter - iter0 + 2);
-  c.ret = kNotConverged;
-  BK_CHECK(cudaMemcpyAsync(ctl, &c, sizeof(c), cudaMemcpyHostToDevice, st));
-  BK_CHECK(cudaStreamSynchronize(st));
+  launch_ctl_init(ctl, ticket, S, iter0, max_iter, tol, hist, hist_cap, -1,
+                  0.0, st);
+  BK_CHECK(cudaGetLastError());
 }
 
 CtlH SolveState::read(cudaStream_t st) const {
@@ -231,9 +223,8 @@ CtlH SolveState::read(cudaStream_t st) const {
 }
 
 void SolveState::set_scalar(short slot, double v, cudaStream_t st) {
-  BK_CHECK(cudaMemcpyAsync(S + slot, &v, sizeof(double),
-                           cudaMemcpyHostToDevice, st));
-  BK_CHECK(cudaStreamSynchronize(st));
+  launch_set_scalar(S, slot, v, st);
+  BK_CHECK(cudaGetLastError());
 }
 
 double SolveState::get_scalar(short slot, cudaStream_t st) const {
@@ -272,7 +263,7 @@ void spmv(const DevCsr& A, const SpmvH<float>& io, const RedH& rd,
 
 static bool run_graph_while(SolveState& ss,
                             const std::function<void(cudaStream_t)>& body,
-                            cudaStream_t st) {
+                            cudaStream_t st, long long& body_kernels) {
   cudaGraph_t g = nullptr;
   cudaGraphExec_t ex = nullptr;
   if (cudaGraphCreate(&g, 0) != cudaSuccess) return false;
@@ -296,8 +287,11 @@ static bool run_graph_while(SolveState& ss,
                                       cudaStreamCaptureModeThreadLocal) !=
         cudaSuccess)
       break;
+    const long long c0 = launch_count();
     body(st);
     launch_loop_control(ss.ctl, (unsigned long long)h, 1, st);
+    body_kernels = launch_count() - c0;
+    launch_count() = c0;   // captured, not launched
     cudaGraph_t captured = nullptr;
     const cudaError_t ce = cudaStreamEndCapture(st, &captured);
     if (ce != cudaSuccess) {
@@ -322,13 +316,18 @@ static bool run_graph_while(SolveState& ss,
 
 CtlH run_loop(SolveState& ss, const std::function<void(cudaStream_t)>& body,
               cudaStream_t st) {
-  CtlH c = ss.read(st);
-  if (c.done) return c;
   Ctx& cx = Ctx::get();
   if (cx.use_cond_graph) {
-    if (run_graph_while(ss, body, st)) return ss.read(st);
+    long long bk_n = 0;
+    if (run_graph_while(ss, body, st, bk_n)) {
+      CtlH c = ss.read(st);
+      launch_count() += bk_n * c.trips;
+      return c;
+    }
     cx.use_cond_graph = false;   // not supported here: poll from now on
   }
+  CtlH c = ss.read(st);
+  if (c.done) return c;
   int chunk = 1;
   for (;;) {
     for (int k = 0; k < chunk; ++k) {

@@ -28,6 +28,9 @@ typedef struct {
     double solve_ms;     /* out: device time of the solve (CUDA events)     */
     double total_ms;     /* out: wall time of the call incl. transfers      */
     double true_res;     /* out: FP64 ||b - A x|| / ||b|| where computed    */
+    long long launches;  /* out: GPU kernel launches the call issued        */
+    int inner_iters;     /* out: mixed solves: inner iterations, all sweeps */
+    int sweeps;          /* out: mixed solves: refinement sweeps            */
 } bksp_gpu_stats;
 
 /* Route statistics of this thread's subsequent bksp calls into *s (NULL
@@ -48,6 +51,45 @@ int bksp_gpu_device_count(void);
  * bit-identical to the reference's dcsrgemm0 (same summation order, no
  * fused multiply-add). */
 int bksp_gpu_dcsrmv(dspmat *A, char trans, const double *x, double *y);
+
+/* ------------------------------------------------ device-resident solves */
+
+typedef struct bksp_gpu_matrix bksp_gpu_matrix;
+
+#define BKSP_GPU_MIRROR 1      /* A holds one triangle: mirror it            */
+#define BKSP_GPU_FP32 2        /* also keep FP32 values (mixed precision)    */
+#define BKSP_GPU_TRANSPOSE 4   /* also build A^T (BiCG)                      */
+
+/* Upload A (host arrays) once; the handle keeps it in GPU memory. */
+int bksp_gpu_matrix_create(dspmat *A, int flags, bksp_gpu_matrix **out);
+int bksp_gpu_matrix_destroy(bksp_gpu_matrix *A);
+int bksp_gpu_matrix_info(const bksp_gpu_matrix *A, int *n, int *nnz);
+
+enum {
+    BKSP_GPU_CG = 1,
+    BKSP_GPU_CR = 2,
+    BKSP_GPU_BICG = 3,
+    BKSP_GPU_BICGSTAB = 4,
+    BKSP_GPU_BICGSTABL = 5
+};
+
+/* The bksp.h methods on device-resident data: b and x are device pointers
+ * to n doubles (x in/out); the work is ordered on `stream` (a cudaStream_t,
+ * NULL for the library's stream) and complete when the call returns.
+ * Returns the bksp code.  stats may be NULL. */
+int bksp_gpu_solve(bksp_gpu_matrix *A, int method, int l, const double *b,
+                   double *x, double tol, int max_iter, void *stream,
+                   bksp_gpu_stats *stats);
+
+/* y = A x on the device, FP64 (fp32 = 0) or FP32 vectors and values
+ * (fp32 = 1, needs BKSP_GPU_FP32); x and y hold n elements.  Asynchronous
+ * on `stream`.  For kernel timing. */
+int bksp_gpu_spmv(bksp_gpu_matrix *A, int fp32, const void *x, void *y,
+                  void *stream);
+
+/* FP64 ||b - A x||_2 / ||b||_2 of device vectors (synchronous). */
+double bksp_gpu_true_residual(bksp_gpu_matrix *A, const double *b,
+                              const double *x, void *stream);
 
 #ifdef __cplusplus
 }
