@@ -12,14 +12,6 @@
 
 using namespace bk;
 
-struct bksp_gpu_matrix {
-  DevCsr A;
-  DevCsr At;
-  bool has_t = false;
-  int flags = 0;
-  int device = 0;
-};
-
 namespace {
 
 cudaStream_t pick(void* stream) {

@@ -9,6 +9,15 @@
 #include "../../include/bksp_gpu.h"
 #include "runtime.h"
 
+// Device-resident operator handle of bksp_gpu.h.
+struct bksp_gpu_matrix {
+  bk::DevCsr A;
+  bk::DevCsr At;
+  bool has_t = false;
+  int flags = 0;
+  int device = 0;
+};
+
 namespace bk {
 
 extern thread_local bksp_gpu_stats* g_stats;

@@ -91,6 +91,23 @@ int bksp_gpu_spmv(bksp_gpu_matrix *A, int fp32, const void *x, void *y,
 double bksp_gpu_true_residual(bksp_gpu_matrix *A, const double *b,
                               const double *x, void *stream);
 
+/* The same FP64 relative true residual, computed without allocating any
+ * memory, for callers that cannot allocate device memory where they need it
+ * (a host application whose memory pool already owns the GPU's memory;
+ * latency-critical loops that cannot take the device-wide synchronisation of
+ * cudaMalloc/cudaFree).  No counterpart in the reference.  Its scratch is a
+ * static device array of about 8 MiB that every GPU loading the library
+ * holds until exit; operators with more than 1,048,576 rows are rejected
+ * with INVALID_PARAMETERS and a message on stderr.  The first call on each
+ * device looks up that array's device address (make it before any stream
+ * capture).  All calls on a device share the array: calls whose GPU work
+ * overlaps race and must be serialised by the caller.  b, x: device
+ * pointers to n doubles; *res receives the residual; returns 0 or
+ * INVALID_PARAMETERS; synchronous on `stream` (NULL: library stream). */
+int bksp_gpu_true_residual_noalloc(bksp_gpu_matrix *A, const double *b,
+                                   const double *x, void *stream,
+                                   double *res);
+
 #ifdef __cplusplus
 }
 #endif
