@@ -238,18 +238,51 @@ def run_ours(a):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    # Headline mode (until the mixed solve lands: plain FP64 BiCGSTAB(l)).
-    mode, step = "plain_fp64", plain_step
-    for _ in range(a.warmup):
-        step()
-    barrier()
-    with Clocks(local) as clk:
-        ms, (ret, st) = timed(step, a.steps)
-    barrier()
-    step_ms = max_over_ranks(float(np.mean(ms)))
-    true_res = G.true_residual(b.data_ptr(), x.data_ptr(), sp)
-    plain_ms = step_ms
-    launches = int(st["launches"]) * a.steps
+    # Learned preconditioner: trained once on small systems of the same
+    # family (setup, outside the timed region); the MLP inference that turns
+    # the operator's rows into M runs inside every timed solve.
+    from bksp_b200 import problems as P
+    t0 = time.perf_counter()
+    model = B.SpaiModel(seed=3)
+    train_mats = [B.GpuMatrix(B.CsrMatrix(*P.convdiff3d(nt)[:3]), B.FP32)
+                  for nt in (12, 16, 24)]
+    train_loss = model.train(train_mats, epochs=200, probes=8, lr=3e-3, seed=7)
+    for m_ in train_mats:
+        m_.close()
+    train_s = time.perf_counter() - t0
+
+    def mixed_step(precond, mdl=None):
+        def f():
+            x.zero_()
+            return G.solve_mixed(b.data_ptr(), x.data_ptr(), l=L_DEG,
+                                 target=TOL_TRUE, precond=precond, model=mdl,
+                                 stream=sp)
+        return f
+
+    modes = {}
+    for name, step in (("plain_fp64", plain_step),
+                       ("mixed_none", mixed_step(B.PRECOND_NONE)),
+                       ("mixed_jacobi", mixed_step(B.PRECOND_JACOBI)),
+                       ("mixed_learned", mixed_step(B.PRECOND_LEARNED, model))):
+        for _ in range(a.warmup):
+            step()
+        barrier()
+        if name == "mixed_learned":
+            with Clocks(local) as clk:
+                ms, (ret_m, st_m) = timed(step, a.steps)
+        else:
+            ms, (ret_m, st_m) = timed(step, a.steps)
+        barrier()
+        tr = G.true_residual(b.data_ptr(), x.data_ptr(), sp)
+        modes[name] = {"s": max_over_ranks(float(np.mean(ms))) / 1e3,
+                       "ret": ret_m, "true_residual": tr,
+                       "iters": st_m.get("iters", st_m.get("hist_len")),
+                       "launches": int(st_m["launches"])}
+    mode = "mixed_learned"
+    step_ms = modes[mode]["s"] * 1e3
+    plain_ms = modes["plain_fp64"]["s"] * 1e3
+    ret, true_res = modes[mode]["ret"], modes[mode]["true_residual"]
+    launches = modes[mode]["launches"] * a.steps
 
     # Dominant kernel alone: SpMV over the same operator, FP64 and FP32.
     xs64 = torch.rand(n, dtype=torch.float64, device=dev)
@@ -298,12 +331,15 @@ def run_ours(a):
         if world > 1:
             dist.barrier()
         t0 = time.perf_counter()
-        r_e2e = B.dbicgstabl(Ap, b_p, L_DEG, TOL_TRUE, 10000, x_p)
+        r_e2e = B.dbicgstabl_mixed(Ap, b_p, x_p, l=L_DEG, target=TOL_TRUE,
+                                   precond=B.PRECOND_LEARNED, model=model)
         dt = time.perf_counter() - t0
         if i >= a.warmup:
             e2e_ms.append(dt * 1e3)
     e2e_s = max_over_ranks(float(np.mean(e2e_ms))) / 1e3
-    h2d = 4 * (n + 1) + 12 * nnz + 16 * n
+    # CSR operator (FP64 values), b, x0, and the learned preconditioner's
+    # per-row slot map (8 int32 per row) built on the host at upload.
+    h2d = 4 * (n + 1) + 12 * nnz + 16 * n + 32 * n
     d2h = 8 * n
 
     cpu = None
@@ -321,6 +357,11 @@ def run_ours(a):
             "config": dict(workload_config(a.nx, n, nnz), mode=mode),
             "ret": ret, "true_residual": true_res,
             "plain_fp64_s": plain_ms / 1e3,
+            "speedup_vs_plain_fp64": plain_ms / step_ms,
+            "modes": modes,
+            "spai_training": {"s": train_s, "final_loss": train_loss,
+                              "systems": "convdiff3d 12^3, 16^3, 24^3",
+                              "epochs": 200, "probes": 8},
             "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ret": r_e2e},
             "roofline": {"bound": "hbm", "kernel": kname,
@@ -335,6 +376,7 @@ def run_ours(a):
         }
         print(json.dumps(line), flush=True)
     G.close()
+    model.close()
     if world > 1:
         dist.destroy_process_group()
     return 0

@@ -55,6 +55,14 @@ class Stats(C.Structure):
                 ("sweeps", C.c_int)]
 
 
+class MixedOpts(C.Structure):
+    """``bksp_gpu_mixed_opts`` (bksp_gpu.h)."""
+    _fields_ = [("l", C.c_int), ("target", C.c_double), ("max_iter", C.c_int),
+                ("precond", C.c_int), ("model", C.c_void_p),
+                ("delta", C.c_double), ("period", C.c_int),
+                ("fallback", C.c_int)]
+
+
 def _load():
     if not os.path.exists(LIB_PATH):
         raise ImportError(
@@ -94,6 +102,19 @@ def _load():
     L.bksp_gpu_true_residual.argtypes = [vp, vp, vp, vp]
     L.bksp_gpu_true_residual.restype = d
     L.bksp_gpu_device_count.restype = i
+    L.bksp_gpu_solve_mixed.argtypes = [vp, vp, vp, C.POINTER(MixedOpts), vp,
+                                       C.POINTER(Stats)]
+    L.bksp_dbicgstabl_mixed.argtypes = [sp, _dp, C.POINTER(MixedOpts), _dp]
+    L.bksp_gpu_spai_create.argtypes = [C.c_uint, C.POINTER(vp)]
+    L.bksp_gpu_spai_destroy.argtypes = [vp]
+    L.bksp_gpu_spai_params.argtypes = [vp, C.POINTER(C.c_float), i]
+    L.bksp_gpu_spai_train.argtypes = [vp, C.POINTER(vp), i, i, i, C.c_float,
+                                      C.c_uint, C.POINTER(d)]
+    L.bksp_gpu_spai_loss_grad.argtypes = [vp, vp, C.POINTER(C.c_float), i,
+                                          C.c_uint, C.POINTER(d),
+                                          C.POINTER(C.c_float)]
+    L.bksp_gpu_spai_save.argtypes = [vp, C.c_char_p]
+    L.bksp_gpu_spai_load.argtypes = [C.c_char_p, C.POINTER(vp)]
     return L
 
 
@@ -289,6 +310,25 @@ class GpuMatrix:
         except Exception:
             pass
 
+    def solve_mixed(self, b_ptr, x_ptr, l=4, target=1e-8, max_iter=10000,
+                    precond=0, model=None, delta=0.0, period=0, fallback=1,
+                    stream=None, hist_cap=0):
+        """Mixed-precision BiCGSTAB(l) on device vectors; (ret, stats)."""
+        o = MixedOpts(l, target, max_iter, precond,
+                      model.h if model is not None else None, delta, period,
+                      fallback)
+        buf = np.zeros(max(int(hist_cap), 1))
+        st = Stats(buf.ctypes.data_as(_dp), int(hist_cap), 0, 0, 0.0, 0.0,
+                   0.0, 0, 0, 0)
+        ret = lib.bksp_gpu_solve_mixed(self.h, b_ptr, x_ptr, C.byref(o),
+                                       stream, C.byref(st))
+        return ret, {"ret": st.ret, "hist": buf[:min(st.hist_len, hist_cap)].copy(),
+                     "iters": st.hist_len, "solve_ms": st.solve_ms,
+                     "true_res": st.true_res, "launches": st.launches,
+                     "inner_iters": st.inner_iters,
+                     "sweeps": st.sweeps // 1000,
+                     "replacements": st.sweeps % 1000}
+
     def solve(self, method, b_ptr, x_ptr, tol, max_iter, l=0, stream=None,
               hist_cap=0):
         """Device pointers b, x (n doubles).  Returns (ret, stats dict)."""
@@ -309,3 +349,82 @@ class GpuMatrix:
 
     def true_residual(self, b_ptr, x_ptr, stream=None):
         return lib.bksp_gpu_true_residual(self.h, b_ptr, x_ptr, stream)
+
+
+PRECOND_NONE, PRECOND_JACOBI, PRECOND_LEARNED = 0, 1, 2
+
+
+class SpaiModel:
+    """``bksp_gpu_spai_model``: the learned SPAI preconditioner's MLP."""
+
+    def __init__(self, seed=0, path=None):
+        h = C.c_void_p()
+        if path is not None:
+            rc = lib.bksp_gpu_spai_load(os.fsencode(path), C.byref(h))
+        else:
+            rc = lib.bksp_gpu_spai_create(int(seed), C.byref(h))
+        if rc != 0:
+            raise RuntimeError(f"spai model creation failed ({rc})")
+        self.h = h
+        self.nparams = lib.bksp_gpu_spai_nparams()
+
+    def close(self):
+        if self.h:
+            lib.bksp_gpu_spai_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def params(self):
+        p = np.zeros(self.nparams, dtype=np.float32)
+        assert lib.bksp_gpu_spai_params(self.h, p.ctypes.data_as(C.POINTER(C.c_float)), 0) == 0
+        return p
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        assert p.size == self.nparams
+        assert lib.bksp_gpu_spai_params(self.h, p.ctypes.data_as(C.POINTER(C.c_float)), 1) == 0
+
+    def train(self, systems, epochs=20, probes=8, lr=1e-3, seed=1):
+        arr = (C.c_void_p * len(systems))(*[s.h for s in systems])
+        loss = C.c_double(0.0)
+        rc = lib.bksp_gpu_spai_train(self.h, arr, len(systems), int(epochs),
+                                     int(probes), float(lr), int(seed),
+                                     C.byref(loss))
+        if rc != 0:
+            raise RuntimeError(f"spai training failed ({rc})")
+        return loss.value
+
+    def loss_grad(self, A, Z=None, probes=8, seed=1):
+        """Loss and gradient; Z: (probes, n) float32 or None (seeded)."""
+        g = np.zeros(self.nparams, dtype=np.float32)
+        loss = C.c_double(0.0)
+        zp = None
+        if Z is not None:
+            Z = np.ascontiguousarray(Z, dtype=np.float32)
+            probes = Z.shape[0]
+            zp = Z.ctypes.data_as(C.POINTER(C.c_float))
+        rc = lib.bksp_gpu_spai_loss_grad(self.h, A.h, zp, int(probes), int(seed),
+                                         C.byref(loss),
+                                         g.ctypes.data_as(C.POINTER(C.c_float)))
+        if rc != 0:
+            raise RuntimeError(f"spai loss/grad failed ({rc})")
+        return loss.value, g
+
+    def save(self, path):
+        if lib.bksp_gpu_spai_save(self.h, os.fsencode(path)) != 0:
+            raise OSError(f"cannot write {path}")
+
+
+def dbicgstabl_mixed(A, b, x, l=4, target=1e-8, max_iter=10000, precond=0,
+                     model=None, fallback=1):
+    """Host-array mixed-precision solve (bksp_dbicgstabl_mixed)."""
+    b = _vec(b)
+    o = MixedOpts(l, target, max_iter, precond,
+                  model.h if model is not None else None, 0.0, 0, fallback)
+    return lib.bksp_dbicgstabl_mixed(A.ptr, b.ctypes.data_as(_dp), C.byref(o),
+                                     _inplace(x))

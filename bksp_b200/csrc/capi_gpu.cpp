@@ -65,8 +65,16 @@ int bksp_gpu_matrix_create(dspmat* A, int flags, bksp_gpu_matrix** out) {
     m->flags = flags;
     m->device = cx.device;
     const int n = *A->row_size;
-    upload_operator(A, (flags & BKSP_GPU_MIRROR) != 0, (flags & BKSP_GPU_FP32) != 0,
-                    m->A, st);
+    const bool f32 = (flags & BKSP_GPU_FP32) != 0;
+    if (flags & BKSP_GPU_MIRROR) {
+      HostCsr h = expand_symmetric(n, A->row, A->col, A->value);
+      upload_csr(n, h.rowptr.data(), h.col.data(), h.val.data(), f32, m->A, st);
+      if (f32) spai_build_slots(n, h.rowptr.data(), h.col.data(), m->spai, st);
+    } else {
+      upload_operator(A, false, f32, m->A, st);
+      if (f32) spai_build_slots(n, A->row, A->col, m->spai, st);
+    }
+    host_diag(A, m);
     if (flags & BKSP_GPU_TRANSPOSE) {
       HostCsr t = transpose(n, A->row, A->col, A->value);
       upload_csr(n, t.rowptr.data(), t.col.data(), t.val.data(),
@@ -87,6 +95,8 @@ int bksp_gpu_matrix_destroy(bksp_gpu_matrix* m) {
   cudaStream_t st = Ctx::get().st;
   m->A.release(st);
   m->At.release(st);
+  m->jacobi.release(st);
+  m->spai.release(st);
   cudaStreamSynchronize(st);
   delete m;
   return 0;

@@ -4,10 +4,12 @@
 #include <cuda_runtime.h>
 
 #include <chrono>
+#include <vector>
 
 #include "../../include/bksp.h"
 #include "../../include/bksp_gpu.h"
 #include "runtime.h"
+#include "spai.h"
 
 // Device-resident operator handle of bksp_gpu.h.
 struct bksp_gpu_matrix {
@@ -16,6 +18,12 @@ struct bksp_gpu_matrix {
   bool has_t = false;
   int flags = 0;
   int device = 0;
+  // Jacobi preconditioner M = diag(A)^-1 as a one-entry-per-row CSR (FP32).
+  bk::DevCsr jacobi;
+  bool has_jacobi = false;
+  bool diag_ok = false;       // every diagonal entry present and non-zero
+  std::vector<double> diag;   // host copy of diag(A)
+  bk::SpaiSlots spai;         // learned-preconditioner slot map / features
 };
 
 namespace bk {
@@ -30,6 +38,7 @@ void download_vec(double* h, const double* d, int n, long long cols,
 void upload_operator(const dspmat* A, bool expand, bool want_fp32, DevCsr& out,
                      cudaStream_t st);
 int hist_cap_for(int max_iter);
+void host_diag(const dspmat* A, bksp_gpu_matrix* m);
 
 // Device + wall timing of one call, reported into the recorded stats.
 struct Timer {

@@ -45,6 +45,14 @@ __device__ __forceinline__ bool finished(const Ctl* c) {
   return *(volatile const int*)&c->done != 0;
 }
 
+// Entry test of every kernel: the solve has finished, or the launch is
+// guarded by a scalar slot that is currently zero (conditional steps such
+// as a residual replacement inside a captured iteration).
+__device__ __forceinline__ bool skip(const Red& rd) {
+  if (finished(rd.ctl)) return true;
+  return rd.guard > 0 && *(volatile const double*)(rd.S + rd.guard) == 0.0;
+}
+
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);

@@ -168,6 +168,85 @@ static __device__ void run_epilogue(const Red& rd) {
       conv_check(rd, sqrt(D[0]) / S[kFnb]);
       if (!rd.ctl->done) bl_beta0(S, l, D[1]);
       break;
+    // ---------------- mixed-precision BiCGSTAB(l) (no reference counterpart;
+    // the BiCG / MR scalar steps are the E_BL_* cases above)
+    case E_MX_INIT: {        // r64 = b - A x0: D0 = (r, r), D1 = (b, b)
+      S[kFnb] = sqrt(D[1]);
+      const double t = sqrt(D[0]) / S[kFnb];
+      S[kMxTrue] = t;
+      S[kMxLastRep] = t;
+      S[kMxSinceRep] = 0.0;
+      S[kMxReps] = 0.0;
+      S[kMxDoRep] = 0.0;
+      if (t <= S[kMxTarget]) {
+        rd.ctl->done = 1;
+        rd.ctl->ret = rd.ctl->iter;
+      } else if (!isfinite(t)) {
+        rd.ctl->done = 1;
+        rd.ctl->ret = kDivergence;
+      }
+      break;
+    }
+    case E_MX_INIT2:         // r0 = p0 = rs = fl(r64): D0 = (rs, r0)
+      S[kBlAlpha] = 0.0;
+      S[kBlG0] = 1.0;
+      S[kBlOmega + l] = 1.0;
+      bl_beta0(S, l, D[0]);
+      break;
+    case E_MX_CHECK: {       // after the update: D0 = (r0, r0), D1 = (rs, r0)
+      Ctl* c = rd.ctl;
+      const double rec = sqrt(D[0]) / S[kFnb];
+      S[kErr] = rec;
+      if (c->hist && c->hist_len < c->hist_cap) c->hist[c->hist_len] = rec;
+      c->hist_len++;
+      if (!isfinite(rec)) {
+        c->done = 1;
+        c->ret = kDivergence;
+        break;
+      }
+      S[kMxSinceRep] += 1.0;
+      const bool rep = rec <= S[kMxTarget] ||
+                       rec < S[kMxDelta] * S[kMxLastRep] ||
+                       S[kMxSinceRep] >= S[kMxPeriod];
+      if (rep) {
+        S[kMxDoRep] = 1.0;   // the replacement block decides convergence
+      } else {
+        S[kMxDoRep] = 0.0;
+        bl_beta0(S, l, D[1]);
+        c->iter++;
+        if (c->iter >= c->max_iter) {
+          c->done = 1;
+          c->ret = kNotConverged;
+        }
+      }
+      break;
+    }
+    case E_MX_TRUE: {        // r64 = b - A x64 after accumulation: D0 = (r, r)
+      Ctl* c = rd.ctl;
+      const double t = sqrt(D[0]) / S[kFnb];
+      S[kMxTrue] = t;
+      S[kMxLastRep] = t;
+      S[kMxSinceRep] = 0.0;
+      S[kMxReps] += 1.0;
+      if (t <= S[kMxTarget]) {
+        c->done = 1;
+        c->ret = c->iter;
+      } else if (!isfinite(t)) {
+        c->done = 1;
+        c->ret = kDivergence;
+      } else {
+        c->iter++;
+        if (c->iter >= c->max_iter) {
+          c->done = 1;
+          c->ret = kNotConverged;
+        }
+      }
+      break;
+    }
+    case E_MX_REBETA:        // r0 = fl(r64) replaced: D0 = (rs, r0)
+      S[kMxDoRep] = 0.0;
+      bl_beta0(S, l, D[0]);
+      break;
     default:
       break;
   }

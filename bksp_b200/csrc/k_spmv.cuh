@@ -54,7 +54,7 @@ template <typename VT, typename XT, int ND>
 __global__ void __launch_bounds__(kThreads)
 k_spmv(CsrH A, SpmvH<XT> io, Red rd) {
   const VT* __restrict__ Aval = static_cast<const VT*>(A.val);
-  if (finished(rd.ctl)) return;
+  if (skip(rd)) return;
   __shared__ XT prod[kTileNnz + 8];
   __shared__ XT wsum[kWarps];
   double acc[ND > 0 ? ND : 1];

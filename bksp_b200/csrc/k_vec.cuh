@@ -19,7 +19,7 @@ namespace bk {
 template <typename T, int MI, int MO, int ND>
 __global__ void __launch_bounds__(kThreads)
 k_lincomb(const LcH<T> d, Red rd) {
-  if (finished(rd.ctl)) return;
+  if (skip(rd)) return;
   using PV = typename Pack<T>::V;
   constexpr int P = Pack<T>::N;
   __shared__ T cs[MO][MI];

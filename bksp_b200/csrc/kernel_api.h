@@ -49,6 +49,7 @@ struct RedH {
   double* S;
   CtlH* ctl;
   short out, epi, a0, a1;
+  short guard;   // > 0: the kernel runs only while S[guard] != 0
 };
 
 // Device CSR matrix (one value precision).
@@ -109,6 +110,13 @@ void launch_epilogue(const RedH& rd, cudaStream_t st);
 // Element-wise precision conversions / mixed-precision updates.
 void launch_convert_d2f(const double* a, float* b, long long n, cudaStream_t st);
 void launch_convert_f2d(const float* a, double* b, long long n, cudaStream_t st);
+// Mixed precision: o0 (= o1 = o2 when given) = fl32(in), with the dot
+// (w, o0) when nd = 1 (w == nullptr: (o0, o0)); and x64 += t32, y32 = 0.
+void launch_mx_d2f(const double* in, float* o0, float* o1, float* o2,
+                   const float* w, int nd, long long n, const RedH& rd,
+                   cudaStream_t st);
+void launch_mx_accum(double* x, const float* t, float* y, long long n,
+                     const RedH& rd, cudaStream_t st);
 // Solve start: reset control + ticket, optionally preset S[slot] (slot < 0:
 // none).  Scalar preset without host synchronisation.
 void launch_ctl_init(CtlH* c, unsigned* ticket, double* S, int iter0,

@@ -100,6 +100,58 @@ void launch_convert_f2d(const float* a, double* b, long long n, cudaStream_t st)
   k_convert_f2d<<<grid_for(n), kThreads, 0, st>>>(a, b, n);
 }
 
+// ------------------------------------------------- mixed-precision steps
+
+// o0 = o1 = o2 = fl32(in) (null outputs skipped); optional dot (w, o0),
+// where w == nullptr with ND = 1 means (o0, o0).
+template <int ND>
+__global__ void __launch_bounds__(kThreads)
+k_mx_d2f(const double* __restrict__ in, float* o0, float* o1, float* o2,
+         const float* w, long long n, Red rd) {
+  if (skip(rd)) return;
+  double acc[ND > 0 ? ND : 1];
+  if (ND > 0) acc[0] = 0.0;
+  for (long long i = (long long)blockIdx.x * kThreads + threadIdx.x; i < n;
+       i += (long long)gridDim.x * kThreads) {
+    const float v = (float)in[i];
+    const float wv = (ND > 0 && w) ? w[i] : v;   // read before any store
+    o0[i] = v;
+    if (o1) o1[i] = v;
+    if (o2) o2[i] = v;
+    if (ND > 0) acc[0] += (double)wv * (double)v;
+  }
+  if (ND > 0 || rd.epi) finish_reduction<ND>(acc, rd);
+}
+
+void launch_mx_d2f(const double* in, float* o0, float* o1, float* o2,
+                   const float* w, int nd, long long n, const RedH& rd,
+                   cudaStream_t st) {
+  ++launch_count();
+  const int g = grid_for(n);
+  if (nd)
+    k_mx_d2f<1><<<g, kThreads, 0, st>>>(in, o0, o1, o2, w, n, rd);
+  else
+    k_mx_d2f<0><<<g, kThreads, 0, st>>>(in, o0, o1, o2, w, n, rd);
+}
+
+// x64 += t32 (the preconditioned correction M y), then y32 = 0.
+__global__ void __launch_bounds__(kThreads)
+k_mx_accum(double* __restrict__ x, const float* __restrict__ t,
+           float* __restrict__ y, long long n, Red rd) {
+  if (skip(rd)) return;
+  for (long long i = (long long)blockIdx.x * kThreads + threadIdx.x; i < n;
+       i += (long long)gridDim.x * kThreads) {
+    x[i] += (double)t[i];
+    y[i] = 0.0f;
+  }
+}
+
+void launch_mx_accum(double* x, const float* t, float* y, long long n,
+                     const RedH& rd, cudaStream_t st) {
+  ++launch_count();
+  k_mx_accum<<<grid_for(n), kThreads, 0, st>>>(x, t, y, n, rd);
+}
+
 // ------------------------------------------------------- scalar / control
 
 // Start of a solve: control block and arrival ticket reset on the device
@@ -137,7 +189,7 @@ void launch_set_scalar(double* S, short slot, double v, cudaStream_t st) {
 }
 
 __global__ void k_epilogue(Red rd) {
-  if (finished(rd.ctl)) return;
+  if (skip(rd)) return;
   run_epilogue(rd);
 }
 

@@ -186,14 +186,15 @@ void upload_csr(int n, const int* rowptr, const int* col, const double* val,
 
 void SolveState::create(int cap, cudaStream_t st) {
   S = dalloc_n<double>(kScalars, st);
-  ctl = dalloc_n<CtlH>(1, st);
+  ctl = dalloc_n<CtlH>(2, st);
+  ctl_free = ctl + 1;
   part = dalloc_n<double>((long long)kMaxDotsApi * kGridCap, st);
   ticket = dalloc_n<unsigned>(4, st);
   hist_cap = cap;
   hist = cap > 0 ? dalloc_n<double>(cap, st) : nullptr;
   BK_CHECK(cudaMemsetAsync(S, 0, sizeof(double) * kScalars, st));
   BK_CHECK(cudaMemsetAsync(ticket, 0, sizeof(unsigned) * 4, st));
-  BK_CHECK(cudaMemsetAsync(ctl, 0, sizeof(CtlH), st));
+  BK_CHECK(cudaMemsetAsync(ctl, 0, 2 * sizeof(CtlH), st));
 }
 
 void SolveState::release(cudaStream_t st) {
@@ -204,6 +205,7 @@ void SolveState::release(cudaStream_t st) {
   dfree(hist, st);
   S = nullptr;
   ctl = nullptr;
+  ctl_free = nullptr;
   part = nullptr;
   ticket = nullptr;
   hist = nullptr;

@@ -93,12 +93,22 @@ struct SolveState {
   unsigned* ticket = nullptr;
   double* hist = nullptr;
   int hist_cap = 0;
+  CtlH* ctl_free = nullptr;   // a control block that is never finished
   void create(int hist_cap, cudaStream_t st);
   void release(cudaStream_t st);
   // Reset control: iteration index starts at iter0, budget max_iter.
   void start(int iter0, int max_iter, double tol, cudaStream_t st);
   RedH red(short out, short epi, short a0 = 0, short a1 = 0) const {
-    return RedH{part, ticket, S, ctl, out, epi, a0, a1};
+    return RedH{part, ticket, S, ctl, out, epi, a0, a1, 0};
+  }
+  // For launches after the iteration loop (not skipped by `done`).
+  RedH red_after(short out, short epi) const {
+    return RedH{part, ticket, S, ctl_free, out, epi, 0, 0, 0};
+  }
+  // Same, for a launch that runs only while S[guard] != 0.
+  RedH red_if(short guard, short out, short epi, short a0 = 0,
+              short a1 = 0) const {
+    return RedH{part, ticket, S, ctl, out, epi, a0, a1, guard};
   }
   CtlH read(cudaStream_t st) const;
   void set_scalar(short slot, double v, cudaStream_t st);

@@ -35,6 +35,19 @@ enum : short {
   kBlMaxL = 8,
 };
 
+// Mixed-precision BiCGSTAB(l) (FP32 vectors, FP64 scalars, FP64 reliable
+// residual replacement); shares the BiCGSTAB(l) slots above.
+enum : short {
+  kMxTarget = 200,    // FP64 true relative residual to reach
+  kMxDelta = 201,     // replace when rec < delta * (residual at last replacement)
+  kMxLastRep = 202,   // true residual at the last replacement
+  kMxDoRep = 203,     // guard: replacement pending in this iteration
+  kMxPeriod = 204,    // replace at least every `period` outer iterations
+  kMxSinceRep = 205,  // outer iterations since the last replacement
+  kMxTrue = 206,      // last FP64 true relative residual
+  kMxReps = 207,      // replacements performed
+};
+
 // Epilogue codes.
 enum : short {
   E_NONE = 0,
@@ -50,6 +63,8 @@ enum : short {
   // BiCGSTAB(l) (src/bicgstabl.c)
   E_BL_INIT0, E_BL_BETA0, E_BL_ALPHA, E_BL_BETA, E_BL_TAU, E_BL_SIG,
   E_BL_CHECK,
+  // mixed-precision BiCGSTAB(l)
+  E_MX_INIT, E_MX_INIT2, E_MX_CHECK, E_MX_TRUE, E_MX_REBETA,
   E_COUNT_BASE,
 };
 

@@ -25,4 +25,21 @@ SolveOut bicgstab(const DevCsr& A, const double* b, double* x, double tol,
 SolveOut bicgstabl(const DevCsr& A, const double* b, int l, double* x,
                    double tol, int max_iter, SolveState& ss, cudaStream_t st);
 
+// Mixed-precision right-preconditioned BiCGSTAB(l): FP32 matrix values and
+// Krylov vectors (A.v32 / M->v32), FP64 dot products, scalars and solution,
+// FP64 reliable residual replacement; stops on the FP64 true relative
+// residual.  M == nullptr: no preconditioner.
+struct MixedOpts {
+  double target = 1e-8;   // FP64 true relative residual to reach
+  double delta = 1e-3;    // replacement when the recursive residual fell by delta
+  int period = 6;         // ... or every `period` outer iterations
+};
+struct MixedOut : SolveOut {
+  int replacements = 0;
+  double true_res = 0.0;
+};
+MixedOut bicgstabl_mixed(const DevCsr& A, const DevCsr* M, const double* b,
+                         int l, double* x, int max_iter, const MixedOpts& o,
+                         SolveState& ss, cudaStream_t st);
+
 }  // namespace bk

@@ -1,0 +1,202 @@
+// Mixed-precision, right-preconditioned BiCGSTAB(l) -- the fast path of the
+// BiCGSTAB(l) family (no reference counterpart: the reference computes in
+// FP64 only).  The recurrences are those of src/bicgstabl.c:54-126 applied
+// to A M y = b (x = x0 + M y), with
+//   * A and M values and all Krylov vectors in FP32 (half the bytes of the
+//     FP64 path), dot products and every scalar in FP64;
+//   * reliable updates: when the recursive residual has fallen by `delta`
+//     since the last replacement, or `period` outer iterations have passed,
+//     or it is below the target, the FP32 correction is folded into the
+//     FP64 solution (x += M y, y = 0), the FP64 true residual b - A x is
+//     computed with the FP64 matrix and replaces r0 -- all inside the
+//     captured iteration, behind a device-side guard;
+//   * convergence is decided on that FP64 true residual only.
+#include <algorithm>
+
+#include "solvers.h"
+
+namespace bk {
+
+namespace {
+
+template <typename T>
+T* zeros(long long n, cudaStream_t st) {
+  T* p = dalloc_n<T>(n, st);
+  BK_CHECK(cudaMemsetAsync(p, 0, sizeof(T) * (size_t)n, st));
+  return p;
+}
+
+constexpr int Y = 0, B = 1, W0 = 2;
+constexpr int OUT = Lc<float>::OUT;
+
+template <typename T>
+void set_dot(SpmvH<T>& io, int k, int a, int b) {
+  io.dot[k][0] = (unsigned char)a;
+  io.dot[k][1] = (unsigned char)b;
+  io.nd = std::max(io.nd, k + 1);
+}
+
+}  // namespace
+
+MixedOut bicgstabl_mixed(const DevCsr& A, const DevCsr* M, const double* b,
+                         int l, double* x, int max_iter, const MixedOpts& o,
+                         SolveState& ss, cudaStream_t st) {
+  if (l < 1 || l > kBlMaxL) throw CudaError("bicgstabl: l out of range");
+  if (!A.v32 || (M && !M->v32)) throw CudaError("mixed solve: FP32 values missing");
+  MixedOut out;
+  const long long np = pad64(A.n);
+  float* w = zeros<float>((2 * (l + 1) + 3) * np, st);
+  auto R = [&](int i) { return w + i * np; };
+  auto P = [&](int i) { return w + (l + 1 + i) * np; };
+  float* rs = w + 2 * (l + 1) * np;
+  float* y = rs + np;
+  float* t = y + np;
+  double* r64 = zeros<double>(np, st);
+
+  ss.start(0, max_iter, 0.0, st);
+  ss.set_scalar(kL, (double)l, st);
+  ss.set_scalar(kMxTarget, o.target, st);
+  ss.set_scalar(kMxDelta, o.delta, st);
+  ss.set_scalar(kMxPeriod, (double)std::max(1, o.period), st);
+
+  // r64 = b - A x0 (FP64), ||b||; r0 = p0 = rs = fl32(r64), (rs, r0).
+  {
+    SpmvH<double> io = spmv_io<double>(x, r64);
+    io.b = b;
+    io.mode = 1;
+    set_dot(io, 0, Y, Y);
+    set_dot(io, 1, B, B);
+    spmv(A, io, ss.red(kD, E_MX_INIT), st);
+    launch_mx_d2f(r64, R(0), P(0), rs, nullptr, 1, np, ss.red(kD, E_MX_INIT2), st);
+  }
+
+  // v -> A M v (FP32), optional dot (rs, A M v) into the epilogue `epi`.
+  auto op = [&](const float* v, float* dst, bool dot, short epi, cudaStream_t s) {
+    const float* src = v;
+    if (M) {
+      spmv(*M, spmv_io<float>(v, t), ss.red(kD, E_NONE), s);
+      src = t;
+    }
+    SpmvH<float> io = spmv_io<float>(src, dst);
+    if (dot) {
+      io.w0 = rs;
+      set_dot(io, 0, W0, Y);
+    }
+    spmv(A, io, ss.red(kD, epi), s);
+  };
+
+  auto body = [&](cudaStream_t s) {
+    for (int j = 0; j < l; ++j) {
+      {  // p_i = beta p_i + r_i
+        Lc<float> u(np);
+        const int ip = u.in(P(0), true), ir = u.in(R(0), true);
+        const int op_ = u.out(P(0), true);
+        u.term(op_, ip, cf_slot(kBlBeta)).term(op_, ir, cf_const(1));
+        u.batch(j + 1, np);
+        u.launch(ss.red(kD, E_NONE), s);
+      }
+      op(P(j), P(j + 1), true, E_BL_ALPHA, s);
+      {  // r_i -= alpha p_{i+1}; y += alpha p_0
+        Lc<float> u(np);
+        const int ir = u.in(R(0), true), ip = u.in(P(1), true);
+        const int orr = u.out(R(0), true);
+        u.term(orr, ir, cf_const(1)).term(orr, ip, cf_slot(kBlAlpha, -1));
+        u.batch(j + 1, np);
+        u.launch(ss.red(kD, E_NONE), s);
+        Lc<float> v(np);
+        const int iy = v.in(y), i0 = v.in(P(0));
+        const int oy = v.out(y);
+        v.term(oy, iy, cf_const(1)).term(oy, i0, cf_slot(kBlAlpha));
+        v.launch(ss.red(kD, E_NONE), s);
+      }
+      op(R(j), R(j + 1), j + 1 < l, j + 1 < l ? E_BL_BETA : E_NONE, s);
+    }
+    // MR part (modified Gram-Schmidt), FP64 dots of FP32 vectors.
+    for (int j = 1; j <= l; ++j) {
+      if (j == 1) {
+        Lc<float> u(np);
+        const int i1 = u.in(R(1)), i0 = u.in(R(0));
+        u.dot(i1, i1).dot(i0, i1);
+        u.launch(ss.red(kD, E_BL_SIG, 0, 1), s);
+        continue;
+      }
+      {
+        Lc<float> u(np);
+        const int ij = u.in(R(j)), i1 = u.in(R(1));
+        u.dot(ij, i1);
+        u.launch(ss.red(kD, E_BL_TAU, 1, (short)j), s);
+      }
+      for (int i = 1; i < j; ++i) {
+        Lc<float> u(np);
+        const int ij = u.in(R(j)), ii = u.in(R(i));
+        const int oj = u.out(R(j));
+        u.term(oj, ij, cf_const(1))
+            .term(oj, ii, cf_slot((short)(kBlTau + i * l + j), -1));
+        if (i + 1 < j) {
+          const int in = u.in(R(i + 1));
+          u.dot(OUT + oj, in);
+          u.launch(ss.red(kD, E_BL_TAU, (short)(i + 1), (short)j), s);
+        } else {
+          const int i0 = u.in(R(0));
+          u.dot(OUT + oj, OUT + oj).dot(i0, OUT + oj);
+          u.launch(ss.red(kD, E_BL_SIG, 0, (short)j), s);
+        }
+      }
+    }
+    {  // update y, r0, p0; recursive residual test / replacement trigger
+      Lc<float> u(np);
+      const int iy = u.in(y);
+      int ir[kBlMaxL + 1], ip[kBlMaxL + 1];
+      for (int i = 0; i <= l; ++i) ir[i] = u.in(R(i));
+      for (int i = 0; i <= l; ++i) ip[i] = u.in(P(i));
+      const int irs = u.in(rs);
+      const int oy = u.out(y), orr = u.out(R(0)), op_ = u.out(P(0));
+      u.term(oy, iy, cf_const(1)).term(oy, ir[0], cf_slot(kBlOmega + 1));
+      u.term(orr, ir[0], cf_const(1))
+          .term(orr, ir[l], cf_slot((short)(kBlOmegaD + l), -1));
+      u.term(op_, ip[0], cf_const(1))
+          .term(op_, ip[l], cf_slot((short)(kBlOmega + l), -1));
+      for (int i = 1; i < l; ++i) {
+        u.term(op_, ip[i], cf_slot((short)(kBlOmega + i), -1));
+        u.term(orr, ir[i], cf_slot((short)(kBlOmegaD + i), -1));
+        u.term(oy, ir[i], cf_slot((short)(kBlOmegaDD + i)));
+      }
+      u.dot(OUT + orr, OUT + orr).dot(irs, OUT + orr);
+      u.launch(ss.red(kD, E_MX_CHECK), s);
+    }
+    // Reliable update, guarded by S[kMxDoRep].
+    const float* corr = y;
+    if (M) {
+      spmv(*M, spmv_io<float>(y, t), ss.red_if(kMxDoRep, kD, E_NONE), s);
+      corr = t;
+    }
+    launch_mx_accum(x, corr, y, np, ss.red_if(kMxDoRep, kD, E_NONE), s);
+    {
+      SpmvH<double> io = spmv_io<double>(x, r64);
+      io.b = b;
+      io.mode = 1;
+      set_dot(io, 0, Y, Y);
+      spmv(A, io, ss.red_if(kMxDoRep, kD, E_MX_TRUE), s);
+    }
+    launch_mx_d2f(r64, R(0), nullptr, nullptr, rs, 1, np,
+                  ss.red_if(kMxDoRep, kD, E_MX_REBETA), s);
+  };
+  const CtlH c = run_loop(ss, body, st);
+  // Fold any correction not yet accumulated (budget exhausted / breakdown).
+  const float* corr = y;
+  if (M) {
+    spmv(*M, spmv_io<float>(y, t), ss.red_after(kD, E_NONE), st);
+    corr = t;
+  }
+  launch_mx_accum(x, corr, y, np, ss.red_after(kD, E_NONE), st);
+  BK_CHECK(cudaGetLastError());
+  out.ret = c.ret;
+  out.iters = c.hist_len;
+  out.replacements = (int)ss.get_scalar(kMxReps, st);
+  out.true_res = ss.get_scalar(kMxTrue, st);
+  dfree(w, st);
+  dfree(r64, st);
+  return out;
+}
+
+}  // namespace bk

@@ -1,0 +1,43 @@
+// Learned SPAI preconditioner (host side): model handle, per-operator slot
+// map and features, inference into M values on A's pattern, training.
+#pragma once
+
+#include <vector>
+
+#include "runtime.h"
+#include "spai_api.h"
+
+struct bksp_gpu_matrix;
+
+struct bksp_gpu_spai_model {
+  float* w = nullptr;      // kSpaiParams parameters (device)
+  float* am = nullptr;     // Adam first moments
+  float* av = nullptr;     // Adam second moments
+  float* grad = nullptr;   // last gradient
+  double* loss = nullptr;  // last loss (device scalar)
+  int step = 0;
+  int device = 0;
+};
+
+namespace bk {
+
+// Per-operator data of the learned preconditioner, owned by the matrix
+// handle: slot of every row entry (near-to-far diagonal order), features.
+struct SpaiSlots {
+  bool ok = false;           // the operator has <= 3 negative and <= 4
+                             // positive diagonal offsets, incl. the diagonal
+  int* slot_entry = nullptr; // n x kSlots CSR indices (-1: absent), device
+  float* feat = nullptr;     // n x kSlots features, device (lazy)
+  float* dinv = nullptr;     // n, device (lazy)
+  void release(cudaStream_t st);
+};
+
+// Host analysis of the uploaded CSR (rows as on the device).
+void spai_build_slots(int n, const int* rowptr, const int* col, SpaiSlots& s,
+                      cudaStream_t st);
+// M (FP32 values in mvals, nnz + 8 floats) on A's pattern from the model;
+// returns a CSR view sharing A's index arrays.
+DevCsr spai_apply(bksp_gpu_spai_model* model, bksp_gpu_matrix* m,
+                  float* mvals, cudaStream_t st);
+
+}  // namespace bk

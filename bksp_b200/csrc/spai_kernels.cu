@@ -1,0 +1,366 @@
+// Learned sparse-approximate-inverse preconditioner: kernels of the per-row
+// MLP (no reference counterpart; bksp has no preconditioners).
+//
+// A row i of a stencil-like matrix is described by its entries on up to
+// kSlots diagonals ("slots", ordered near-to-far: slot 3 is the diagonal,
+// slots 2,1,0 the negative offsets nearest first, slots 4..7 the positive
+// ones).  Features f_i[s] = a_{i,j_s} / a_ii (slot 3: the row sum / a_ii).
+// The MLP  f -> relu(W1 f + b1) -> relu(W2 h1 + b2) -> W3 h2 + b3 = o
+// predicts the SPAI row on A's pattern: m_{i,j_s} = o_s / a_ii.
+//
+// Training minimises  L = sum_i ||(Z - M W)_i||^2 / (rows * probes)  with
+// W = A Z for random probe blocks Z, i.e. ||(I - M A) Z||_F^2 scaled; the
+// loss decomposes by rows of M, so each thread owns one row end to end
+// (forward, residual, backward) and a CTA reduces its rows' weight
+// gradients through shared memory into per-CTA partials, which the Adam
+// kernel sums in a fixed order (deterministic).
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "spai_api.h"
+
+namespace bk {
+
+namespace {
+
+constexpr int S = kSlots;   // 8
+constexpr int H = kHidden;  // 64
+
+// Parameter layout (floats): W1[H][S], b1[H], W2[H][H], b2[H], W3[S][H], b3[S].
+constexpr int oW1 = 0, ob1 = oW1 + H * S, oW2 = ob1 + H, ob2 = oW2 + H * H,
+              oW3 = ob2 + H, ob3 = oW3 + S * H, kP = ob3 + S;
+static_assert(kP == kSpaiParams, "parameter count");
+
+__device__ __forceinline__ void load_params(float* sw, const float* w) {
+  for (int p = threadIdx.x; p < kP; p += blockDim.x) sw[p] = w[p];
+}
+
+// Forward pass of one row; returns o[S], keeps h1, h2.
+__device__ __forceinline__ void forward(const float* sw, const float (&f)[S],
+                                        float (&h1)[H], float (&h2)[H],
+                                        float (&o)[S]) {
+#pragma unroll
+  for (int a = 0; a < H; ++a) {
+    float z = sw[ob1 + a];
+#pragma unroll
+    for (int s = 0; s < S; ++s) z = fmaf(sw[oW1 + a * S + s], f[s], z);
+    h1[a] = fmaxf(z, 0.0f);
+  }
+#pragma unroll
+  for (int a = 0; a < H; ++a) {
+    float z = sw[ob2 + a];
+#pragma unroll
+    for (int b = 0; b < H; ++b) z = fmaf(sw[oW2 + a * H + b], h1[b], z);
+    h2[a] = fmaxf(z, 0.0f);
+  }
+#pragma unroll
+  for (int s = 0; s < S; ++s) {
+    float z = sw[ob3 + s];
+#pragma unroll
+    for (int b = 0; b < H; ++b) z = fmaf(sw[oW3 + s * H + b], h2[b], z);
+    o[s] = z;
+  }
+}
+
+// Forward pass writing the activations to a per-row stage `my` (f at 0,
+// h1 at S, h2 at S + H): bounded register use for the training kernel.
+__device__ __forceinline__ void forward_staged(const float* sw,
+                                               const float (&f)[S], float* my,
+                                               float (&o)[S]) {
+  float h1[H];
+#pragma unroll
+  for (int a = 0; a < H; ++a) {
+    float z = sw[ob1 + a];
+#pragma unroll
+    for (int s = 0; s < S; ++s) z = fmaf(sw[oW1 + a * S + s], f[s], z);
+    h1[a] = fmaxf(z, 0.0f);
+    my[S + a] = h1[a];
+  }
+#pragma unroll 1
+  for (int a = 0; a < H; ++a) {
+    float z = sw[ob2 + a];
+#pragma unroll
+    for (int b = 0; b < H; ++b) z = fmaf(sw[oW2 + a * H + b], h1[b], z);
+    my[S + H + a] = fmaxf(z, 0.0f);
+  }
+#pragma unroll
+  for (int s = 0; s < S; ++s) o[s] = sw[ob3 + s];
+#pragma unroll 4
+  for (int b = 0; b < H; ++b) {
+    const float hb = my[S + H + b];
+#pragma unroll
+    for (int s = 0; s < S; ++s) o[s] = fmaf(sw[oW3 + s * H + b], hb, o[s]);
+  }
+}
+
+}  // namespace
+
+// Features and 1/a_ii of every row.  slot_entry[i*S + s]: CSR index of the
+// row's entry on slot s, or -1.
+__global__ void k_spai_features(int n, const int* __restrict__ rowptr,
+                                const double* __restrict__ val,
+                                const int* __restrict__ slot_entry,
+                                float* __restrict__ feat,
+                                float* __restrict__ dinv) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int ed = slot_entry[i * S + kCenterSlot];
+  const double d = ed >= 0 ? val[ed] : 0.0;
+  const double di = d != 0.0 ? 1.0 / d : 0.0;
+  double rowsum = 0.0;
+  for (int k = rowptr[i]; k < rowptr[i + 1]; ++k) rowsum += val[k];
+#pragma unroll
+  for (int s = 0; s < S; ++s) {
+    const int e = slot_entry[i * S + s];
+    float v = 0.0f;
+    if (s == kCenterSlot) v = (float)(rowsum * di);
+    else if (e >= 0) v = (float)(val[e] * di);
+    feat[i * S + s] = v;
+  }
+  dinv[i] = (float)di;
+}
+
+// Inference: M values on A's pattern (entries without a slot get 0).
+__global__ void __launch_bounds__(256)
+k_spai_infer(int n, const float* __restrict__ w, const float* __restrict__ feat,
+             const float* __restrict__ dinv, const int* __restrict__ slot_entry,
+             float* __restrict__ mval) {
+  __shared__ float sw[kP];
+  load_params(sw, w);
+  __syncthreads();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float f[S], h1[H], h2[H], o[S];
+#pragma unroll
+  for (int s = 0; s < S; ++s) f[s] = feat[i * S + s];
+  forward(sw, f, h1, h2, o);
+  const float di = dinv[i];
+#pragma unroll
+  for (int s = 0; s < S; ++s) {
+    const int e = slot_entry[i * S + s];
+    if (e >= 0) mval[e] = o[s] * di;
+  }
+}
+
+// One training pass over rows [0, n): loss partial and weight-gradient
+// partials per CTA.  Z and AZ are column-major probe blocks (probes x ldz).
+// `col` maps a slot's CSR entry to its column.
+constexpr int kTrainThreads = 128;
+// Per-row stage: f, h1, h2, dh1, dh2, do; odd stride (273 floats) so each
+// thread's own row is bank-conflict free.
+constexpr int kStage = S + H + H + H + H + S + 1;
+
+__global__ void __launch_bounds__(kTrainThreads)
+k_spai_grad(int n, const float* __restrict__ w, const float* __restrict__ feat,
+            const float* __restrict__ dinv, const int* __restrict__ slot_entry,
+            const int* __restrict__ col, const float* __restrict__ Z,
+            const float* __restrict__ AZ, int probes, long long ldz,
+            float scale, float* __restrict__ gpart, float* __restrict__ lpart) {
+  extern __shared__ float smem[];
+  float* sw = smem;                      // kP
+  float* st = smem + kP;                 // kTrainThreads x kStage
+  load_params(sw, w);
+  __syncthreads();
+  const int t = threadIdx.x;
+  const int i = blockIdx.x * kTrainThreads + t;
+  float* my = st + t * kStage;
+  float loss = 0.0f;
+  if (i < n) {
+    float o[S];
+    {
+      // Activations go to the stage (also needed by the CTA reduction
+      // below); the backward pass reads them back.
+      float f[S];
+#pragma unroll
+      for (int s = 0; s < S; ++s) {
+        f[s] = feat[i * S + s];
+        my[s] = f[s];
+      }
+      forward_staged(sw, f, my, o);
+    }
+    const float di = dinv[i];
+    int cj[S];
+    float m[S];
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+      const int e = slot_entry[i * S + s];
+      cj[s] = e >= 0 ? col[e] : -1;
+      m[s] = e >= 0 ? o[s] * di : 0.0f;
+    }
+    float dm[S];
+#pragma unroll
+    for (int s = 0; s < S; ++s) dm[s] = 0.0f;
+    for (int c = 0; c < probes; ++c) {
+      const float* azc = AZ + (long long)c * ldz;
+      float r = Z[(long long)c * ldz + i];
+      float wv[S];
+#pragma unroll
+      for (int s = 0; s < S; ++s) {
+        wv[s] = cj[s] >= 0 ? azc[cj[s]] : 0.0f;
+        r = fmaf(-m[s], wv[s], r);
+      }
+      loss = fmaf(r, r, loss);
+#pragma unroll
+      for (int s = 0; s < S; ++s) dm[s] = fmaf(-2.0f * r, wv[s], dm[s]);
+    }
+    float dout[S];
+#pragma unroll
+    for (int s = 0; s < S; ++s) dout[s] = cj[s] >= 0 ? dm[s] * di * scale : 0.0f;
+    float dh2[H];
+#pragma unroll
+    for (int b = 0; b < H; ++b) {
+      float z = 0.0f;
+#pragma unroll
+      for (int s = 0; s < S; ++s) z = fmaf(sw[oW3 + s * H + b], dout[s], z);
+      dh2[b] = my[S + H + b] > 0.0f ? z : 0.0f;
+      my[S + 3 * H + b] = dh2[b];
+    }
+#pragma unroll 1
+    for (int b = 0; b < H; ++b) {
+      float z = 0.0f;
+#pragma unroll
+      for (int a = 0; a < H; ++a) z = fmaf(sw[oW2 + a * H + b], dh2[a], z);
+      my[S + 2 * H + b] = my[S + b] > 0.0f ? z : 0.0f;
+    }
+#pragma unroll
+    for (int s = 0; s < S; ++s) my[S + 4 * H + s] = dout[s];
+  } else {
+    for (int q = 0; q < kStage; ++q) my[q] = 0.0f;
+  }
+  __syncthreads();
+  // CTA reduction of the outer products into this CTA's gradient partial.
+  const int rows = kTrainThreads;
+  for (int p = t; p < kP; p += kTrainThreads) {
+    float g = 0.0f;
+    if (p < ob1) {                       // W1[a][s] += dh1[a] f[s]
+      const int a = p / S, s = p % S;
+      for (int r = 0; r < rows; ++r)
+        g = fmaf(st[r * kStage + S + 2 * H + a], st[r * kStage + s], g);
+    } else if (p < oW2) {                // b1[a] += dh1[a]
+      const int a = p - ob1;
+      for (int r = 0; r < rows; ++r) g += st[r * kStage + S + 2 * H + a];
+    } else if (p < ob2) {                // W2[a][b] += dh2[a] h1[b]
+      const int a = (p - oW2) / H, b = (p - oW2) % H;
+      for (int r = 0; r < rows; ++r)
+        g = fmaf(st[r * kStage + S + 3 * H + a], st[r * kStage + S + b], g);
+    } else if (p < oW3) {                // b2[a] += dh2[a]
+      const int a = p - ob2;
+      for (int r = 0; r < rows; ++r) g += st[r * kStage + S + 3 * H + a];
+    } else if (p < ob3) {                // W3[s][b] += do[s] h2[b]
+      const int s = (p - oW3) / H, b = (p - oW3) % H;
+      for (int r = 0; r < rows; ++r)
+        g = fmaf(st[r * kStage + S + 4 * H + s], st[r * kStage + S + H + b], g);
+    } else {                             // b3[s] += do[s]
+      const int s = p - ob3;
+      for (int r = 0; r < rows; ++r) g += st[r * kStage + S + 4 * H + s];
+    }
+    gpart[(long long)blockIdx.x * kP + p] = g;
+  }
+  // Loss partial (fixed-order block tree).
+  __shared__ float lw[kTrainThreads / 32];
+  float v = loss;
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  if ((t & 31) == 0) lw[t >> 5] = v;
+  __syncthreads();
+  if (t == 0) {
+    float s = 0.0f;
+    for (int k = 0; k < kTrainThreads / 32; ++k) s += lw[k];
+    lpart[blockIdx.x] = s;
+  }
+}
+
+// Sum the per-CTA partials (fixed order) into grad[] and loss; optionally
+// apply one Adam step (step >= 1).
+__global__ void k_spai_reduce_adam(int nblk, const float* __restrict__ gpart,
+                                   const float* __restrict__ lpart,
+                                   float* __restrict__ grad, double* loss,
+                                   float loss_scale, float* w, float* am,
+                                   float* av, int step, float lr) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p == 0) {
+    double l = 0.0;
+    for (int b = 0; b < nblk; ++b) l += (double)lpart[b];
+    *loss = l * (double)loss_scale;
+  }
+  if (p >= kP) return;
+  float g = 0.0f;
+  for (int b = 0; b < nblk; ++b) g += gpart[(long long)b * kP + p];
+  grad[p] = g;
+  if (step <= 0) return;
+  const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+  const float m = b1 * am[p] + (1.0f - b1) * g;
+  const float v = b2 * av[p] + (1.0f - b2) * g * g;
+  am[p] = m;
+  av[p] = v;
+  const float mh = m / (1.0f - powf(b1, (float)step));
+  const float vh = v / (1.0f - powf(b2, (float)step));
+  w[p] -= lr * mh / (sqrtf(vh) + eps);
+}
+
+// Rademacher probes: Z[c][i] = +-1 from a counter hash (seeded).
+__global__ void k_spai_probes(int n, int probes, long long ldz, uint32_t seed,
+                              float* __restrict__ Z) {
+  const long long total = (long long)probes * ldz;
+  for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < total;
+       q += (long long)gridDim.x * blockDim.x) {
+    const long long i = q % ldz;
+    uint32_t h = (uint32_t)q * 2654435761u ^ seed;
+    h ^= h >> 16; h *= 0x7feb352du; h ^= h >> 15; h *= 0x846ca68bu; h ^= h >> 16;
+    Z[q] = i < n ? ((h & 1u) ? 1.0f : -1.0f) : 0.0f;
+  }
+}
+
+// ---------------------------------------------------------------- launches
+
+void launch_spai_features(int n, const int* rowptr, const double* val,
+                          const int* slot_entry, float* feat, float* dinv,
+                          cudaStream_t st) {
+  ++launch_count();
+  k_spai_features<<<(n + 255) / 256, 256, 0, st>>>(n, rowptr, val, slot_entry,
+                                                  feat, dinv);
+}
+
+void launch_spai_infer(int n, const float* w, const float* feat,
+                       const float* dinv, const int* slot_entry, float* mval,
+                       cudaStream_t st) {
+  ++launch_count();
+  k_spai_infer<<<(n + 255) / 256, 256, 0, st>>>(n, w, feat, dinv, slot_entry,
+                                               mval);
+}
+
+int spai_grad_blocks(int n) { return (n + kTrainThreads - 1) / kTrainThreads; }
+
+void launch_spai_grad(int n, const float* w, const float* feat,
+                      const float* dinv, const int* slot_entry, const int* col,
+                      const float* Z, const float* AZ, int probes,
+                      long long ldz, float scale, float* gpart, float* lpart,
+                      cudaStream_t st) {
+  ++launch_count();
+  const size_t sm = sizeof(float) * (kP + kTrainThreads * kStage);
+  static bool attr = false;
+  if (!attr) {
+    cudaFuncSetAttribute(k_spai_grad, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sm);
+    attr = true;
+  }
+  k_spai_grad<<<spai_grad_blocks(n), kTrainThreads, sm, st>>>(
+      n, w, feat, dinv, slot_entry, col, Z, AZ, probes, ldz, scale, gpart, lpart);
+}
+
+void launch_spai_reduce_adam(int nblk, const float* gpart, const float* lpart,
+                             float* grad, double* loss, float loss_scale,
+                             float* w, float* am, float* av, int step, float lr,
+                             cudaStream_t st) {
+  ++launch_count();
+  k_spai_reduce_adam<<<(kP + 255) / 256, 256, 0, st>>>(
+      nblk, gpart, lpart, grad, loss, loss_scale, w, am, av, step, lr);
+}
+
+void launch_spai_probes(int n, int probes, long long ldz, uint32_t seed,
+                        float* Z, cudaStream_t st) {
+  ++launch_count();
+  k_spai_probes<<<148 * 4, 256, 0, st>>>(n, probes, ldz, seed, Z);
+}
+
+}  // namespace bk

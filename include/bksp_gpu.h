@@ -91,6 +91,70 @@ int bksp_gpu_spmv(bksp_gpu_matrix *A, int fp32, const void *x, void *y,
 double bksp_gpu_true_residual(bksp_gpu_matrix *A, const double *b,
                               const double *x, void *stream);
 
+/* ------------------------------------- mixed precision, preconditioners */
+
+#define BKSP_GPU_PRECOND_NONE 0      /* unpreconditioned                     */
+#define BKSP_GPU_PRECOND_JACOBI 1    /* M = diag(A)^-1                       */
+#define BKSP_GPU_PRECOND_LEARNED 2   /* M = MLP-predicted SPAI on A's pattern */
+
+/* A trained per-row MLP predicting sparse-approximate-inverse values. */
+typedef struct bksp_gpu_spai_model bksp_gpu_spai_model;
+
+typedef struct {
+    int l;                      /* BiCGSTAB(l) degree (1..8)                 */
+    double target;              /* FP64 true relative residual to reach      */
+    int max_iter;               /* outer-iteration budget                    */
+    int precond;                /* BKSP_GPU_PRECOND_*                        */
+    bksp_gpu_spai_model *model; /* for BKSP_GPU_PRECOND_LEARNED              */
+    double delta;               /* replacement trigger (0: 1e-3)             */
+    int period;                 /* replacement period, outer its (0: 6)      */
+    int fallback;               /* 1: retry with Jacobi when the learned
+                                   preconditioner stagnates or breaks down   */
+} bksp_gpu_mixed_opts;
+
+/* The learned preconditioner: a per-row MLP (8 -> 64 -> 64 -> 8, FP32)
+ * maps a row's normalised stencil (its entries on up to 8 diagonals, a_ij /
+ * a_ii) to the sparse-approximate-inverse values of that row on A's
+ * pattern.  Trained on the GPU by minimising ||(I - M A) Z||_F^2 over random
+ * probe blocks Z.  An untrained model is Jacobi.  Operators qualify when
+ * created with BKSP_GPU_FP32 and having the diagonal plus at most 3 lower
+ * and 4 upper diagonals in use (stencil matrices). */
+int bksp_gpu_spai_create(unsigned seed, bksp_gpu_spai_model **out);
+int bksp_gpu_spai_destroy(bksp_gpu_spai_model *model);
+int bksp_gpu_spai_nparams(void);
+/* Copy the parameters out (set = 0) or in (set = 1); nparams floats. */
+int bksp_gpu_spai_params(bksp_gpu_spai_model *model, float *host, int set);
+/* Adam training over the rows of nsys operators, `probes` Rademacher probe
+ * vectors per operator and epoch; *loss_out gets the last epoch's mean
+ * loss. */
+int bksp_gpu_spai_train(bksp_gpu_spai_model *model,
+                        bksp_gpu_matrix *const *systems, int nsys, int epochs,
+                        int probes, float lr, unsigned seed, double *loss_out);
+/* Loss and gradient for a given probe block (probes x n column-major host
+ * floats, or NULL for seeded Rademacher probes); operators of at most
+ * 65,536 rows.  grad: nparams floats or NULL. */
+int bksp_gpu_spai_loss_grad(bksp_gpu_spai_model *model, bksp_gpu_matrix *A,
+                            const float *Z, int probes, unsigned seed,
+                            double *loss, float *grad);
+/* Checkpoint file: a one-line JSON header then little-endian FP32 params. */
+int bksp_gpu_spai_save(bksp_gpu_spai_model *model, const char *path);
+int bksp_gpu_spai_load(const char *path, bksp_gpu_spai_model **out);
+
+/* Right-preconditioned BiCGSTAB(l) in mixed precision: FP32 matrix values
+ * and Krylov vectors, FP64 dot products, scalars and solution, FP64
+ * residual replacement, stopping on the FP64 true relative residual
+ * ||b - A x|| / ||b|| <= target.  The matrix needs BKSP_GPU_FP32.  Device
+ * vectors b, x (x in/out).  Returns the index of the converging outer
+ * iteration, NOT_CONVERGED, DIVERGENCE or INVALID_PARAMETERS. */
+int bksp_gpu_solve_mixed(bksp_gpu_matrix *A, const double *b, double *x,
+                         const bksp_gpu_mixed_opts *opts, void *stream,
+                         bksp_gpu_stats *stats);
+
+/* The same with host arrays in the bksp.h style: uploads A, b, x, solves,
+ * downloads x. */
+int bksp_dbicgstabl_mixed(dspmat *A, double *b, const bksp_gpu_mixed_opts *opts,
+                          double *x);
+
 /* The same FP64 relative true residual, computed without allocating any
  * memory, for callers that cannot allocate device memory where they need it
  * (a host application whose memory pool already owns the GPU's memory;

@@ -1,0 +1,145 @@
+"""GPU tests of the mixed-precision solve and the learned SPAI
+preconditioner: FP64 target reached and checked on the host, error against
+an FP64 oracle solve, the MLP gradient against the NumPy oracle, what the
+trained network gains over the unpreconditioned and Jacobi solves, the
+stagnation fallback and checkpoint files."""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+from bksp_b200 import problems as P
+from oracle import mlp
+from oracle import solvers as S
+
+pytestmark = pytest.mark.gpu
+
+
+def _system(gen, nx, seed=1):
+    rp, c, v, n = gen(nx)
+    A = sp.csr_matrix((v, c, rp), shape=(n, n))
+    b = A @ P.uniform(n, seed)
+    return rp, c, v, n, A, b
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+    return torch
+
+
+def _dev(torch, a):
+    return torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).cuda()
+
+
+@pytest.fixture(scope="module")
+def trained(gpu):
+    """A model trained briefly on small 3D convection-diffusion systems."""
+    B = gpu
+    mats = [B.GpuMatrix(B.CsrMatrix(*P.convdiff3d(nx)[:3]), B.FP32) for nx in (12, 16)]
+    model = B.SpaiModel(seed=3)
+    loss0 = model.loss_grad(mats[1], probes=8, seed=5)[0]
+    loss = model.train(mats, epochs=150, probes=8, lr=3e-3, seed=7)
+    yield model, loss0, loss
+    for m in mats:
+        m.close()
+
+
+def test_spai_gradient_matches_oracle(gpu):
+    B = gpu
+    rp, c, v, n = P.convdiff2d(18)
+    G = B.GpuMatrix(B.CsrMatrix(rp, c, v), B.FP32)
+    model = B.SpaiModel(seed=11)
+    rng = np.random.default_rng(4)
+    p = model.params().astype(np.float64)
+    W1, b1, W2, b2, W3, b3 = mlp.unpack(p)
+    W3[...] = rng.uniform(-0.2, 0.2, W3.shape)      # exercise every layer
+    b1[...] = rng.uniform(-0.1, 0.1, b1.shape)
+    model.set_params(p.astype(np.float32))
+    p32 = model.params().astype(np.float64)
+    Z = rng.choice([-1.0, 1.0], size=(4, n)).astype(np.float32)
+    loss_g, g_g = model.loss_grad(G, Z=Z)
+    A32 = sp.csr_matrix((v.astype(np.float32).astype(np.float64), c, rp), shape=(n, n))
+    AZ = (A32 @ Z.astype(np.float64).T).T
+    loss_o, g_o = mlp.loss_grad(p32, rp, c, v, n, Z.astype(np.float64), AZ)
+    assert abs(loss_g - loss_o) <= 1e-4 * loss_o
+    assert np.linalg.norm(g_g - g_o) <= 1e-3 * np.linalg.norm(g_o)
+    G.close()
+
+
+@pytest.mark.parametrize("precond", [0, 1])
+def test_mixed_reaches_fp64_target(gpu, torch_cuda, precond):
+    B, torch = gpu, torch_cuda
+    rp, c, v, n, A, b = _system(P.convdiff3d, 24)
+    G = B.GpuMatrix(B.CsrMatrix(rp, c, v), B.FP32)
+    bd, xd = _dev(torch, b), torch.zeros(n, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    ret, st = G.solve_mixed(bd.data_ptr(), xd.data_ptr(), l=4, target=1e-8,
+                            precond=precond, hist_cap=1000)
+    x = xd.cpu().numpy()
+    assert ret >= 0, st
+    tr = S.true_residual(A, b, x)
+    assert tr <= 1e-8 and abs(tr - st["true_res"]) <= 1e-3 * tr + 1e-15
+    ret_o, x_o, _ = S.bicgstabl(A, b, 4, 1e-12, 1000)
+    assert np.linalg.norm(x - x_o) <= 1e-6 * np.linalg.norm(x_o)
+    assert st["replacements"] >= 1
+    G.close()
+
+
+def test_learned_preconditioner_gains(gpu, torch_cuda, trained):
+    B, torch = gpu, torch_cuda
+    model, loss0, loss = trained
+    assert loss < 0.8 * loss0, (loss0, loss)
+    rp, c, v, n, A, b = _system(P.convdiff3d, 32)
+    G = B.GpuMatrix(B.CsrMatrix(rp, c, v), B.FP32)
+    bd = _dev(torch, b)
+    its = {}
+    for name, pc, md in (("none", 0, None), ("jacobi", 1, None),
+                         ("learned", 2, model)):
+        xd = torch.zeros(n, dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        ret, st = G.solve_mixed(bd.data_ptr(), xd.data_ptr(), l=4, target=1e-8,
+                                precond=pc, model=md, fallback=0)
+        assert ret >= 0, (name, st)
+        assert S.true_residual(A, b, xd.cpu().numpy()) <= 1e-8
+        its[name] = st["iters"]
+    # What the trained network buys: fewer outer iterations than the same
+    # solve without it (Jacobi is a no-op on this constant-diagonal matrix).
+    assert its["learned"] <= 0.8 * its["none"], its
+    G.close()
+
+
+def test_fallback_on_broken_model(gpu, torch_cuda):
+    B, torch = gpu, torch_cuda
+    rp, c, v, n, A, b = _system(P.convdiff3d, 16)
+    G = B.GpuMatrix(B.CsrMatrix(rp, c, v), B.FP32)
+    bad = B.SpaiModel(seed=1)
+    p = bad.params()
+    p[-8:] = np.nan                         # output bias NaN -> M is NaN
+    bad.set_params(p)
+    bd = _dev(torch, b)
+    xd = torch.zeros(n, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    ret, st = G.solve_mixed(bd.data_ptr(), xd.data_ptr(), precond=2, model=bad,
+                            fallback=0)
+    assert ret == B.DIVERGENCE
+    xd.zero_()
+    torch.cuda.synchronize()
+    ret, st = G.solve_mixed(bd.data_ptr(), xd.data_ptr(), precond=2, model=bad,
+                            fallback=1)
+    assert ret >= 0 and st["sweeps"] == 2
+    assert S.true_residual(A, b, xd.cpu().numpy()) <= 1e-8
+    G.close()
+
+
+def test_checkpoint_roundtrip_and_host_api(gpu, trained, tmp_path):
+    B = gpu
+    model = trained[0]
+    path = str(tmp_path / "spai.bin")
+    model.save(path)
+    loaded = B.SpaiModel(path=path)
+    assert np.array_equal(loaded.params(), model.params())
+    rp, c, v, n, A, b = _system(P.convdiff3d, 20)
+    x = np.zeros(n)
+    ret = B.dbicgstabl_mixed(B.CsrMatrix(rp, c, v), b, x, l=4, target=1e-8,
+                             precond=2, model=loaded)
+    assert ret >= 0 and S.true_residual(A, b, x) <= 1e-8
