@@ -194,6 +194,71 @@ int dbicgstabl(dspmat* A, double* b, int l, double tol, int max_iter,
   return solve_single(Method::BICGSTABL, A, b, l, tol, max_iter, x);
 }
 
+}  // extern "C"
+
+// ------------------------------------------------------- shifted methods
+
+namespace {
+
+int solve_shifted(bool stab, dspmat* A, double* b, int l, double* sigma,
+                  int ns, double tol, int max_iter, double* x) {
+  if (check_matrix(A) != 0 || !b || !x || ns < 0 || ns > kMaxShifts ||
+      (ns > 0 && !sigma))
+    return INVALID_PARAMETERS;
+  if (stab && (l < 1 || l > kBlMaxL)) return INVALID_PARAMETERS;
+  try {
+    Ctx& cx = Ctx::get();
+    cudaStream_t st = cx.st;
+    Timer tm(st);
+    const int n = *A->row_size;
+    DevCsr dA, dAt;
+    upload_operator(A, false, false, dA, st);
+    if (!stab) {
+      HostCsr t = transpose(n, A->row, A->col, A->value);
+      upload_csr(n, t.rowptr.data(), t.col.data(), t.val.data(), false, dAt, st);
+    }
+    double* db = upload_vec(b, n, 1, st);
+    double* dx = upload_vec(x, n, (long long)ns + 1, st);
+    SolveState ss;
+    ss.create(hist_cap_for(max_iter), st);
+    tm.begin_solve();
+    SolveOut o = stab ? bk::shbicgstabl(dA, db, l, sigma, ns, dx, tol, max_iter, ss, st)
+                      : bk::shbicg(dA, dAt, db, sigma, ns, dx, tol, max_iter, ss, st);
+    tm.end_solve();
+    download_vec(x, dx, n, (long long)ns + 1, st);
+    tm.report(o.ret, &ss, o.iters);
+    ss.release(st);
+    dfree(db, st);
+    dfree(dx, st);
+    dA.release(st);
+    dAt.release(st);
+    BK_CHECK(cudaStreamSynchronize(st));
+    return o.ret;
+  } catch (const std::exception& e) {
+    if (std::getenv("BKSP_GPU_VERBOSE")) std::fprintf(stderr, "bksp: %s\n", e.what());
+    cudaGetLastError();
+    return INVALID_PARAMETERS;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int dshbicg(dspmat* A, double* b, double* sigma, int sigma_size, double tol,
+            int max_iter, double* x) {
+  return solve_shifted(false, A, b, 0, sigma, sigma_size, tol, max_iter, x);
+}
+
+int dshbicgstabl(dspmat* A, double* b, int l, double* sigma, int sigma_size,
+                 double tol, int max_iter, double* x) {
+  return solve_shifted(true, A, b, l, sigma, sigma_size, tol, max_iter, x);
+}
+
+}  // extern "C"
+
+extern "C" {
+
 // ---------------------------------------------------------- dense helpers
 // Host-side containers (reference src/util.c:5-67); no computation.
 

@@ -5,7 +5,5 @@ extern "C" {
 int dblcg(dspmat*, dmat*, double, int, dmat*) { return INVALID_PARAMETERS; }
 int dblbicgstab(dspmat*, dmat*, double, int, dmat*) { return INVALID_PARAMETERS; }
 int dblbicgstabl(dspmat*, dmat*, int, double, int, dmat*) { return INVALID_PARAMETERS; }
-int dshbicg(dspmat*, double*, double*, int, double, int, double*) { return INVALID_PARAMETERS; }
-int dshbicgstabl(dspmat*, double*, int, double*, int, double, int, double*) { return INVALID_PARAMETERS; }
 int myqr(int, int, double*, double*) { return INVALID_PARAMETERS; }
 }

@@ -51,6 +51,96 @@ __device__ __forceinline__ void bl_back_substitution(double* S, int l) {
   }
 }
 
+// Shifted BiCGSTAB(l) helpers (src/shbicgstabl.c, src/util_shift.c).
+__device__ __forceinline__ void horner_shift(const double* gamma, int l,
+                                             double sigma, double* out) {
+  // The reference's dhorner (src/util_shift.c:5-27), step for step.
+  out[l] = -gamma[l - 1];
+  for (int i = l - 1; i > 0; --i) out[i] = -sigma * out[i + 1] - gamma[i - 1];
+  out[0] = -sigma * out[1] + 1.0;
+  for (int i = 1; i < l; ++i)
+    for (int j = l - 1; j >= i; --j) out[j] += -sigma * out[j + 1];
+  for (int i = 1; i <= l; ++i) out[i] = -out[i] / out[0];
+}
+
+__device__ __forceinline__ double binom(int n, int r) {
+  if (n < 0 || r < 0 || n < r) return 0.0;
+  double c = 1.0;
+  for (int q = 1; q <= r; ++q) c = c * (double)(n - r + q) / (double)q;
+  return c;
+}
+
+__device__ __forceinline__ double ipow(double x, int p) {
+  double y = 1.0;
+  for (int q = 0; q < p; ++q) y *= x;
+  return y;
+}
+
+// End of the MR part of shifted BiCGSTAB(l): seed omega, omega'' and the
+// per-shift update coefficients (src/shbicgstabl.c:175-227).
+static __device__ void shl_mr_finish(double* S, int l, int ns) {
+  double* om = S + kBlOmega;
+  const double* omd = S + kBlOmegaD;
+  double* omdd = S + kBlOmegaDD;
+  const double* tau = S + kBlTau;
+  om[l - 1] = omd[l - 1];
+  for (int j = l - 2; j >= 0; --j) {
+    double t = 0.0;
+    for (int i = j + 1; i < l; ++i) t += tau[j * l + i] * om[i];
+    om[j] = omd[j] - t;
+  }
+  for (int j = 0; j < l - 1; ++j) {
+    double t = 0.0;
+    for (int i = j + 1; i < l - 1; ++i) t += tau[j * l + i] * om[i + 1];
+    omdd[j] = om[j + 1] + t;
+  }
+  for (int k = 0; k < ns; ++k) {
+    const double sg = S[kShSigma + k];
+    double h[kBlMaxL + 1], oms[kBlMaxL], omsd[kBlMaxL], omsdd[kBlMaxL];
+    horner_shift(om, l, sg, h);
+    const double psi = h[0];
+    for (int i = 0; i < l; ++i) oms[i] = h[i + 1];
+    const double e = S[kShTheta + k] * S[kShPi + k];
+    S[kShTheta + k] = S[kShTheta + k] * psi;
+    for (int j = 0; j < l; ++j) {
+      double t = 0.0;
+      for (int i = j; i < l; ++i) t += ipow(sg, i - j) * binom(i, j) * oms[i];
+      omsd[j] = t;
+    }
+    for (int j = 0; j < l - 1; ++j) {
+      double t = 0.0;
+      for (int i = j + 1; i < l - 1; ++i) t += tau[j * l + i] * omsd[i + 1];
+      omsdd[j] = omsd[j + 1] + t;
+    }
+    double* cx = S + kShCx + k * 8;
+    cx[0] = omsd[0] / e;
+    for (int i = 1; i < l; ++i) cx[i] = omsdd[i - 1] / e;
+    S[kShPsiInv + k] = 1.0 / psi;
+  }
+}
+
+// pi_new / beta_k / alpha_k of every shift after a seed alpha (shared by
+// shifted BiCG, src/shbicg.c:78-88, and shifted BiCGSTAB(l), :111-121).
+__device__ __forceinline__ void shift_scalars(double* S, int ns, double alpha,
+                                              double beta) {
+  const double aold = S[kShAlphaOld];
+  for (int k = 0; k < ns; ++k) {
+    const double pi = S[kShPi + k], po = S[kShPiOld + k];
+    const double pn = (1.0 + alpha * S[kShSigma + k]) * pi +
+                      alpha * beta / aold * (po - pi);
+    S[kShPiNew + k] = pn;
+    S[kShBeta + k] = (po / pi) * (po / pi) * beta;
+    S[kShAlpha + k] = pi / pn * alpha;
+  }
+}
+
+__device__ __forceinline__ void shift_rotate(double* S, int ns) {
+  for (int k = 0; k < ns; ++k) {
+    S[kShPiOld + k] = S[kShPi + k];
+    S[kShPi + k] = S[kShPiNew + k];
+  }
+}
+
 __device__ __forceinline__ void bl_beta0(double* S, int l, double g1) {
   // src/bicgstabl.c:57 gamma0 = -omega[l] gamma0, then :60-62 for j = 0.
   const double g0 = -S[kBlOmega + l] * S[kBlG0];
@@ -246,6 +336,87 @@ static __device__ void run_epilogue(const Red& rd) {
     case E_MX_REBETA:        // r0 = fl(r64) replaced: D0 = (rs, r0)
       S[kMxDoRep] = 0.0;
       bl_beta0(S, l, D[0]);
+      break;
+    // ---------------- shifted BiCG, src/shbicg.c
+    case E_SHB_INIT: {       // :27-46; then rho / beta of iteration 0 (:52-53)
+      const int ns = (int)S[kNs];
+      S[kFnb] = sqrt(D[0]);
+      S[kShAlphaOld] = 1.0;
+      S[kShRhoOld] = 1.0;
+      for (int k = 0; k < ns; ++k) {
+        S[kShPi + k] = 1.0;
+        S[kShPiOld + k] = 1.0;
+      }
+      S[kShRho] = D[1];
+      S[kShBetaS] = -S[kShRho] / S[kShRhoOld];
+      break;
+    }
+    case E_SHB_ALPHA: {      // :72, :78-88
+      const double alpha = S[kShRho] / D[0];
+      S[kShAlphaS] = alpha;
+      shift_scalars(S, (int)S[kNs], alpha, S[kShBetaS]);
+      break;
+    }
+    case E_SHB_CHECK: {      // :105-115, then :52-53 of the next iteration
+      const int ns = (int)S[kNs];
+      S[kShAlphaOld] = S[kShAlphaS];
+      S[kShRhoOld] = S[kShRho];
+      shift_rotate(S, ns);
+      conv_check(rd, sqrt(D[1]) / S[kFnb]);
+      S[kShRho] = D[0];
+      S[kShBetaS] = -S[kShRho] / S[kShRhoOld];
+      break;
+    }
+    // ---------------- shifted BiCGSTAB(l), src/shbicgstabl.c
+    case E_SHL_INIT: {       // :25, :39-43, :60-66; then :88-92 (m = 0, j = 0)
+      const int ns = (int)S[kNs];
+      S[kFnb] = sqrt(D[0]);
+      S[kBlAlpha] = 0.0;
+      S[kShAlphaOld] = 1.0;
+      S[kShRhoOld] = 1.0;
+      for (int i = 0; i < l; ++i) S[kBlOmega + i] = 0.0;
+      S[kBlOmega + l - 1] = 1.0;
+      for (int k = 0; k < ns; ++k) {
+        S[kShPi + k] = 1.0;
+        S[kShPiOld + k] = 1.0;
+        S[kShTheta + k] = 1.0;
+      }
+      S[kShRhoOld] = -S[kBlOmega + l - 1] * S[kShRhoOld];
+      S[kShRho] = D[1];
+      S[kBlBeta] = S[kBlAlpha] * S[kShRho] / S[kShRhoOld];
+      break;
+    }
+    case E_SHL_BETA:         // :91 (j > 0); beta after the rotation below
+      S[kShRhoNext] = D[0];
+      break;
+    case E_SHL_ALPHA:        // :105, :111-121
+      S[kBlAlpha] = S[kShRho] / D[0];
+      shift_scalars(S, (int)S[kNs], S[kBlAlpha], S[kBlBeta]);
+      break;
+    case E_SHL_ROTATE:       // :156-161, then :91-92 of step j + 1 (a0 = 1)
+      S[kShAlphaOld] = S[kBlAlpha];
+      S[kShRhoOld] = S[kShRho];
+      shift_rotate(S, (int)S[kNs]);
+      if (rd.a0) {
+        S[kShRho] = S[kShRhoNext];
+        S[kBlBeta] = S[kBlAlpha] * S[kShRho] / S[kShRhoOld];
+      }
+      break;
+    case E_SHL_TAU:          // :168
+      S[kBlTau + rd.a0 * l + rd.a1] = D[0] / S[kBlSigma + rd.a0];
+      break;
+    case E_SHL_SIG:          // :171-172, then :175-227 after the last one
+      S[kBlSigma + rd.a1] = D[0];
+      S[kBlOmegaD + rd.a1] = D[1] / D[0];
+      if (rd.a1 == l - 1) shl_mr_finish(S, l, (int)S[kNs]);
+      break;
+    case E_SHL_CHECK:        // :244-247, then :88-92 of the next iteration
+      conv_check(rd, sqrt(D[0]) / S[kFnb]);
+      if (!rd.ctl->done) {
+        S[kShRhoOld] = -S[kBlOmega + l - 1] * S[kShRhoOld];
+        S[kShRho] = D[1];
+        S[kBlBeta] = S[kBlAlpha] * S[kShRho] / S[kShRhoOld];
+      }
       break;
     default:
       break;

@@ -8,7 +8,7 @@
 
 namespace bk {
 
-constexpr int kScalars = 512;     // FP64 scalar slots per solve
+constexpr int kScalars = 8192;    // FP64 scalar slots per solve
 constexpr int kGridCap = 148 * 8; // reduction grid cap (= kMaxBlocks)
 constexpr int kNotConverged = -1;
 constexpr int kDivergence = -2;
@@ -117,6 +117,17 @@ void launch_mx_d2f(const double* in, float* o0, float* o1, float* o2,
                    cudaStream_t st);
 void launch_mx_accum(double* x, const float* t, float* y, long long n,
                      const RedH& rd, cudaStream_t st);
+// Fused all-shift update of the shifted methods (k_shift.cuh).
+struct ShiftArgsH {
+  const double* r;
+  const double* p;
+  double* x;
+  double* xs;
+  double* ps;
+  long long np;
+  int ns, l, j, mode;
+};
+void launch_shift(const ShiftArgsH& a, const RedH& rd, cudaStream_t st);
 // Solve start: reset control + ticket, optionally preset S[slot] (slot < 0:
 // none).  Scalar preset without host synchronisation.
 void launch_ctl_init(CtlH* c, unsigned* ticket, double* S, int iter0,

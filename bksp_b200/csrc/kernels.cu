@@ -7,6 +7,7 @@
 #include "epilogues.cuh"
 #include "k_spmv.cuh"
 #include "k_vec.cuh"
+#include "k_shift.cuh"
 #include "kernel_api.h"
 
 namespace bk {
@@ -98,6 +99,20 @@ void launch_convert_d2f(const double* a, float* b, long long n, cudaStream_t st)
 void launch_convert_f2d(const float* a, double* b, long long n, cudaStream_t st) {
   ++launch_count();
   k_convert_f2d<<<grid_for(n), kThreads, 0, st>>>(a, b, n);
+}
+
+// ------------------------------------------------------- shifted methods
+
+void launch_shift(const ShiftArgsH& a, const RedH& rd, cudaStream_t st) {
+  ++launch_count();
+  ShiftArgs s{a.r, a.p, a.x, a.xs, a.ps, a.np, a.ns, a.l, a.j, a.mode};
+  const int g = grid_for(a.np);
+  switch (a.mode) {
+    case 0: k_shift<0><<<g, kThreads, 0, st>>>(s, rd); break;
+    case 1: k_shift<1><<<g, kThreads, 0, st>>>(s, rd); break;
+    case 2: k_shift<2><<<g, kThreads, 0, st>>>(s, rd); break;
+    default: k_shift<3><<<g, kThreads, 0, st>>>(s, rd); break;
+  }
 }
 
 // ------------------------------------------------- mixed-precision steps

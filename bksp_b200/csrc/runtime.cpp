@@ -229,6 +229,14 @@ void SolveState::set_scalar(short slot, double v, cudaStream_t st) {
   BK_CHECK(cudaGetLastError());
 }
 
+void SolveState::set_scalars(short slot, const double* host, int count,
+                             cudaStream_t st) {
+  if (count <= 0) return;
+  BK_CHECK(cudaMemcpyAsync(S + slot, host, sizeof(double) * count,
+                           cudaMemcpyHostToDevice, st));
+  BK_CHECK(cudaStreamSynchronize(st));
+}
+
 double SolveState::get_scalar(short slot, cudaStream_t st) const {
   double v = 0.0;
   BK_CHECK(cudaMemcpyAsync(&v, S + slot, sizeof(double),

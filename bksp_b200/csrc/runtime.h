@@ -112,6 +112,7 @@ struct SolveState {
   }
   CtlH read(cudaStream_t st) const;
   void set_scalar(short slot, double v, cudaStream_t st);
+  void set_scalars(short slot, const double* host, int count, cudaStream_t st);
   double get_scalar(short slot, cudaStream_t st) const;
 };
 

@@ -48,6 +48,22 @@ enum : short {
   kMxReps = 207,      // replacements performed
 };
 
+// Shifted methods: per-shift arrays (kMaxShifts entries each).
+enum : short {
+  kMaxShifts = 256,
+  kShSigma = 2048,    // sigma_k
+  kShPi = 2304,       // pi_k
+  kShPiOld = 2560,    // pi_old_k
+  kShPiNew = 2816,    // pi_new_k
+  kShAlpha = 3072,    // alpha_k
+  kShBeta = 3328,     // beta_k
+  kShTheta = 3584,    // theta_k (shifted BiCGSTAB(l))
+  kShPsiInv = 3840,   // 1 / psi_k
+  kShCx = 4096,       // x_k update coefficients, [k][i], 8 per shift
+  kShAlphaOld = 24, kShRho = 25, kShRhoOld = 26,   // seed scalars
+  kShBetaS = 27, kShAlphaS = 28, kShRhoNext = 29,
+};
+
 // Epilogue codes.
 enum : short {
   E_NONE = 0,
@@ -65,6 +81,11 @@ enum : short {
   E_BL_CHECK,
   // mixed-precision BiCGSTAB(l)
   E_MX_INIT, E_MX_INIT2, E_MX_CHECK, E_MX_TRUE, E_MX_REBETA,
+  // shifted BiCG (src/shbicg.c)
+  E_SHB_INIT, E_SHB_ALPHA, E_SHB_CHECK,
+  // shifted BiCGSTAB(l) (src/shbicgstabl.c)
+  E_SHL_INIT, E_SHL_BETA, E_SHL_ALPHA, E_SHL_ROTATE, E_SHL_TAU, E_SHL_SIG,
+  E_SHL_CHECK,
   E_COUNT_BASE,
 };
 

@@ -25,6 +25,15 @@ SolveOut bicgstab(const DevCsr& A, const double* b, double* x, double tol,
 SolveOut bicgstabl(const DevCsr& A, const double* b, int l, double* x,
                    double tol, int max_iter, SolveState& ss, cudaStream_t st);
 
+// Shifted methods: x holds (ns + 1) padded vectors (seed first), the
+// shifted parts zero on entry (the reference's assumption).
+SolveOut shbicg(const DevCsr& A, const DevCsr& At, const double* b,
+                const double* sigma_host, int ns, double* x, double tol,
+                int max_iter, SolveState& ss, cudaStream_t st);
+SolveOut shbicgstabl(const DevCsr& A, const double* b, int l,
+                     const double* sigma_host, int ns, double* x, double tol,
+                     int max_iter, SolveState& ss, cudaStream_t st);
+
 // Mixed-precision right-preconditioned BiCGSTAB(l): FP32 matrix values and
 // Krylov vectors (A.v32 / M->v32), FP64 dot products, scalars and solution,
 // FP64 reliable residual replacement; stops on the FP64 true relative
