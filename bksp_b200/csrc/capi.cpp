@@ -22,6 +22,7 @@
 #include "capi_internal.h"
 #include "runtime.h"
 #include "solvers.h"
+#include "solvers_block.h"
 
 using namespace bk;
 
@@ -192,6 +193,154 @@ int dbicgstab(dspmat* A, double* b, double tol, int max_iter, double* x) {
 int dbicgstabl(dspmat* A, double* b, int l, double tol, int max_iter,
                double* x) {
   return solve_single(Method::BICGSTABL, A, b, l, tol, max_iter, x);
+}
+
+}  // extern "C"
+
+// --------------------------------------------------------- block methods
+
+namespace {
+
+enum class BMethod { CG, BICGSTAB, BICGSTABL };
+
+int solve_block(BMethod m, dspmat* A, dmat* B, int l, double tol, int max_iter,
+                dmat* X) {
+  if (check_matrix(A) != 0 || !B || !X || !B->value || !X->value)
+    return INVALID_PARAMETERS;
+  if (m == BMethod::CG && !is_symmetric(A)) return INVALID_MATRIX_TYPE;
+  const int n = *A->row_size, s = B->col_size;
+  if (B->row_size != n || X->row_size != n || X->col_size != s || s < 1 ||
+      s > kBlockMaxS)
+    return INVALID_PARAMETERS;
+  if (m == BMethod::BICGSTABL && (l < 1 || l > kBlMaxL)) return INVALID_PARAMETERS;
+  try {
+    Ctx& cx = Ctx::get();
+    cudaStream_t st = cx.st;
+    Timer tm(st);
+    DevCsr dA;
+    upload_operator(A, m == BMethod::CG, false, dA, st);
+    const long long np = pad64(n);
+    double* tmp = dalloc_n<double>((long long)n * s, st);
+    double* dB = dalloc_n<double>(np * s, st);
+    double* dX = dalloc_n<double>(np * s, st);
+    BK_CHECK(cudaMemsetAsync(dB, 0, sizeof(double) * np * s, st));
+    BK_CHECK(cudaMemsetAsync(dX, 0, sizeof(double) * np * s, st));
+    BK_CHECK(cudaMemcpyAsync(tmp, B->value, sizeof(double) * n * s,
+                             cudaMemcpyHostToDevice, st));
+    launch_cm2rm(tmp, dB, n, s, st);
+    BK_CHECK(cudaMemcpyAsync(tmp, X->value, sizeof(double) * n * s,
+                             cudaMemcpyHostToDevice, st));
+    launch_cm2rm(tmp, dX, n, s, st);
+    SolveState ss;
+    ss.create(hist_cap_for(max_iter), st);
+    SolveOut o;
+    double true_res = 0.0;
+    {
+      BlockCtx bc(n, s, ss, st);
+      tm.begin_solve();
+      switch (m) {
+        case BMethod::CG: o = bk::blcg(bc, dA, dB, dX, tol, max_iter); break;
+        case BMethod::BICGSTAB: o = bk::blbicgstab(bc, dA, dB, dX, tol, max_iter); break;
+        case BMethod::BICGSTABL:
+          o = bk::blbicgstabl(bc, dA, dB, dX, l, tol, max_iter, &true_res);
+          break;
+      }
+      tm.end_solve();
+      bc.release();
+    }
+    launch_rm2cm(dX, tmp, n, s, st);
+    BK_CHECK(cudaMemcpyAsync(X->value, tmp, sizeof(double) * n * s,
+                             cudaMemcpyDeviceToHost, st));
+    BK_CHECK(cudaStreamSynchronize(st));
+    if (m == BMethod::BICGSTABL) {
+      // The reference prints this summary on every exit
+      // (src/blbicgstabl.c:220-224).
+      const double err = ss.get_scalar(kErr, st);
+      const int it = o.ret >= 0 ? o.ret : max_iter;
+      std::printf("Block BiCGSTAB(%d) has converged at:\n"
+                  "        The number of iteration ... %d\n"
+                  "        Frobenius norm of the relative residual ... %e\n"
+                  "        Frobenius norm of the true residual ... %e\n",
+                  l, it, err, true_res);
+      std::fflush(stdout);
+    }
+    tm.report(o.ret, &ss, o.iters);
+    if (g_stats) g_stats->true_res = true_res;
+    ss.release(st);
+    dfree(tmp, st);
+    dfree(dB, st);
+    dfree(dX, st);
+    dA.release(st);
+    BK_CHECK(cudaStreamSynchronize(st));
+    return o.ret;
+  } catch (const std::exception& e) {
+    if (std::getenv("BKSP_GPU_VERBOSE")) std::fprintf(stderr, "bksp: %s\n", e.what());
+    cudaGetLastError();
+    return INVALID_PARAMETERS;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int dblcg(dspmat* A, dmat* B, double tol, int max_iter, dmat* X) {
+  return solve_block(BMethod::CG, A, B, 0, tol, max_iter, X);
+}
+
+int dblbicgstab(dspmat* A, dmat* B, double tol, int max_iter, dmat* X) {
+  return solve_block(BMethod::BICGSTAB, A, B, 0, tol, max_iter, X);
+}
+
+int dblbicgstabl(dspmat* A, dmat* B, int l, double tol, int max_iter, dmat* X) {
+  return solve_block(BMethod::BICGSTABL, A, B, l, tol, max_iter, X);
+}
+
+// Thin QR on the GPU (reference src/myqr.c:4-39): mat (m-by-n,
+// column-major) becomes Q, r (n-by-n, column-major) receives the upper-
+// triangular R with non-negative diagonal.  Returns 0, or
+// INVALID_PARAMETERS (bad sizes, n > 16, rank-deficient input, CUDA error).
+int myqr(int m, int n, double* mat, double* r) {
+  if (m < 1 || n < 1 || n > kBlockMaxS || m < n || !mat || !r)
+    return INVALID_PARAMETERS;
+  try {
+    Ctx& cx = Ctx::get();
+    cudaStream_t st = cx.st;
+    const long long np = pad64(m);
+    double* tmp = dalloc_n<double>((long long)m * n, st);
+    double* V = dalloc_n<double>(np * n, st);
+    BK_CHECK(cudaMemsetAsync(V, 0, sizeof(double) * np * n, st));
+    BK_CHECK(cudaMemcpyAsync(tmp, mat, sizeof(double) * m * n,
+                             cudaMemcpyHostToDevice, st));
+    launch_cm2rm(tmp, V, m, n, st);
+    SolveState ss;
+    ss.create(0, st);
+    int rc = 0;
+    {
+      BlockCtx bc(m, n, ss, st);
+      bk::thin_qr(bc, V);
+      const CtlH c = ss.read(st);
+      if (c.done) rc = INVALID_PARAMETERS;   // Cholesky breakdown
+    }
+    launch_rm2cm(V, tmp, m, n, st);
+    BK_CHECK(cudaMemcpyAsync(mat, tmp, sizeof(double) * m * n,
+                             cudaMemcpyDeviceToHost, st));
+    std::vector<double> R((size_t)n * n);
+    BK_CHECK(cudaMemcpyAsync(R.data(), ss.S + kBkR, sizeof(double) * n * n,
+                             cudaMemcpyDeviceToHost, st));
+    BK_CHECK(cudaStreamSynchronize(st));
+    for (int i = 0; i < n; ++i)        // column-major, zero below the diagonal
+      for (int j = 0; j < n; ++j) r[i * n + j] = j <= i ? R[(size_t)j * n + i] : 0.0;
+    ss.release(st);
+    dfree(tmp, st);
+    dfree(V, st);
+    BK_CHECK(cudaStreamSynchronize(st));
+    return rc;
+  } catch (const std::exception& e) {
+    if (std::getenv("BKSP_GPU_VERBOSE")) std::fprintf(stderr, "bksp: %s\n", e.what());
+    cudaGetLastError();
+    return INVALID_PARAMETERS;
+  }
 }
 
 }  // extern "C"

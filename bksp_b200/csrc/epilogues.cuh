@@ -5,6 +5,7 @@
 #pragma once
 #include "dev_common.cuh"
 #include "solver_defs.h"
+#include "epi_block.cuh"
 
 namespace bk {
 
@@ -139,6 +140,68 @@ __device__ __forceinline__ void shift_rotate(double* S, int ns) {
     S[kShPiOld + k] = S[kShPi + k];
     S[kShPi + k] = S[kShPiNew + k];
   }
+}
+
+// One Cholesky-QR pass on the Gram matrix in kBkG1: R_pass with
+// R^T R = G (+ shift), kBkRinv = R^-1, kBkR = R_pass * kBkR (kBkR = R_pass
+// for the first pass).  The first pass is shifted (shifted CholeskyQR3,
+// Fukaya et al. 2020), so the three passes together give Q R = V with
+// orthonormal Q to rounding for any numerically full-rank V.
+static __device__ bool qr_pass(double* S, int pass) {
+  const int s = (int)S[kBkS];
+  double* G = S + kBkG1;
+  double* Rp = S + kBkScr;
+  double shift = 0.0;
+  if (pass == 1) {
+    double tr = 0.0;
+    for (int i = 0; i < s; ++i) tr += G[i * s + i];
+    const double m = S[kBkRows];
+    shift = 11.0 * (m * s + s * (s + 1.0)) * 1.1102230246251565e-16 * tr;
+  }
+  if (!dm_chol(G, Rp, s, shift)) return false;
+  dm_triinv(Rp, S + kBkRinv, s);
+  if (pass == 1) {
+    dm_copy(Rp, S + kBkR, s);
+  } else {
+    dm_mul(Rp, S + kBkR, S + kBkScr2, s);
+    dm_copy(S + kBkScr2, S + kBkR, s);
+  }
+  return true;
+}
+
+static __device__ void qr_post(const Red& rd, int action) {
+  double* S = rd.S;
+  const int s = (int)S[kBkS];
+  switch (action) {
+    case QR_POST_BCG:        // src/blcg.c:95-105
+      dm_copy(S + kBkR, S + kBkBeta, s);
+      dm_mul(S + kBkBeta, S + kBkC, S + kBkScr, s);
+      dm_copy(S + kBkScr, S + kBkC, s);
+      conv_check(rd, dm_fro(S + kBkC, s) / S[kFnb]);
+      break;
+    case QR_POST_BCG_INIT:   // src/blcg.c:58, :61-63
+      dm_copy(S + kBkR, S + kBkC, s);
+      dm_eye(S + kBkBeta, s);
+      break;
+    case QR_POST_BBL_INIT:   // src/blbicgstabl.c:88
+      dm_copy(S + kBkR, S + kBkXi, s);
+      break;
+    case QR_POST_BBL_T:      // src/blbicgstabl.c:135-148
+      dm_copy(S + kBkR, S + kBkT, s);
+      dm_copy(S + kBkXi, S + kBkXiOld, s);
+      dm_mul(S + kBkT, S + kBkXiOld, S + kBkXi, s);
+      dm_copy(S + kBkT, S + kBkScr, s);
+      dm_inv(S + kBkScr, S + kBkPiv, S + kBkTinv, s);
+      dm_mul(S + kBkAlpha, S + kBkTinv, S + kBkATinv, s);
+      break;
+    default:
+      break;
+  }
+}
+
+static __device__ void fail_divergence(const Red& rd) {
+  rd.ctl->done = 1;
+  rd.ctl->ret = kDivergence;
 }
 
 __device__ __forceinline__ void bl_beta0(double* S, int l, double g1) {
@@ -418,6 +481,91 @@ static __device__ void run_epilogue(const Red& rd) {
         S[kBlBeta] = S[kBlAlpha] * S[kShRho] / S[kShRhoOld];
       }
       break;
+    // ---------------- Cholesky-QR passes
+    case E_QR1:
+      if (!qr_pass(S, 1)) fail_divergence(rd);
+      break;
+    case E_QR2:
+      if (!qr_pass(S, 2)) fail_divergence(rd);
+      break;
+    case E_QR3:
+      if (!qr_pass(S, 3)) fail_divergence(rd);
+      else qr_post(rd, rd.a0);
+      break;
+    // ---------------- Block CG, src/blcg.c
+    case E_BCG_INIT:         // :60 ||B||_F, then the first pass of myqr (:58)
+      S[kFnb] = sqrt(D[0]);
+      if (!qr_pass(S, 1)) fail_divergence(rd);
+      break;
+    case E_BCG_ALPHA: {      // :78-86  alpha = (P^T A P)^-1, tmp = alpha C
+      const int s = (int)S[kBkS];
+      dm_copy(S + kBkG1, S + kBkLU, s);
+      dm_inv(S + kBkLU, S + kBkPiv, S + kBkAlpha, s);
+      dm_mul(S + kBkAlpha, S + kBkC, S + kBkTmp, s);
+      break;
+    }
+    // ---------------- Block BiCGSTAB, src/blbicgstab.c
+    case E_BBS_INIT:         // :175
+      S[kFnb] = sqrt(D[0]);
+      break;
+    case E_BBS_ALPHA: {      // :185-189  alpha = (Rs^T V)^-1 (Rs^T R)
+      const int s = (int)S[kBkS];
+      dm_copy(S + kBkG1, S + kBkLU, s);
+      dm_lu(S + kBkLU, S + kBkPiv, s);
+      dm_copy(S + kBkG2, S + kBkAlpha, s);
+      dm_lu_solve(S + kBkLU, S + kBkPiv, S + kBkAlpha, s, s);
+      break;
+    }
+    case E_BBS_OMEGA:        // :200-201
+      S[kOmega1] = D[0] / D[1];
+      break;
+    case E_BBS_BETA: {       // :212-214, :226-229
+      const int s = (int)S[kBkS];
+      for (int q = 0; q < s * s; ++q) S[kBkBeta + q] = -S[kBkG1 + q];
+      dm_lu_solve(S + kBkLU, S + kBkPiv, S + kBkBeta, s, s);
+      conv_check(rd, sqrt(D[0]) / S[kFnb]);
+      break;
+    }
+    // ---------------- Block BiCGSTAB(l), src/blbicgstabl.c
+    case E_BBL_INIT: {       // :31-38, :67-76, :93 and the first myqr pass (:88)
+      const int s = (int)S[kBkS];
+      S[kFnb] = sqrt(D[0]);
+      for (int q = 0; q < s * s; ++q) S[kBkAlpha + q] = 0.0;
+      dm_eye(S + kBkGam0, s);
+      for (int i = 0; i <= l; ++i) S[kBlOmega + i] = 0.0;
+      S[kBlOmega + l] = 1.0;
+      // :98  gamma0 = -omega[l] gamma0 of the first iteration
+      for (int q = 0; q < s * s; ++q) S[kBkGam0 + q] *= -S[kBlOmega + l];
+      if (!qr_pass(S, 1)) fail_divergence(rd);
+      break;
+    }
+    case E_BBL_BETA: {       // :102-108  beta = -alpha gamma0^-1 gamma1
+      const int s = (int)S[kBkS];
+      dm_copy(S + kBkG1, S + kBkGam1, s);
+      dm_copy(S + kBkGam0, S + kBkLU, s);
+      dm_lu(S + kBkLU, S + kBkPiv, s);
+      dm_copy(S + kBkGam1, S + kBkTmp, s);
+      dm_lu_solve(S + kBkLU, S + kBkPiv, S + kBkTmp, s, s);
+      dm_mul(S + kBkAlpha, S + kBkTmp, S + kBkBeta, s);
+      for (int q = 0; q < s * s; ++q) S[kBkBeta + q] = -S[kBkBeta + q];
+      dm_copy(S + kBkGam1, S + kBkGam0, s);
+      break;
+    }
+    case E_BBL_ALPHA: {      // :121-124  alpha = (Rs^T P_{j+1})^-1 gamma1
+      const int s = (int)S[kBkS];
+      dm_copy(S + kBkG1, S + kBkLU, s);
+      dm_lu(S + kBkLU, S + kBkPiv, s);
+      dm_copy(S + kBkGam1, S + kBkAlpha, s);
+      dm_lu_solve(S + kBkLU, S + kBkPiv, S + kBkAlpha, s, s);
+      break;
+    }
+    case E_BBL_CHECK: {      // :209-212, then :98 of the next iteration
+      const int s = (int)S[kBkS];
+      const double err = dm_fro(S + kBkXi, s) / S[kFnb];
+      conv_check(rd, err);
+      for (int q = 0; q < s * s; ++q) S[kBkGam0 + q] *= -S[kBlOmega + l];
+      break;
+    }
     default:
       break;
   }

@@ -1,0 +1,211 @@
+// Block (multiple right-hand side) kernels: K2 SpMM and K4/K5 fused block
+// linear combination + Gram products, for the block methods (reference
+// src/blcg.c, src/blbicgstab.c, src/blbicgstabl.c, which call mkl_dcsrmm /
+// dcsrgemm1 and n-by-s-by-s cblas_dgemm).
+//
+// Blocks are n-by-s, s <= 16, stored ROW-major in HBM (row i's s values
+// contiguous, 128 bytes at s = 16), so one sparse row gathers whole
+// 128-byte rows of X.  s-by-s coefficient matrices live in the scalar slots
+// (row-major, M[b][c] at S[slot + b * s + c]).
+#pragma once
+#include "dev_common.cuh"
+
+namespace bk {
+
+constexpr int kBlkS = 16;           // max block width
+constexpr int kBlkTileRows = 16;    // rows per tile of the block kernel
+
+// ------------------------------------------------------------------ SpMM
+// Y = alpha * A X  (mode 0), Y = C + alpha * A X  (mode 1), with the
+// reference's per-entry rounding (y += (alpha a_k) x_k, no FMA).  Optional
+// Frobenius dots (Y, W) and (Y, Y) into S[out], S[out + 1].
+struct SpmmArgs {
+  const double* X;
+  double* Y;
+  const double* C;
+  const double* W;
+  double alpha;
+  int mode, s, nd;
+};
+
+template <int ND>
+__global__ void __launch_bounds__(kThreads)
+k_spmm(CsrH A, SpmmArgs a, Red rd) {
+  if (skip(rd)) return;
+  const double* __restrict__ val = static_cast<const double*>(A.val);
+  const int lane = threadIdx.x & (kBlkS - 1);
+  const int grp = (blockIdx.x * kThreads + threadIdx.x) / kBlkS;
+  const int ngrp = gridDim.x * kThreads / kBlkS;
+  const int s = a.s;
+  double acc[ND > 0 ? ND : 1];
+#pragma unroll
+  for (int d = 0; d < ND; ++d) acc[d] = 0.0;
+  for (int row = grp; row < A.n; row += ngrp) {
+    if (lane < s) {
+      double y = 0.0;
+      const int k0 = __ldg(A.rowptr + row), k1 = __ldg(A.rowptr + row + 1);
+      for (int k = k0; k < k1; ++k) {
+        const double av = mul_rn(a.alpha, __ldg(val + k));
+        y = add_rn(y, mul_rn(av, __ldg(a.X + (long long)__ldg(A.col + k) * s + lane)));
+      }
+      const long long o = (long long)row * s + lane;
+      if (a.mode == 1) y = add_rn(a.C[o], y);
+      a.Y[o] = y;
+      if (ND > 0) acc[0] += y * a.W[o];
+      if (ND > 1) acc[1] += y * y;
+    }
+  }
+  if (ND > 0 || rd.epi) finish_reduction<ND>(acc, rd);
+}
+
+// ---------------------------------------------- block linear combination
+// out[o] = sum_i term(o, i) with term = c * in[i] (scalar) or
+// c * in[i] * M (M s-by-s from slots, optionally transposed); then up to
+// two Gram products G_g = U_g^T V_g (U, V among [in..., out...]) written to
+// S[gslot_g + a * s + b], and up to two Frobenius dots.
+struct BlkArgs {
+  const double* in[4];
+  double* out[2];
+  CfH c[2][4];
+  short mslot[2][4];     // >= 0: matrix term
+  unsigned char trans[2][4];
+  int nin, nout, s;
+  long long n;           // rows (padded)
+  int ng;
+  unsigned char gram[2][2];
+  short gslot[2];
+  int nd;
+  unsigned char dot[2][2];
+};
+
+__device__ __forceinline__ void blk_finish(const double* g, int ng, int s,
+                                           const double* dd, int nd,
+                                           const BlkArgs& a, const Red& rd);
+
+__global__ void __launch_bounds__(kThreads)
+k_block(BlkArgs a, Red rd) {
+  if (skip(rd)) return;
+  __shared__ double tile[6][kBlkTileRows][kBlkS + 1];
+  __shared__ double mat[2][4][kBlkS * kBlkS];
+  __shared__ double cs[2][4];
+  const int s = a.s;
+  const int t = threadIdx.x;
+  const int r = t / kBlkS, c = t % kBlkS;   // tile element of this thread
+  for (int q = t; q < 2 * 4; q += kThreads) {
+    const int o = q / 4, i = q % 4;
+    cs[o][i] = (o < a.nout && i < a.nin) ? eval_cf(a.c[o][i], rd.S) : 0.0;
+  }
+  for (int o = 0; o < a.nout; ++o)
+    for (int i = 0; i < a.nin; ++i)
+      if (a.mslot[o][i] >= 0)
+        for (int q = t; q < s * s; q += kThreads) {
+          const int b = q / s, cc = q % s;
+          const int src = a.trans[o][i] ? cc * s + b : b * s + cc;
+          mat[o][i][q] = rd.S[a.mslot[o][i] + src];
+        }
+  __syncthreads();
+  double gacc[2] = {0.0, 0.0};
+  double dacc[2] = {0.0, 0.0};
+  const long long ntiles = (a.n + kBlkTileRows - 1) / kBlkTileRows;
+  for (long long tl = blockIdx.x; tl < ntiles; tl += gridDim.x) {
+    const long long row = tl * kBlkTileRows + r;
+    const bool valid = c < s && row < a.n;
+    for (int i = 0; i < a.nin; ++i)
+      tile[i][r][c] = valid ? a.in[i][row * s + c] : 0.0;
+    __syncthreads();
+    for (int o = 0; o < a.nout; ++o) {
+      double y = 0.0;
+      bool first = true;
+      for (int i = 0; i < a.nin; ++i) {
+        const CfH& cf = a.c[o][i];
+        if (!cf.op) continue;
+        double term;
+        if (a.mslot[o][i] >= 0) {
+          double z = 0.0;
+          for (int b = 0; b < s; ++b) z = fma_rn(tile[i][r][b], mat[o][i][b * s + c], z);
+          term = cs[o][i] * z;
+          y = first ? term : add_rn(y, term);
+        } else {
+          y = first ? mul_rn(cs[o][i], tile[i][r][c])
+                    : fma_rn(cs[o][i], tile[i][r][c], y);
+        }
+        first = false;
+      }
+      if (valid) a.out[o][row * s + c] = y;
+      tile[4 + o][r][c] = valid ? y : 0.0;
+    }
+    __syncthreads();
+    for (int g = 0; g < a.ng; ++g) {
+      // thread (r, c) accumulates G[r][c] = sum_rows U[row][r] V[row][c]
+      const int u = a.gram[g][0], v = a.gram[g][1];
+      const int tu = u < a.nin ? u : 4 + (u - a.nin);
+      const int tv = v < a.nin ? v : 4 + (v - a.nin);
+      if (r < s && c < s) {
+        double z = gacc[g];
+#pragma unroll 4
+        for (int q = 0; q < kBlkTileRows; ++q) z = fma_rn(tile[tu][q][r], tile[tv][q][c], z);
+        gacc[g] = z;
+      }
+    }
+    for (int d = 0; d < a.nd; ++d) {
+      const int u = a.dot[d][0], v = a.dot[d][1];
+      const int tu = u < a.nin ? u : 4 + (u - a.nin);
+      const int tv = v < a.nin ? v : 4 + (v - a.nin);
+      dacc[d] = fma_rn(tile[tu][r][c], tile[tv][r][c], dacc[d]);
+    }
+    __syncthreads();
+  }
+  if (a.ng > 0 || a.nd > 0 || rd.epi) blk_finish(gacc, a.ng, s, dacc, a.nd, a, rd);
+}
+
+// Deterministic reduction of per-thread Gram entries (thread t owns entry t
+// of each Gram) and Frobenius dots across the grid; the last block writes
+// the sums to the scalar slots and runs the epilogue.  Partials layout:
+// part[(slot) * kMaxBlocks + block], slots 0..2*256-1 Grams, 512.. dots.
+__device__ __forceinline__ void blk_finish(const double* g, int ng, int s,
+                                           const double* dd, int nd,
+                                           const BlkArgs& a, const Red& rd) {
+  __shared__ double wsum[2][kWarps];
+  __shared__ int is_last;
+  const int t = threadIdx.x;
+  for (int q = 0; q < ng; ++q)
+    rd.part[(q * 256 + t) * kMaxBlocks + blockIdx.x] = g[q];
+  for (int d = 0; d < nd; ++d) {
+    const double v = warp_sum(dd[d]);
+    if ((t & 31) == 0) wsum[d][t >> 5] = v;
+  }
+  __syncthreads();
+  if (t == 0) {
+    for (int d = 0; d < nd; ++d) {
+      double v = 0.0;
+      for (int w = 0; w < kWarps; ++w) v += wsum[d][w];
+      rd.part[(512 + d) * kMaxBlocks + blockIdx.x] = v;
+    }
+    __threadfence();
+    const unsigned tk = atomicAdd(rd.ticket, 1u);
+    is_last = (tk == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!is_last) return;
+  __threadfence();
+  const int nb = gridDim.x;
+  const int r = t / kBlkS, c = t % kBlkS;
+  for (int q = 0; q < ng; ++q) {
+    double v = 0.0;
+    for (int b = 0; b < nb; ++b) v += __ldcg(rd.part + (q * 256 + t) * kMaxBlocks + b);
+    if (r < s && c < s) rd.S[a.gslot[q] + r * s + c] = v;
+  }
+  if (t < nd) {
+    double v = 0.0;
+    for (int b = 0; b < nb; ++b) v += __ldcg(rd.part + (512 + t) * kMaxBlocks + b);
+    rd.S[rd.out + t] = v;
+  }
+  __syncthreads();
+  if (t == 0) {
+    *rd.ticket = 0u;
+    __threadfence();
+    if (rd.epi) run_epilogue(rd);
+  }
+}
+
+}  // namespace bk

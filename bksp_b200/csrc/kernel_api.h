@@ -128,6 +128,34 @@ struct ShiftArgsH {
   int ns, l, j, mode;
 };
 void launch_shift(const ShiftArgsH& a, const RedH& rd, cudaStream_t st);
+// Block methods (k_block.cuh): row-major n x s blocks, s <= 16.
+struct SpmmH {
+  const double* X;
+  double* Y;
+  const double* C;
+  const double* W;
+  double alpha;
+  int mode, s, nd;   // mode 0: Y = alpha A X; 1: Y = C + alpha A X;
+                     // nd dots: (Y, W), (Y, Y)
+};
+struct BlkH {
+  const double* in[4];
+  double* out[2];
+  CfH c[2][4];
+  short mslot[2][4];
+  unsigned char trans[2][4];
+  int nin, nout, s;
+  long long n;
+  int ng;
+  unsigned char gram[2][2];
+  short gslot[2];
+  int nd;
+  unsigned char dot[2][2];
+};
+void launch_spmm(const CsrH& A, const SpmmH& a, const RedH& rd, cudaStream_t st);
+void launch_block(const BlkH& a, const RedH& rd, cudaStream_t st);
+void launch_cm2rm(const double* cm, double* rm, int n, int s, cudaStream_t st);
+void launch_rm2cm(const double* rm, double* cm, int n, int s, cudaStream_t st);
 // Solve start: reset control + ticket, optionally preset S[slot] (slot < 0:
 // none).  Scalar preset without host synchronisation.
 void launch_ctl_init(CtlH* c, unsigned* ticket, double* S, int iter0,

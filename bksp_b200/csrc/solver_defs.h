@@ -64,6 +64,41 @@ enum : short {
   kShBetaS = 27, kShAlphaS = 28, kShRhoNext = 29,
 };
 
+// Block methods: s-by-s matrices (row-major) in cells of 256 slots.
+constexpr short bk_cell(int m) { return (short)(512 + 256 * m); }
+enum : short {
+  kBkS = 30,                  // block width s (as a double)
+  kBkRows = 31,               // block rows n (as a double)
+  kBkG1 = bk_cell(0),         // Gram outputs of block kernels
+  kBkG2 = bk_cell(1),
+  kBkAlpha = bk_cell(2),
+  kBkBeta = bk_cell(3),
+  kBkC = bk_cell(4),          // Block CG's C
+  kBkTmp = bk_cell(5),
+  kBkRinv = bk_cell(6),       // inverse of the last Cholesky-QR factor
+  kBkR = bk_cell(7),          // accumulated R of the running QR
+  kBkLU = bk_cell(8),         // LU of the current s-by-s system
+  kBkPiv = bk_cell(9),        // its pivots
+  kBkXi = bk_cell(10),        // Block BiCGSTAB(l)'s xi
+  kBkGam0 = bk_cell(11),
+  kBkGam1 = bk_cell(12),
+  kBkT = bk_cell(13),
+  kBkTinv = bk_cell(14),
+  kBkXiOld = bk_cell(15),
+  kBkATinv = bk_cell(16),     // alpha * t^-1
+  kBkScr = bk_cell(17),       // scratch
+  kBkScr2 = bk_cell(18),
+};
+
+// Actions run after the third Cholesky-QR pass (E_QR3's a0).
+enum : short {
+  QR_POST_NONE = 0,
+  QR_POST_BCG = 1,        // beta = R, C = beta C, error = ||C||_F / ||B||_F
+  QR_POST_BCG_INIT = 2,   // C = R, beta = I
+  QR_POST_BBL_INIT = 3,   // xi = R
+  QR_POST_BBL_T = 4,      // t = R: xi_old = xi, xi = t xi, t^-1, alpha t^-1
+};
+
 // Epilogue codes.
 enum : short {
   E_NONE = 0,
@@ -86,6 +121,14 @@ enum : short {
   // shifted BiCGSTAB(l) (src/shbicgstabl.c)
   E_SHL_INIT, E_SHL_BETA, E_SHL_ALPHA, E_SHL_ROTATE, E_SHL_TAU, E_SHL_SIG,
   E_SHL_CHECK,
+  // Cholesky-QR passes of the block methods (a0: action after pass 3)
+  E_QR1, E_QR2, E_QR3,
+  // Block CG (src/blcg.c)
+  E_BCG_INIT, E_BCG_ALPHA,
+  // Block BiCGSTAB (src/blbicgstab.c)
+  E_BBS_INIT, E_BBS_ALPHA, E_BBS_OMEGA, E_BBS_BETA,
+  // Block BiCGSTAB(l) (src/blbicgstabl.c)
+  E_BBL_INIT, E_BBL_BETA, E_BBL_ALPHA, E_BBL_CHECK,
   E_COUNT_BASE,
 };
 
