@@ -54,6 +54,11 @@ def args_():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--nx", type=int, default=NX)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--profile", default=None,
+                   choices=["plain_fp64", "mixed_none", "mixed_learned", "spmv"],
+                   help="profiling driver: set up, run one warm solve, then "
+                        "one solve (or SpMV launches) between "
+                        "cudaProfilerStart/Stop, print nothing else")
     return p.parse_args()
 
 
@@ -126,7 +131,8 @@ class Clocks:
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap,"
+         "clocks.mem")
 
     def __init__(self, index):
         self.index = index
@@ -167,8 +173,11 @@ class Clocks:
                  "sw_power_cap"]
         reasons = sorted({names[i] for r in self.rows for i in range(4)
                           if r[5 + i].lower() == "active"})
+        mem = [float(r[9]) for r in self.rows
+               if len(r) > 9 and r[9].replace(".", "").isdigit()]
         return {"sm_mhz": float(np.median(sm)) if sm else None,
                 "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "mem_mhz": float(np.median(mem)) if mem else None,
                 "samples": len(self.rows)}
 
 
@@ -258,6 +267,10 @@ def run_ours(a):
                                  target=TOL_TRUE, precond=precond, model=mdl,
                                  stream=sp)
         return f
+
+    if a.profile:
+        return profile_run(a, torch, G, b, x, sp, plain_step, mixed_step, B, n,
+                           model)
 
     modes = {}
     for name, step in (("plain_fp64", plain_step),
@@ -379,6 +392,38 @@ def run_ours(a):
     model.close()
     if world > 1:
         dist.destroy_process_group()
+    return 0
+
+
+def profile_run(a, torch, G, b, x, sp, plain_step, mixed_step, B, n, model):
+    """One region between cudaProfilerStart/Stop, for ncu
+    (--profile-from-start off)."""
+    if a.profile == "spmv":
+        x64 = torch.rand(n, dtype=torch.float64, device=b.device)
+        y64 = torch.empty_like(x64)
+        x32 = x64.float()
+        y32 = torch.empty_like(x32)
+        for _ in range(3):
+            G.spmv(x64.data_ptr(), y64.data_ptr(), False, sp)
+            G.spmv(x32.data_ptr(), y32.data_ptr(), True, sp)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()
+        for _ in range(3):
+            G.spmv(x64.data_ptr(), y64.data_ptr(), False, sp)
+            G.spmv(x32.data_ptr(), y32.data_ptr(), True, sp)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
+        return 0
+    step = {"plain_fp64": plain_step,
+            "mixed_none": mixed_step(B.PRECOND_NONE),
+            "mixed_learned": mixed_step(B.PRECOND_LEARNED, model)}[a.profile]
+    ret, st = step()          # warm: graph instantiation, features, pools
+    torch.cuda.synchronize()
+    torch.cuda.profiler.start()
+    ret, st = step()
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+    print(f"profiled {a.profile}: ret {ret} launches {st['launches']}", flush=True)
     return 0
 
 

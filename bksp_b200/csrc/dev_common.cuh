@@ -66,7 +66,7 @@ __device__ __forceinline__ float warp_sumf(float v) {
 }
 
 // Scalar epilogue dispatcher (epilogues.cuh).
-static __device__ void run_epilogue(const Red& rd);
+static __device__ __noinline__ void run_epilogue(const Red& rd);
 
 // Block-reduce ND per-thread accumulators, publish the block's partials and
 // let the last-arriving block finish the sums into S[out..] and run the

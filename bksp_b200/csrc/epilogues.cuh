@@ -212,7 +212,7 @@ __device__ __forceinline__ void bl_beta0(double* S, int l, double g1) {
   S[kBlG1] = g1;
 }
 
-static __device__ void run_epilogue(const Red& rd) {
+static __device__ __noinline__ void run_epilogue(const Red& rd) {
   double* S = rd.S;
   const double* D = S + rd.out;
   const int l = (int)S[kL];

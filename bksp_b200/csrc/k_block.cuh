@@ -29,7 +29,7 @@ struct SpmmArgs {
 };
 
 template <int ND>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 8)
 k_spmm(CsrH A, SpmmArgs a, Red rd) {
   if (skip(rd)) return;
   const double* __restrict__ val = static_cast<const double*>(A.val);

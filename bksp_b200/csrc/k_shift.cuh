@@ -33,7 +33,7 @@ struct ShiftArgs {
 };
 
 template <int MODE>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 4)
 k_shift(ShiftArgs a, Red rd) {
   if (skip(rd)) return;
   __shared__ double c0[kMaxShifts], c1[kMaxShifts], c2[kMaxShifts],

@@ -51,7 +51,7 @@ __device__ __forceinline__ void load4<float, float>(const float* val, int kb,
 
 // VT: matrix value type; XT: vector type (the accumulation type is XT).
 template <typename VT, typename XT, int ND>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 8)
 k_spmv(CsrH A, SpmvH<XT> io, Red rd) {
   const VT* __restrict__ Aval = static_cast<const VT*>(A.val);
   if (skip(rd)) return;

@@ -17,7 +17,7 @@
 namespace bk {
 
 template <typename T, int MI, int MO, int ND>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, (MI > 4 ? 4 : 6))
 k_lincomb(const LcH<T> d, Red rd) {
   if (skip(rd)) return;
   using PV = typename Pack<T>::V;
