@@ -99,6 +99,7 @@ def _load():
     L.bksp_gpu_matrix_info.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L.bksp_gpu_solve.argtypes = [vp, i, i, vp, vp, d, i, vp, C.POINTER(Stats)]
     L.bksp_gpu_spmv.argtypes = [vp, i, vp, vp, vp]
+    L.bksp_gpu_matrix_variant.argtypes = [vp, i]
     L.bksp_gpu_true_residual.argtypes = [vp, vp, vp, vp]
     L.bksp_gpu_true_residual.restype = d
     L.bksp_gpu_device_count.restype = i
@@ -341,6 +342,13 @@ class GpuMatrix:
                      "hist_len": st.hist_len, "solve_ms": st.solve_ms,
                      "true_res": st.true_res, "launches": st.launches,
                      "inner_iters": st.inner_iters, "sweeps": st.sweeps}
+
+    SPMV_VARIANTS = {0: "tile", 1: "tma", 2: "vec4", 3: "vec8", 4: "vec16",
+                     5: "vec32", 6: "wtile"}
+
+    def variant(self, v=-1):
+        """Query (v < 0) or set the SpMV kernel variant; returns it."""
+        return lib.bksp_gpu_matrix_variant(self.h, int(v))
 
     def spmv(self, x_ptr, y_ptr, fp32=False, stream=None):
         rc = lib.bksp_gpu_spmv(self.h, int(bool(fp32)), x_ptr, y_ptr, stream)

@@ -102,6 +102,16 @@ int bksp_gpu_matrix_destroy(bksp_gpu_matrix* m) {
   return 0;
 }
 
+int bksp_gpu_matrix_variant(bksp_gpu_matrix* m, int variant) {
+  if (!m) return INVALID_PARAMETERS;
+  if (variant > 6) return INVALID_PARAMETERS;
+  if (variant >= 0) {
+    m->A.variant = variant;
+    m->At.variant = variant;
+  }
+  return m->A.variant;
+}
+
 int bksp_gpu_matrix_info(const bksp_gpu_matrix* m, int* n, int* nnz) {
   if (!m) return INVALID_PARAMETERS;
   if (n) *n = m->A.n;

@@ -60,6 +60,7 @@ struct CsrH {
   const int* rb;
   int n;
   int nrb;
+  int variant;   // SpMV kernel variant (kernels.cu: spmv_dispatch)
 };
 
 // One linear-combination launch: out[o] = sum_i c[o][i] * in[i], terms

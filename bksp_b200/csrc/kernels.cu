@@ -2,11 +2,16 @@
 // scalar epilogues are one device function shared by all reductions) and
 // the host-callable launch wrappers declared in kernel_api.h.
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
+#include <string>
 
 #include "dev_common.cuh"
 #include "epilogues.cuh"
 #include "k_spmv.cuh"
+#include "k_spmv_tma.cuh"
+#include "k_spmv_vec.cuh"
+#include "k_spmv_wtile.cuh"
 #include "k_vec.cuh"
 #include "k_shift.cuh"
 #include "k_block.cuh"
@@ -28,9 +33,93 @@ static inline int grid_for(long long work_items) {
 
 // ------------------------------------------------------------------ SpMV
 
+// SpMV kernel variants (every one sums a row in the reference's order):
+//   0 tile (register-staged products), 1 tile with TMA bulk copies,
+//   2..5 vector CSR with 4, 8, 16, 32 lanes per row, 6 warp tile.
+// CsrH.variant carries the choice made for the operator (autotuner);
+// BKSP_GPU_SPMV=tile|tma|vec4|vec8|vec16|vec32 overrides it.
+static int spmv_override() {
+  static int v = -2;
+  if (v == -2) {
+    const char* e = std::getenv("BKSP_GPU_SPMV");
+    v = -1;
+    if (e) {
+      const std::string s(e);
+      if (s == "tile") v = 0;
+      else if (s == "tma") v = 1;
+      else if (s == "vec4") v = 2;
+      else if (s == "vec8") v = 3;
+      else if (s == "vec16") v = 4;
+      else if (s == "vec32") v = 5;
+      else if (s == "wtile") v = 6;
+    }
+  }
+  return v;
+}
+
+template <typename VT, typename XT, int L>
+static void spmv_vec_launch(const CsrH& A, const SpmvH<XT>& io, const RedH& rd,
+                            cudaStream_t st) {
+  long long g = ((long long)A.n * L + kThreads - 1) / kThreads;
+  if (g > kMaxBlocks) g = kMaxBlocks;
+  if (g < 1) g = 1;
+  switch (io.nd) {
+    case 0: k_spmv_vec<VT, XT, 0, L><<<(int)g, kThreads, 0, st>>>(A, io, rd); break;
+    case 1: k_spmv_vec<VT, XT, 1, L><<<(int)g, kThreads, 0, st>>>(A, io, rd); break;
+    case 2: k_spmv_vec<VT, XT, 2, L><<<(int)g, kThreads, 0, st>>>(A, io, rd); break;
+    default: k_spmv_vec<VT, XT, 3, L><<<(int)g, kThreads, 0, st>>>(A, io, rd); break;
+  }
+}
+
+template <typename VT, typename XT, int ND>
+static void spmv_tma_launch(const CsrH& A, const SpmvH<XT>& io, const RedH& rd,
+                            cudaStream_t st) {
+  const size_t sm = 2 * (size_t)kStageEnt * (sizeof(int) + sizeof(VT));
+  static int attr_dev = -1, per_sm = 1;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (attr_dev != dev) {
+    cudaFuncSetAttribute(k_spmv_tma<VT, XT, ND>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_spmv_tma<VT, XT, ND>,
+                                                  kThreads, sm);
+    if (per_sm < 1) per_sm = 1;
+    attr_dev = dev;
+  }
+  int g = kSMs * per_sm;
+  if (g > kMaxBlocks) g = kMaxBlocks;
+  if (g > A.nrb) g = A.nrb > 0 ? A.nrb : 1;
+  k_spmv_tma<VT, XT, ND><<<g, kThreads, sm, st>>>(A, io, rd);
+}
+
 template <typename VT, typename XT>
 static void spmv_dispatch(const CsrH& A, const SpmvH<XT>& io, const RedH& rd,
                           cudaStream_t st) {
+  int var = spmv_override();
+  if (var < 0) var = A.variant;
+  switch (var) {
+    case 1:
+      switch (io.nd) {
+        case 0: spmv_tma_launch<VT, XT, 0>(A, io, rd, st); return;
+        case 1: spmv_tma_launch<VT, XT, 1>(A, io, rd, st); return;
+        case 2: spmv_tma_launch<VT, XT, 2>(A, io, rd, st); return;
+        default: spmv_tma_launch<VT, XT, 3>(A, io, rd, st); return;
+      }
+    case 2: spmv_vec_launch<VT, XT, 4>(A, io, rd, st); return;
+    case 3: spmv_vec_launch<VT, XT, 8>(A, io, rd, st); return;
+    case 4: spmv_vec_launch<VT, XT, 16>(A, io, rd, st); return;
+    case 5: spmv_vec_launch<VT, XT, 32>(A, io, rd, st); return;
+    case 6: {
+      const int g = A.nrb < kMaxBlocks ? (A.nrb > 0 ? A.nrb : 1) : kMaxBlocks;
+      switch (io.nd) {
+        case 0: k_spmv_wtile<VT, XT, 0><<<g, kThreads, 0, st>>>(A, io, rd); return;
+        case 1: k_spmv_wtile<VT, XT, 1><<<g, kThreads, 0, st>>>(A, io, rd); return;
+        case 2: k_spmv_wtile<VT, XT, 2><<<g, kThreads, 0, st>>>(A, io, rd); return;
+        default: k_spmv_wtile<VT, XT, 3><<<g, kThreads, 0, st>>>(A, io, rd); return;
+      }
+    }
+    default: break;
+  }
   const int g = A.nrb < kMaxBlocks ? (A.nrb > 0 ? A.nrb : 1) : kMaxBlocks;
   switch (io.nd) {
     case 0: k_spmv<VT, XT, 0><<<g, kThreads, 0, st>>>(A, io, rd); break;

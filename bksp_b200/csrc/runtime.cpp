@@ -3,6 +3,8 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstdlib>
+#include <mutex>
+#include <unordered_map>
 
 namespace bk {
 
@@ -149,6 +151,98 @@ std::vector<int> make_row_blocks(int n, const int* rowptr) {
   return rb;
 }
 
+// SpMV variant from the mean row length: vector CSR with the smallest lane
+// count that covers a typical row.
+static int heuristic_variant(int n, int nnz) {
+  const double avg = n > 0 ? (double)nnz / n : 0.0;
+  if (avg <= 4.5) return 2;
+  if (avg <= 9.0) return 3;
+  if (avg <= 18.0) return 4;
+  return 5;
+}
+
+namespace {
+struct TuneKey {
+  int n, nnz, dev;
+  bool fp32;
+  bool operator==(const TuneKey& o) const {
+    return n == o.n && nnz == o.nnz && dev == o.dev && fp32 == o.fp32;
+  }
+};
+struct TuneHash {
+  size_t operator()(const TuneKey& k) const {
+    return ((size_t)k.n * 1000003u) ^ ((size_t)k.nnz * 7919u) ^
+           ((size_t)k.dev << 1) ^ (size_t)k.fp32;
+  }
+};
+std::mutex g_tune_mu;
+std::unordered_map<TuneKey, int, TuneHash> g_tune_cache;
+}  // namespace
+
+// Autotuner: time every SpMV variant on this operator (FP32 values when
+// present, else FP64), keep the fastest; cached per (n, nnz, device).
+// BKSP_GPU_AUTOTUNE=0 keeps the mean-row-length heuristic.
+void autotune_spmv(DevCsr& A, cudaStream_t st) {
+  const char* e = std::getenv("BKSP_GPU_AUTOTUNE");
+  if (e && std::string(e) == "0") return;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const bool f32 = A.v32 != nullptr;
+  const TuneKey key{A.n, A.nnz, dev, f32};
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) {
+      A.variant = it->second;
+      return;
+    }
+  }
+  const long long np = pad64(A.n);
+  const size_t w = f32 ? sizeof(float) : sizeof(double);
+  void* x = dalloc(np * w, st);
+  void* y = dalloc(np * w, st);
+  BK_CHECK(cudaMemsetAsync(x, 0, np * w, st));
+  SolveState ss;
+  ss.create(0, st);
+  ss.start(0, 1, 0.0, st);
+  cudaEvent_t e0, e1;
+  BK_CHECK(cudaEventCreate(&e0));
+  BK_CHECK(cudaEventCreate(&e1));
+  const int cands[] = {6, 0, 1, 2, 3, 4};
+  int best = A.variant;
+  float best_ms = 1e30f;
+  for (int v : cands) {
+    A.variant = v;
+    auto run = [&]() {
+      if (f32)
+        spmv(A, spmv_io<float>(static_cast<const float*>(x), static_cast<float*>(y)),
+             ss.red(kD, E_NONE), st);
+      else
+        spmv(A, spmv_io<double>(static_cast<const double*>(x), static_cast<double*>(y)),
+             ss.red(kD, E_NONE), st);
+    };
+    run();
+    BK_CHECK(cudaEventRecord(e0, st));
+    for (int r = 0; r < 5; ++r) run();
+    BK_CHECK(cudaEventRecord(e1, st));
+    BK_CHECK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    BK_CHECK(cudaEventElapsedTime(&ms, e0, e1));
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = v;
+    }
+  }
+  A.variant = best;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  ss.release(st);
+  dfree(x, st);
+  dfree(y, st);
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune_cache[key] = best;
+}
+
 void upload_csr(int n, const int* rowptr, const int* col, const double* val,
                 bool want_fp32, DevCsr& out, cudaStream_t st) {
   if (n <= 0) throw CudaError("matrix: empty");
@@ -182,6 +276,8 @@ void upload_csr(int n, const int* rowptr, const int* col, const double* val,
     launch_convert_d2f(out.v64, out.v32, padn, st);
     BK_CHECK(cudaGetLastError());
   }
+  out.variant = heuristic_variant(n, nnz);
+  if (n >= (1 << 16)) autotune_spmv(out, st);
 }
 
 void SolveState::create(int cap, cudaStream_t st) {

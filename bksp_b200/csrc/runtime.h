@@ -55,8 +55,9 @@ struct DevCsr {
   double* v64 = nullptr;
   float* v32 = nullptr;
   int* rb = nullptr;
-  CsrH h64() const { return CsrH{rowptr, col, v64, rb, n, nrb}; }
-  CsrH h32() const { return CsrH{rowptr, col, v32, rb, n, nrb}; }
+  int variant = 3;   // SpMV kernel variant chosen for this operator
+  CsrH h64() const { return CsrH{rowptr, col, v64, rb, n, nrb, variant}; }
+  CsrH h32() const { return CsrH{rowptr, col, v32, rb, n, nrb, variant}; }
   void release(cudaStream_t st);
 };
 
@@ -81,7 +82,11 @@ HostCsr transpose(int n, const int* rowptr, const int* col, const double* val);
 void upload_csr(int n, const int* rowptr, const int* col, const double* val,
                 bool want_fp32, DevCsr& out, cudaStream_t st);
 
-// Row-block partition used by the SpMV tile kernel.
+// Pick the fastest SpMV kernel variant for A by timing them (cached per
+// operator signature); called by upload_csr for large operators.
+void autotune_spmv(DevCsr& A, cudaStream_t st);
+
+// Row-block partition used by the SpMV tile kernels.
 std::vector<int> make_row_blocks(int n, const int* rowptr);
 
 // Per-solve device state: scalar slots, control block, reduction scratch,

@@ -103,6 +103,7 @@ DevCsr spai_apply(bksp_gpu_spai_model* model, bksp_gpu_matrix* m, float* mvals,
   v.rowptr = m->A.rowptr;
   v.col = m->A.col;
   v.rb = m->A.rb;
+  v.variant = m->A.variant;
   v.v32 = mvals;
   return v;
 }

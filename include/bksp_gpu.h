@@ -81,6 +81,14 @@ int bksp_gpu_solve(bksp_gpu_matrix *A, int method, int l, const double *b,
                    double *x, double tol, int max_iter, void *stream,
                    bksp_gpu_stats *stats);
 
+/* SpMV kernel variant of the operator: 0 tile, 1 tile with TMA bulk
+ * copies, 2..5 vector CSR with 4, 8, 16, 32 lanes per row, 6 warp tile
+ * (each warp streams and sums its own 32 rows).  variant < 0
+ * queries, otherwise sets.  Returns the variant in use.  The library picks
+ * one by timing all of them when it uploads an operator of >= 65,536
+ * rows (by mean row length below that). */
+int bksp_gpu_matrix_variant(bksp_gpu_matrix *A, int variant);
+
 /* y = A x on the device, FP64 (fp32 = 0) or FP32 vectors and values
  * (fp32 = 1, needs BKSP_GPU_FP32); x and y hold n elements.  Asynchronous
  * on `stream`.  For kernel timing. */

@@ -60,6 +60,48 @@ def test_spmv_bit_exact_vs_reference_order(gpu, testmats):
                                atol=1e-20)
 
 
+@pytest.mark.parametrize("variant", range(7))
+def test_spmv_variants_bit_exact(gpu, testmats, variant):
+    """Every SpMV kernel variant sums rows in the reference's order."""
+    import torch
+    rng = np.random.default_rng(variant)
+    cases = [(testmats["pde_rowptr"], testmats["pde_col"], testmats["pde_val"])]
+    n = 3000                                   # ragged rows, some long
+    lens = rng.integers(0, 40, n)
+    lens[[5, 77]] = [3000, 2049]
+    rp = np.zeros(n + 1, np.int64)
+    np.cumsum(lens, out=rp[1:])
+    cases.append((rp.astype(np.int32), rng.integers(0, n, rp[-1]).astype(np.int32),
+                  rng.uniform(-1, 1, rp[-1])))
+    # Large enough that every CTA of the persistent kernels walks several
+    # row blocks (more row blocks than the grid cap of 148 * 8 CTAs).
+    rp3, c3, v3, n3 = P.convdiff3d(72)
+    assert (n3 + 255) // 256 > 148 * 8
+    cases.append((rp3, c3, v3))
+    for rp, c, v in cases:
+        G = gpu.GpuMatrix(gpu.CsrMatrix(rp, c, v), gpu.FP32)
+        assert G.variant(variant) == variant
+        x = rng.uniform(-1, 1, G.n)
+        ref = _row_sums_sequential(rp, c, v, x)
+        xd = torch.from_numpy(x).cuda()
+        yd = torch.zeros(G.n, dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        G.spmv(xd.data_ptr(), yd.data_ptr(), False)
+        torch.cuda.synchronize()
+        y = yd.cpu().numpy()
+        short = np.diff(rp) <= 2048
+        assert np.array_equal(y[short], ref[short])
+        np.testing.assert_allclose(y, ref, rtol=1e-12, atol=1e-12)
+        x32 = torch.from_numpy(x.astype(np.float32)).cuda()
+        y32 = torch.zeros(G.n, dtype=torch.float32, device="cuda")
+        torch.cuda.synchronize()
+        G.spmv(x32.data_ptr(), y32.data_ptr(), True)
+        torch.cuda.synchronize()
+        ref32 = sp.csr_matrix((v.astype(np.float32), c, rp), shape=(G.n, G.n)) @ x.astype(np.float32)
+        np.testing.assert_allclose(y32.cpu().numpy(), ref32, rtol=2e-5, atol=2e-4)
+        G.close()
+
+
 @pytest.mark.parametrize("nrows,rowlen", [(1, 5000), (3, 2049), (700, 0), (1000, 1)])
 def test_spmv_ragged_and_long_rows(gpu, nrows, rowlen):
     rng = np.random.default_rng(nrows)
