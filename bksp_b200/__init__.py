@@ -284,7 +284,7 @@ def version():
 # ------------------------------------------------------ device-resident API
 
 MIRROR, FP32, TRANSPOSE = 1, 2, 4
-CG, CR, BICG, BICGSTAB, BICGSTABL = 1, 2, 3, 4, 5
+CG, CR, BICG, BICGSTAB, BICGSTABL, BICGSTABL_FAST = 1, 2, 3, 4, 5, 6
 
 
 class GpuMatrix:

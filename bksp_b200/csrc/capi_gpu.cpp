@@ -124,7 +124,9 @@ int bksp_gpu_solve(bksp_gpu_matrix* m, int method, int l, const double* b,
                    bksp_gpu_stats* stats) {
   if (!m || !b || !x) return INVALID_PARAMETERS;
   if (method == BKSP_GPU_BICG && !m->has_t) return INVALID_PARAMETERS;
-  if (method == BKSP_GPU_BICGSTABL && (l < 1 || l > kBlMaxL)) return INVALID_PARAMETERS;
+  if ((method == BKSP_GPU_BICGSTABL || method == BKSP_GPU_BICGSTABL_FAST) &&
+      (l < 1 || l > kBlMaxL))
+    return INVALID_PARAMETERS;
   bksp_gpu_stats* saved = g_stats;
   g_stats = stats;
   int ret = INVALID_PARAMETERS;
@@ -150,6 +152,9 @@ int bksp_gpu_solve(bksp_gpu_matrix* m, int method, int l, const double* b,
       case BKSP_GPU_BICG: o = bk::bicg(m->A, m->At, db, dx, tol, max_iter, ss, st); break;
       case BKSP_GPU_BICGSTAB: o = bk::bicgstab(m->A, db, dx, tol, max_iter, ss, st); break;
       case BKSP_GPU_BICGSTABL: o = bk::bicgstabl(m->A, db, l, dx, tol, max_iter, ss, st); break;
+      case BKSP_GPU_BICGSTABL_FAST:
+        o = bk::bicgstabl(m->A, db, l, dx, tol, max_iter, ss, st, true);
+        break;
       default: throw CudaError("unknown method");
     }
     BK_CHECK(cudaMemcpyAsync(x, dx, sizeof(double) * n, cudaMemcpyDeviceToDevice, st));

@@ -204,6 +204,50 @@ static __device__ void fail_divergence(const Red& rd) {
   rd.ctl->ret = kDivergence;
 }
 
+// One-pass minimal-residual step of BiCGSTAB(l): the modified Gram-Schmidt
+// quantities of src/bicgstabl.c:84-91 (tau_ij, sigma_j, omega'_j) from the
+// Gram matrix G_ij = <r_i, r_j> by an LDL^T recurrence (equal in exact
+// arithmetic), the omega / omega'' back substitution, and the update
+// coefficients mapped from the orthogonalised r'_j back onto r_j
+// (r' = r U^-1 with U unit upper, U_ij = tau_ij).
+static __device__ void blf_mr(double* S, int l) {
+  const int M = l + 1;
+  auto G = [&](int i, int j) {
+    if (i > j) { const int t = i; i = j; j = t; }
+    return S[kGramOut + i * M - i * (i - 1) / 2 + (j - i)];
+  };
+  double* tau = S + kBlTau;
+  double* sig = S + kBlSigma;
+  double* omd = S + kBlOmegaD;
+  double h[kBlMaxL + 1];
+  for (int j = 1; j <= l; ++j) {
+    for (int i = 1; i < j; ++i) {
+      double t = G(i, j);
+      for (int k = 1; k < i; ++k) t -= tau[k * l + i] * sig[k] * tau[k * l + j];
+      tau[i * l + j] = t / sig[i];
+    }
+    double sj = G(j, j);
+    for (int k = 1; k < j; ++k) sj -= tau[k * l + j] * tau[k * l + j] * sig[k];
+    sig[j] = sj;
+    double hj = G(0, j);
+    for (int i = 1; i < j; ++i) hj -= tau[i * l + j] * h[i];
+    h[j] = hj;
+    omd[j] = hj / sj;
+  }
+  bl_back_substitution(S, l);
+  double* cr = S + kBlfCr;
+  double* cx = S + kBlfCx;
+  for (int j = 1; j <= l; ++j) {
+    cr[j] = omd[j];
+    cx[j] = j < l ? S[kBlOmegaDD + j] : 0.0;
+  }
+  for (int i = l - 1; i >= 1; --i)
+    for (int j = i + 1; j <= l; ++j) {
+      cr[i] -= tau[i * l + j] * cr[j];
+      cx[i] -= tau[i * l + j] * cx[j];
+    }
+}
+
 __device__ __forceinline__ void bl_beta0(double* S, int l, double g1) {
   // src/bicgstabl.c:57 gamma0 = -omega[l] gamma0, then :60-62 for j = 0.
   const double g0 = -S[kBlOmega + l] * S[kBlG0];
@@ -316,6 +360,9 @@ static __device__ __noinline__ void run_epilogue(const Red& rd) {
       S[kBlSigma + rd.a1] = D[0];
       S[kBlOmegaD + rd.a1] = D[1] / D[0];
       if (rd.a1 == l) bl_back_substitution(S, l);
+      break;
+    case E_BLF_MR:           // :84-109 in one pass (see blf_mr)
+      blf_mr(S, l);
       break;
     case E_BL_CHECK:         // :122-125, then :57-62 of the next iteration
       conv_check(rd, sqrt(D[0]) / S[kFnb]);

@@ -116,4 +116,38 @@ k_lincomb(const LcH<T> d, Red rd) {
   if (ND > 0 || rd.epi) finish_reduction<ND>(acc, rd);
 }
 
+// All pairwise dot products <v_i, v_j>, i <= j < M, of M vectors in one
+// pass (FP64 accumulation), pair (i, j) reduced into S[out + idx] with idx
+// running over i, then j >= i.  The one-pass minimal-residual step of
+// BiCGSTAB(l) (its Gram matrix of r_0..r_l).
+template <typename T, int M>
+__global__ void __launch_bounds__(kThreads, (M > 5 ? 2 : 4))
+k_gram_vec(const GramH<T> g, Red rd) {
+  if (skip(rd)) return;
+  using PV = typename Pack<T>::V;
+  constexpr int P = Pack<T>::N;
+  constexpr int NP = M * (M + 1) / 2;
+  double acc[NP];
+#pragma unroll
+  for (int q = 0; q < NP; ++q) acc[q] = 0.0;
+  const long long npk = g.n / P;
+  for (long long q = (long long)blockIdx.x * kThreads + threadIdx.x; q < npk;
+       q += (long long)gridDim.x * kThreads) {
+    T v[M][P];
+#pragma unroll
+    for (int i = 0; i < M; ++i) unpack<T>(reinterpret_cast<const PV*>(g.v[i])[q], v[i]);
+    int idx = 0;
+#pragma unroll
+    for (int i = 0; i < M; ++i)
+#pragma unroll
+      for (int j = i; j < M; ++j) {
+        double s = 0.0;
+#pragma unroll
+        for (int e = 0; e < P; ++e) s += (double)v[i][e] * (double)v[j][e];
+        acc[idx++] += s;
+      }
+  }
+  finish_reduction<NP>(acc, rd);
+}
+
 }  // namespace bk

@@ -15,6 +15,7 @@ constexpr int kDivergence = -2;
 constexpr int kLcMaxIn = 24;   // widest linear combination (inputs)
 constexpr int kLcMaxOut = 4;   // widest linear combination (outputs)
 constexpr int kMaxDotsApi = 8;
+constexpr int kPartRows = 64;  // rows of the per-block partials buffer
 constexpr int kTileNnz = 2048;  // SpMV row block: max stored entries
 constexpr int kTileRows = 256;  // SpMV row block: max rows (= threads)
 
@@ -82,6 +83,15 @@ struct LcH {
   unsigned char dot[kMaxDotsApi][2];
 };
 
+// All pairwise dots of m <= kGramMax vectors (k_gram_vec).
+constexpr int kGramMax = 9;
+template <typename T>
+struct GramH {
+  const T* v[kGramMax];
+  long long n;
+  int m;
+};
+
 template <typename T>
 struct SpmvH {
   const T* x;
@@ -108,6 +118,8 @@ void launch_lincomb_d(const LcH<double>& d, const RedH& rd, cudaStream_t st);
 void launch_lincomb_f(const LcH<float>& d, const RedH& rd, cudaStream_t st);
 // Run only a scalar epilogue (one thread).
 void launch_epilogue(const RedH& rd, cudaStream_t st);
+void launch_gram_d(const GramH<double>& g, const RedH& rd, cudaStream_t st);
+void launch_gram_f(const GramH<float>& g, const RedH& rd, cudaStream_t st);
 // Element-wise precision conversions / mixed-precision updates.
 void launch_convert_d2f(const double* a, float* b, long long n, cudaStream_t st);
 void launch_convert_f2d(const float* a, double* b, long long n, cudaStream_t st);

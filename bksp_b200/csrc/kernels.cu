@@ -169,6 +169,30 @@ void launch_lincomb_f(const LcH<float>& d, const RedH& rd, cudaStream_t st) {
   lc_dispatch<float>(d, rd, st);
 }
 
+// ------------------------------------------------------ pairwise Gram
+
+template <typename T>
+static void gram_dispatch(const GramH<T>& g, const RedH& rd, cudaStream_t st) {
+  ++launch_count();
+  const int gr = grid_for(g.n / Pack<T>::N);
+  switch (g.m) {
+    case 2: k_gram_vec<T, 2><<<gr, kThreads, 0, st>>>(g, rd); break;
+    case 3: k_gram_vec<T, 3><<<gr, kThreads, 0, st>>>(g, rd); break;
+    case 4: k_gram_vec<T, 4><<<gr, kThreads, 0, st>>>(g, rd); break;
+    case 5: k_gram_vec<T, 5><<<gr, kThreads, 0, st>>>(g, rd); break;
+    case 6: k_gram_vec<T, 6><<<gr, kThreads, 0, st>>>(g, rd); break;
+    case 7: k_gram_vec<T, 7><<<gr, kThreads, 0, st>>>(g, rd); break;
+    case 8: k_gram_vec<T, 8><<<gr, kThreads, 0, st>>>(g, rd); break;
+    default: k_gram_vec<T, 9><<<gr, kThreads, 0, st>>>(g, rd); break;
+  }
+}
+void launch_gram_d(const GramH<double>& g, const RedH& rd, cudaStream_t st) {
+  gram_dispatch<double>(g, rd, st);
+}
+void launch_gram_f(const GramH<float>& g, const RedH& rd, cudaStream_t st) {
+  gram_dispatch<float>(g, rd, st);
+}
+
 // ----------------------------------------------------------- conversions
 
 __global__ void k_convert_d2f(const double* __restrict__ a, float* __restrict__ b,

@@ -33,6 +33,9 @@ enum : short {
   kBlSigma = 80,      // sigma[0..l]
   kBlTau = 96,        // tau[i*l + j], (l+1)^2 <= 81 entries
   kBlMaxL = 8,
+  kBlfCr = 180,       // one-pass MR: r0 update coefficients on r_1..r_l
+  kBlfCx = 190,       // one-pass MR: x update coefficients on r_1..r_l
+  kGramOut = 300,     // pairwise Gram <r_i, r_j>, i <= j (45 slots)
 };
 
 // Mixed-precision BiCGSTAB(l) (FP32 vectors, FP64 scalars, FP64 reliable
@@ -114,6 +117,7 @@ enum : short {
   // BiCGSTAB(l) (src/bicgstabl.c)
   E_BL_INIT0, E_BL_BETA0, E_BL_ALPHA, E_BL_BETA, E_BL_TAU, E_BL_SIG,
   E_BL_CHECK,
+  E_BLF_MR,         // one-pass minimal-residual step from the Gram matrix
   // mixed-precision BiCGSTAB(l)
   E_MX_INIT, E_MX_INIT2, E_MX_CHECK, E_MX_TRUE, E_MX_REBETA,
   // shifted BiCG (src/shbicg.c)

@@ -5,6 +5,7 @@
 #include "solvers.h"
 
 #include <algorithm>
+#include <cstring>
 
 namespace bk {
 
@@ -264,7 +265,8 @@ SolveOut bicgstab(const DevCsr& A, const double* b, double* x, double tol,
 
 // ---------------------------------------------------------- BiCGSTAB(l)
 SolveOut bicgstabl(const DevCsr& A, const double* b, int l, double* x,
-                   double tol, int max_iter, SolveState& ss, cudaStream_t st) {
+                   double tol, int max_iter, SolveState& ss, cudaStream_t st,
+                   bool fast_mr) {
   SolveOut o;
   if (l < 1 || l > kBlMaxL) throw CudaError("bicgstabl: l out of range");
   const long long np = pad64(A.n);
@@ -332,35 +334,45 @@ SolveOut bicgstabl(const DevCsr& A, const double* b, int l, double* x,
           }
         }
       }
-      // ---- MR part, :84-109 (modified Gram-Schmidt on r_1..r_l)
-      for (int j = 1; j <= l; ++j) {
-        if (j == 1) {
-          Lc<double> u(np);
-          const int i1 = u.in(R(1)), i0 = u.in(R(0));
-          u.dot(i1, i1).dot(i0, i1);
-          u.launch(ss.red(kD, E_BL_SIG, 0, 1), s);
-          continue;
-        }
-        {
-          Lc<double> u(np);
-          const int ij = u.in(R(j)), i1 = u.in(R(1));
-          u.dot(ij, i1);
-          u.launch(ss.red(kD, E_BL_TAU, 1, (short)j), s);
-        }
-        for (int i = 1; i < j; ++i) {
-          Lc<double> u(np);
-          const int ij = u.in(R(j)), ii = u.in(R(i));
-          const int oj = u.out(R(j));
-          u.term(oj, ij, cf_const(1))
-              .term(oj, ii, cf_slot((short)(kBlTau + i * l + j), -1));
-          if (i + 1 < j) {
-            const int in = u.in(R(i + 1));
-            u.dot(OUT + oj, in);
-            u.launch(ss.red(kD, E_BL_TAU, (short)(i + 1), (short)j), s);
-          } else {
-            const int i0 = u.in(R(0));
-            u.dot(OUT + oj, OUT + oj).dot(i0, OUT + oj);
-            u.launch(ss.red(kD, E_BL_SIG, 0, (short)j), s);
+      // ---- MR part, :84-109
+      if (fast_mr) {
+        GramH<double> g;
+        std::memset(&g, 0, sizeof(g));
+        for (int i = 0; i <= l; ++i) g.v[i] = R(i);
+        g.n = np;
+        g.m = l + 1;
+        launch_gram_d(g, ss.red(kGramOut, E_BLF_MR), s);
+      } else {
+        // modified Gram-Schmidt on r_1..r_l, as the reference
+        for (int j = 1; j <= l; ++j) {
+          if (j == 1) {
+            Lc<double> u(np);
+            const int i1 = u.in(R(1)), i0 = u.in(R(0));
+            u.dot(i1, i1).dot(i0, i1);
+            u.launch(ss.red(kD, E_BL_SIG, 0, 1), s);
+            continue;
+          }
+          {
+            Lc<double> u(np);
+            const int ij = u.in(R(j)), i1 = u.in(R(1));
+            u.dot(ij, i1);
+            u.launch(ss.red(kD, E_BL_TAU, 1, (short)j), s);
+          }
+          for (int i = 1; i < j; ++i) {
+            Lc<double> u(np);
+            const int ij = u.in(R(j)), ii = u.in(R(i));
+            const int oj = u.out(R(j));
+            u.term(oj, ij, cf_const(1))
+                .term(oj, ii, cf_slot((short)(kBlTau + i * l + j), -1));
+            if (i + 1 < j) {
+              const int in = u.in(R(i + 1));
+              u.dot(OUT + oj, in);
+              u.launch(ss.red(kD, E_BL_TAU, (short)(i + 1), (short)j), s);
+            } else {
+              const int i0 = u.in(R(0));
+              u.dot(OUT + oj, OUT + oj).dot(i0, OUT + oj);
+              u.launch(ss.red(kD, E_BL_SIG, 0, (short)j), s);
+            }
           }
         }
       }
@@ -374,14 +386,22 @@ SolveOut bicgstabl(const DevCsr& A, const double* b, int l, double* x,
         const int irs = u.in(rs);
         const int ox = u.out(x), orr = u.out(R(0)), op = u.out(P(0));
         u.term(ox, ix, cf_const(1)).term(ox, ir[0], cf_slot(kBlOmega + 1));
-        u.term(orr, ir[0], cf_const(1))
-            .term(orr, ir[l], cf_slot((short)(kBlOmegaD + l), -1));
+        u.term(orr, ir[0], cf_const(1));
         u.term(op, ip[0], cf_const(1))
             .term(op, ip[l], cf_slot((short)(kBlOmega + l), -1));
-        for (int i = 1; i < l; ++i) {
+        for (int i = 1; i < l; ++i)
           u.term(op, ip[i], cf_slot((short)(kBlOmega + i), -1));
-          u.term(orr, ir[i], cf_slot((short)(kBlOmegaD + i), -1));
-          u.term(ox, ir[i], cf_slot((short)(kBlOmegaDD + i)));
+        if (fast_mr) {       // coefficients on the unorthogonalised r_i
+          for (int i = 1; i <= l; ++i) {
+            u.term(orr, ir[i], cf_slot((short)(kBlfCr + i), -1));
+            u.term(ox, ir[i], cf_slot((short)(kBlfCx + i)));
+          }
+        } else {
+          u.term(orr, ir[l], cf_slot((short)(kBlOmegaD + l), -1));
+          for (int i = 1; i < l; ++i) {
+            u.term(orr, ir[i], cf_slot((short)(kBlOmegaD + i), -1));
+            u.term(ox, ir[i], cf_slot((short)(kBlOmegaDD + i)));
+          }
         }
         u.dot(OUT + orr, OUT + orr).dot(irs, OUT + orr);
         u.launch(ss.red(kD, E_BL_CHECK), s);

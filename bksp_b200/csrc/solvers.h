@@ -22,8 +22,11 @@ SolveOut bicg(const DevCsr& A, const DevCsr& At, const double* b, double* x,
               double tol, int max_iter, SolveState& ss, cudaStream_t st);
 SolveOut bicgstab(const DevCsr& A, const double* b, double* x, double tol,
                   int max_iter, SolveState& ss, cudaStream_t st);
+// fast_mr: the minimal-residual step from one Gram pass (blf_mr) instead
+// of the reference's modified Gram-Schmidt sweeps.
 SolveOut bicgstabl(const DevCsr& A, const double* b, int l, double* x,
-                   double tol, int max_iter, SolveState& ss, cudaStream_t st);
+                   double tol, int max_iter, SolveState& ss, cudaStream_t st,
+                   bool fast_mr = false);
 
 // Shifted methods: x holds (ns + 1) padded vectors (seed first), the
 // shifted parts zero on entry (the reference's assumption).
@@ -42,6 +45,7 @@ struct MixedOpts {
   double target = 1e-8;   // FP64 true relative residual to reach
   double delta = 1e-3;    // replacement when the recursive residual fell by delta
   int period = 6;         // ... or every `period` outer iterations
+  bool fast_mr = true;    // one-pass minimal-residual step
 };
 struct MixedOut : SolveOut {
   int replacements = 0;

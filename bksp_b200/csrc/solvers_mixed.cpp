@@ -12,6 +12,7 @@
 //     captured iteration, behind a device-side guard;
 //   * convergence is decided on that FP64 true residual only.
 #include <algorithm>
+#include <cstring>
 
 #include "solvers.h"
 
@@ -111,35 +112,45 @@ MixedOut bicgstabl_mixed(const DevCsr& A, const DevCsr* M, const double* b,
       }
       op(R(j), R(j + 1), j + 1 < l, j + 1 < l ? E_BL_BETA : E_NONE, s);
     }
-    // MR part (modified Gram-Schmidt), FP64 dots of FP32 vectors.
-    for (int j = 1; j <= l; ++j) {
-      if (j == 1) {
-        Lc<float> u(np);
-        const int i1 = u.in(R(1)), i0 = u.in(R(0));
-        u.dot(i1, i1).dot(i0, i1);
-        u.launch(ss.red(kD, E_BL_SIG, 0, 1), s);
-        continue;
-      }
-      {
-        Lc<float> u(np);
-        const int ij = u.in(R(j)), i1 = u.in(R(1));
-        u.dot(ij, i1);
-        u.launch(ss.red(kD, E_BL_TAU, 1, (short)j), s);
-      }
-      for (int i = 1; i < j; ++i) {
-        Lc<float> u(np);
-        const int ij = u.in(R(j)), ii = u.in(R(i));
-        const int oj = u.out(R(j));
-        u.term(oj, ij, cf_const(1))
-            .term(oj, ii, cf_slot((short)(kBlTau + i * l + j), -1));
-        if (i + 1 < j) {
-          const int in = u.in(R(i + 1));
-          u.dot(OUT + oj, in);
-          u.launch(ss.red(kD, E_BL_TAU, (short)(i + 1), (short)j), s);
-        } else {
-          const int i0 = u.in(R(0));
-          u.dot(OUT + oj, OUT + oj).dot(i0, OUT + oj);
-          u.launch(ss.red(kD, E_BL_SIG, 0, (short)j), s);
+    // MR part, FP64 dots of FP32 vectors.
+    if (o.fast_mr) {
+      GramH<float> g;
+      std::memset(&g, 0, sizeof(g));
+      for (int i = 0; i <= l; ++i) g.v[i] = R(i);
+      g.n = np;
+      g.m = l + 1;
+      launch_gram_f(g, ss.red(kGramOut, E_BLF_MR), s);
+    } else {
+      // modified Gram-Schmidt, as the reference
+      for (int j = 1; j <= l; ++j) {
+        if (j == 1) {
+          Lc<float> u(np);
+          const int i1 = u.in(R(1)), i0 = u.in(R(0));
+          u.dot(i1, i1).dot(i0, i1);
+          u.launch(ss.red(kD, E_BL_SIG, 0, 1), s);
+          continue;
+        }
+        {
+          Lc<float> u(np);
+          const int ij = u.in(R(j)), i1 = u.in(R(1));
+          u.dot(ij, i1);
+          u.launch(ss.red(kD, E_BL_TAU, 1, (short)j), s);
+        }
+        for (int i = 1; i < j; ++i) {
+          Lc<float> u(np);
+          const int ij = u.in(R(j)), ii = u.in(R(i));
+          const int oj = u.out(R(j));
+          u.term(oj, ij, cf_const(1))
+              .term(oj, ii, cf_slot((short)(kBlTau + i * l + j), -1));
+          if (i + 1 < j) {
+            const int in = u.in(R(i + 1));
+            u.dot(OUT + oj, in);
+            u.launch(ss.red(kD, E_BL_TAU, (short)(i + 1), (short)j), s);
+          } else {
+            const int i0 = u.in(R(0));
+            u.dot(OUT + oj, OUT + oj).dot(i0, OUT + oj);
+            u.launch(ss.red(kD, E_BL_SIG, 0, (short)j), s);
+          }
         }
       }
     }
@@ -152,14 +163,22 @@ MixedOut bicgstabl_mixed(const DevCsr& A, const DevCsr* M, const double* b,
       const int irs = u.in(rs);
       const int oy = u.out(y), orr = u.out(R(0)), op_ = u.out(P(0));
       u.term(oy, iy, cf_const(1)).term(oy, ir[0], cf_slot(kBlOmega + 1));
-      u.term(orr, ir[0], cf_const(1))
-          .term(orr, ir[l], cf_slot((short)(kBlOmegaD + l), -1));
+      u.term(orr, ir[0], cf_const(1));
       u.term(op_, ip[0], cf_const(1))
           .term(op_, ip[l], cf_slot((short)(kBlOmega + l), -1));
-      for (int i = 1; i < l; ++i) {
+      for (int i = 1; i < l; ++i)
         u.term(op_, ip[i], cf_slot((short)(kBlOmega + i), -1));
-        u.term(orr, ir[i], cf_slot((short)(kBlOmegaD + i), -1));
-        u.term(oy, ir[i], cf_slot((short)(kBlOmegaDD + i)));
+      if (o.fast_mr) {     // coefficients on the unorthogonalised r_i
+        for (int i = 1; i <= l; ++i) {
+          u.term(orr, ir[i], cf_slot((short)(kBlfCr + i), -1));
+          u.term(oy, ir[i], cf_slot((short)(kBlfCx + i)));
+        }
+      } else {
+        u.term(orr, ir[l], cf_slot((short)(kBlOmegaD + l), -1));
+        for (int i = 1; i < l; ++i) {
+          u.term(orr, ir[i], cf_slot((short)(kBlOmegaD + i), -1));
+          u.term(oy, ir[i], cf_slot((short)(kBlOmegaDD + i)));
+        }
       }
       u.dot(OUT + orr, OUT + orr).dot(irs, OUT + orr);
       u.launch(ss.red(kD, E_MX_CHECK), s);

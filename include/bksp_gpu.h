@@ -70,7 +70,12 @@ enum {
     BKSP_GPU_CR = 2,
     BKSP_GPU_BICG = 3,
     BKSP_GPU_BICGSTAB = 4,
-    BKSP_GPU_BICGSTABL = 5
+    BKSP_GPU_BICGSTABL = 5,
+    /* BiCGSTAB(l) whose minimal-residual step is computed from one pass
+     * over r_0..r_l (their Gram matrix, LDL^T on the device) instead of
+     * the reference's modified Gram-Schmidt sweeps: the same recurrence in
+     * exact arithmetic, fewer passes over memory. */
+    BKSP_GPU_BICGSTABL_FAST = 6
 };
 
 /* The bksp.h methods on device-resident data: b and x are device pointers

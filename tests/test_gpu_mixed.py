@@ -143,3 +143,25 @@ def test_checkpoint_roundtrip_and_host_api(gpu, trained, tmp_path):
     ret = B.dbicgstabl_mixed(B.CsrMatrix(rp, c, v), b, x, l=4, target=1e-8,
                              precond=2, model=loaded)
     assert ret >= 0 and S.true_residual(A, b, x) <= 1e-8
+
+
+@pytest.mark.parametrize("fast", [False, True])
+def test_one_pass_mr_matches_mgs(gpu, torch_cuda, golden, fast):
+    """BiCGSTAB(l) with the one-pass (Gram) minimal-residual step follows the
+    reference's iteration as closely as the MGS form does."""
+    B, torch = gpu, torch_cuda
+    rp, c, v, n, A, b = _system(P.convdiff3d, 24)
+    G = B.GpuMatrix(B.CsrMatrix(rp, c, v), B.FP32)
+    bd = _dev(torch, b)
+    for l in (1, 2, 4):
+        xd = torch.zeros(n, dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        ret, st = G.solve(B.BICGSTABL_FAST if fast else B.BICGSTABL,
+                          bd.data_ptr(), xd.data_ptr(), 1e-10, 2000, l=l,
+                          hist_cap=500)
+        gk = golden[f"cfg2/bicgstabl{l}_cd24"]
+        assert abs(ret - gk["ret"]) <= 2, (l, ret, gk["ret"])
+        k = min(10, len(gk["hist"]))
+        np.testing.assert_allclose(st["hist"][:k], gk["hist"][:k], rtol=1e-6)
+        assert S.true_residual(A, b, xd.cpu().numpy()) < 1e-9
+    G.close()
