@@ -65,6 +65,15 @@ k_spmv(CsrH A, SpmvH<XT> io, Red rd) {
   for (int blk = blockIdx.x; blk < A.nrb; blk += gridDim.x) {
     const int r0 = A.rb[blk], r1 = A.rb[blk + 1];
     const int k0 = __ldg(A.rowptr + r0), k1 = __ldg(A.rowptr + r1);
+    // This thread's epilogue operands (b, w0, w1 of its row), loaded now so
+    // their latency overlaps the tile's loads instead of following them.
+    XT bv = XT(0), w0 = XT(0), w1 = XT(0);
+    if (tid < r1 - r0) {
+      const int myrow = r0 + tid;
+      if (io.b) bv = io.b[myrow];
+      if (ND > 0 && io.w0) w0 = io.w0[myrow];
+      if (ND > 0 && io.w1) w1 = io.w1[myrow];
+    }
     XT sum = XT(0);
     int row = -1;
     if (r1 - r0 == 1 && k1 - k0 > kTileNnz) {
@@ -109,14 +118,11 @@ k_spmv(CsrH A, SpmvH<XT> io, Red rd) {
       __syncthreads();
     }
     if (row >= 0) {
-      XT y = sum, bv = XT(0), w0 = XT(0), w1 = XT(0);
-      if (io.b) bv = io.b[row];
+      XT y = sum;
       if (io.mode == 1) y = add_rn(bv, -sum);
       io.y[row] = y;
       if (io.y2) io.y2[row] = y;
       if (ND > 0) {
-        if (io.w0) w0 = io.w0[row];
-        if (io.w1) w1 = io.w1[row];
 #pragma unroll
         for (int d = 0; d < ND; ++d)
           acc[d] += (double)spmv_operand(io.dot[d][0], y, bv, w0, w1) *

@@ -13,7 +13,7 @@ constexpr int kGridCap = 148 * 8; // reduction grid cap (= kMaxBlocks)
 constexpr int kNotConverged = -1;
 constexpr int kDivergence = -2;
 constexpr int kLcMaxIn = 24;   // widest linear combination (inputs)
-constexpr int kLcMaxOut = 4;   // widest linear combination (outputs)
+constexpr int kLcMaxOut = 6;   // widest linear combination (outputs)
 constexpr int kMaxDotsApi = 8;
 constexpr int kPartRows = 64;  // rows of the per-block partials buffer
 constexpr int kTileNnz = 2048;  // SpMV row block: max stored entries

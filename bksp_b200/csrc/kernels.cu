@@ -157,7 +157,9 @@ template <typename T>
 static void lc_dispatch(const LcH<T>& d, const RedH& rd, cudaStream_t st) {
   if (d.nin <= 4 && d.nout <= 2) lc_nd<T, 4, 2>(d, rd, st);
   else if (d.nin <= 8 && d.nout <= 4) lc_nd<T, 8, 4>(d, rd, st);
-  else lc_nd<T, 24, 4>(d, rd, st);
+  else if (d.nout <= 4) lc_nd<T, 24, 4>(d, rd, st);
+  else if (d.nin <= 16) lc_nd<T, 16, 6>(d, rd, st);
+  else lc_nd<T, 24, 6>(d, rd, st);
 }
 
 void launch_lincomb_d(const LcH<double>& d, const RedH& rd, cudaStream_t st) {

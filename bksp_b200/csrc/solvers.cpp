@@ -308,20 +308,35 @@ SolveOut bicgstabl(const DevCsr& A, const double* b, int l, double* x,
           set_dot(a, 0, W0, Y);
           spmv(A, a, ss.red(kD, E_BL_ALPHA), s);
         }
-        {  // :73-75  r_i -= alpha p_{i+1}, i = 0..j
+        if (j + 2 <= kLcMaxOut) {
+          // :73-75 and :79 in one pass: r_i -= alpha p_{i+1} (i <= j),
+          // x += alpha p_0
           Lc<double> u(np);
-          const int ir = u.in(R(0), true), ip = u.in(P(1), true);
-          const int orr = u.out(R(0), true);
-          u.term(orr, ir, cf_const(1)).term(orr, ip, cf_slot(kBlAlpha, -1));
-          u.batch(j + 1, np);
-          u.launch(ss.red(kD, E_NONE), s);
-        }
-        {  // :79  x += alpha p_0
-          Lc<double> u(np);
-          const int ix = u.in(x), ip = u.in(P(0));
+          const int ix = u.in(x), ip0 = u.in(P(0));
           const int ox = u.out(x);
-          u.term(ox, ix, cf_const(1)).term(ox, ip, cf_slot(kBlAlpha));
+          u.term(ox, ix, cf_const(1)).term(ox, ip0, cf_slot(kBlAlpha));
+          for (int i = 0; i <= j; ++i) {
+            const int ir = u.in(R(i)), ip = u.in(P(i + 1));
+            const int orr = u.out(R(i));
+            u.term(orr, ir, cf_const(1)).term(orr, ip, cf_slot(kBlAlpha, -1));
+          }
           u.launch(ss.red(kD, E_NONE), s);
+        } else {
+          {  // :73-75  r_i -= alpha p_{i+1}, i = 0..j
+            Lc<double> u(np);
+            const int ir = u.in(R(0), true), ip = u.in(P(1), true);
+            const int orr = u.out(R(0), true);
+            u.term(orr, ir, cf_const(1)).term(orr, ip, cf_slot(kBlAlpha, -1));
+            u.batch(j + 1, np);
+            u.launch(ss.red(kD, E_NONE), s);
+          }
+          {  // :79  x += alpha p_0
+            Lc<double> u(np);
+            const int ix = u.in(x), ip = u.in(P(0));
+            const int ox = u.out(x);
+            u.term(ox, ix, cf_const(1)).term(ox, ip, cf_slot(kBlAlpha));
+            u.launch(ss.red(kD, E_NONE), s);
+          }
         }
         {  // :76  r_{j+1} = A r_j (+ (rs, r_{j+1}) for the next j, :60)
           SpmvH<double> a = spmv_io<double>(R(j), R(j + 1));

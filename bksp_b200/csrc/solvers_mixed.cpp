@@ -97,7 +97,18 @@ MixedOut bicgstabl_mixed(const DevCsr& A, const DevCsr* M, const double* b,
         u.launch(ss.red(kD, E_NONE), s);
       }
       op(P(j), P(j + 1), true, E_BL_ALPHA, s);
-      {  // r_i -= alpha p_{i+1}; y += alpha p_0
+      if (j + 2 <= kLcMaxOut) {   // r_i -= alpha p_{i+1}, y += alpha p_0
+        Lc<float> u(np);
+        const int iy = u.in(y), ip0 = u.in(P(0));
+        const int oy = u.out(y);
+        u.term(oy, iy, cf_const(1)).term(oy, ip0, cf_slot(kBlAlpha));
+        for (int i = 0; i <= j; ++i) {
+          const int ir = u.in(R(i)), ip = u.in(P(i + 1));
+          const int orr = u.out(R(i));
+          u.term(orr, ir, cf_const(1)).term(orr, ip, cf_slot(kBlAlpha, -1));
+        }
+        u.launch(ss.red(kD, E_NONE), s);
+      } else {
         Lc<float> u(np);
         const int ir = u.in(R(0), true), ip = u.in(P(1), true);
         const int orr = u.out(R(0), true);
