@@ -54,6 +54,11 @@ def args_():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--nx", type=int, default=NX)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--workload", default="convdiff3d",
+                   choices=["convdiff3d", "kappa_batch"],
+                   help="kappa_batch: the batched workload (64 kappa-diffusion "
+                        "systems, BiCGSTAB(2)), one JSON line of its own")
+    p.add_argument("--batch-count", type=int, default=64)
     p.add_argument("--profile", default=None,
                    choices=["plain_fp64", "mixed_none", "mixed_learned", "spmv"],
                    help="profiling driver: set up, run one warm solve, then "
@@ -329,10 +334,21 @@ def run_ours(a):
     kern = {"spmv_fp64": variants[G.SPMV_VARIANTS[tuned]]["fp64_ms"],
             "spmv_fp32": variants[G.SPMV_VARIANTS[tuned]]["fp32_ms"]}
     wv = 8 if mode == "plain_fp64" else 4
-    kname = "spmv_fp64" if wv == 8 else "spmv_fp32"
-    alg_bytes = nnz * (wv + 4) + 4 * (n + 1) + 2 * wv * n
+    fp = "fp64" if wv == 8 else "fp32"
+    vname = G.SPMV_VARIANTS[tuned]
+    kname = f"spmv_{vname}_{fp}"
+    ndia = len(G.diagonals())
+    if vname == "dia" and ndia:
+        # Diagonal form: the stored diagonals (zero where a row lacks one),
+        # one mask byte per row, x and y once.
+        alg_bytes = ndia * wv * n + n + 2 * wv * n
+    else:
+        # CSR: values + column indices, row pointers, x and y once.
+        alg_bytes = nnz * (wv + 4) + 4 * (n + 1) + 2 * wv * n
+    csr_bytes = nnz * (wv + 4) + 4 * (n + 1) + 2 * wv * n
     peak, peak_kind = peaks()
-    achieved = alg_bytes / (kern[kname] * 1e-3) / 1e9
+    launch_ms = kern["spmv_" + fp]
+    achieved = alg_bytes / (launch_ms * 1e-3) / 1e9
     traffic = None
     try:
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
@@ -350,18 +366,22 @@ def run_ours(a):
     _, b_p = pinned(b_h)
     xt_, x_p = pinned(np.zeros(n))
     Ap = B.CsrMatrix(rp_p, c_p, v_p)
-    e2e_ms = []
+    e2e_ms, e2e_rets = [], []
     for i in range(a.warmup + a.steps):
         x_p[:] = 0.0
         if world > 1:
             dist.barrier()
-        t0 = time.perf_counter()
-        r_e2e = B.dbicgstabl_mixed(Ap, b_p, x_p, l=L_DEG, target=TOL_TRUE,
-                                   precond=B.PRECOND_LEARNED, model=model)
-        dt = time.perf_counter() - t0
+        with B.record() as st_e:
+            t0 = time.perf_counter()
+            r_e2e = B.dbicgstabl_mixed(Ap, b_p, x_p, l=L_DEG, target=TOL_TRUE,
+                                       precond=B.PRECOND_LEARNED, model=model)
+            dt = time.perf_counter() - t0
+        e2e_rets.append(r_e2e)
         if i >= a.warmup:
             e2e_ms.append(dt * 1e3)
     e2e_s = max_over_ranks(float(np.mean(e2e_ms))) / 1e3
+    e2e_true = float(np.linalg.norm(b_h - P.csr_matvec(rp, c, v, x_p)) /
+                     np.linalg.norm(b_h))
     # CSR operator (FP64 values), b, x0, and the learned preconditioner's
     # per-row slot map (8 int32 per row) built on the host at upload.
     h2d = 4 * (n + 1) + 12 * nnz + 16 * n + 32 * n
@@ -388,13 +408,15 @@ def run_ours(a):
                               "systems": "convdiff3d 12^3, 16^3, 24^3",
                               "epochs": 200, "probes": 8},
             "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": h2d,
-                    "d2h_bytes_per_step": d2h, "ret": r_e2e},
+                    "d2h_bytes_per_step": d2h, "ret": r_e2e, "rets": e2e_rets,
+                    "iters": st_e.get("hist_len"), "true_residual": e2e_true},
             "roofline": {"bound": "hbm", "kernel": kname,
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": traffic, "alg_bytes": alg_bytes,
-                         "launch_ms": kern[kname],
-                         "variant": G.SPMV_VARIANTS[tuned],
+                         "csr_alg_bytes": csr_bytes,
+                         "launch_ms": launch_ms,
+                         "variant": vname, "diagonals": ndia,
                          "spmv_variants_ms": variants},
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
@@ -462,10 +484,133 @@ def cpu_baseline(rp, c, v, n, b):
                 "sample": f"failed: {e}"}
 
 
+def run_batch(a):
+    """The batched workload: 64 systems -div(kappa grad u) = f, 7-point
+    finite volumes on L^3 grids, L ~ U{32..96} (seed 4), kappa = exp(GRF),
+    f ~ N(0,1); time to an FP64 true relative residual of 1e-8 on every
+    system.  value: mixed-precision BiCGSTAB(2) with the learned SPAI
+    preconditioner (trained beforehand on 64 smaller systems of the same
+    family, seeds 1000+i), all systems in one batched call; plain_fp64_s:
+    FP64 BiCGSTAB(2) on the Jacobi right-scaled systems A D^-1 y = b, x = D^-1 y,
+    batched the same way; sequential_s: the learned solve one system at a
+    time."""
+    import torch
+    import bksp_b200 as B
+    from bksp_b200 import problems as P
+    torch.cuda.set_device(0)
+    t0 = time.perf_counter()
+    systems = P.kappa_batch(count=a.batch_count)
+    gen_s = time.perf_counter() - t0
+    ntot = sum(s[3] for s in systems)
+    nnz = sum(int(s[0][-1]) for s in systems)
+    t0 = time.perf_counter()
+    mats = [B.GpuMatrix(B.CsrMatrix(rp, c, v), B.FP32) for rp, c, v, n, b in systems]
+    dev = torch.device("cuda", 0)
+    bs = [torch.from_numpy(s[4]).to(dev) for s in systems]
+    xs = [torch.zeros_like(b) for b in bs]
+    # Jacobi right-scaled copies for the FP64 comparator.
+    scaled, dinv = [], []
+    for rp, c, v, n, b in systems:
+        rows = np.repeat(np.arange(n), np.diff(rp))
+        d = np.zeros(n)
+        d[rows[c == rows]] = v[c == rows]
+        scaled.append(B.GpuMatrix(B.CsrMatrix(rp, c, v / d[c])))
+        dinv.append(torch.from_numpy(1.0 / d).to(dev))
+    upload_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    model = B.SpaiModel(seed=3)
+    Ls = np.random.default_rng(999).integers(16, 33, 64)
+    train = [B.GpuMatrix(B.CsrMatrix(*P.kappa_diffusion3d(int(L), 1000 + i)[:3]), B.FP32)
+             for i, L in enumerate(Ls)]
+    loss = model.train(train, epochs=100, probes=8, lr=3e-3, seed=7)
+    for m in train:
+        m.close()
+    train_s = time.perf_counter() - t0
+    torch.cuda.synchronize()
+
+    def timed(fn, k):
+        ms, last = [], None
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        for _ in range(k):
+            for x in xs:
+                x.zero_()
+            torch.cuda.synchronize()
+            e0.record()
+            last = fn()
+            e1.record()
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        return float(np.mean(ms)), last
+
+    def learned(workers=0):
+        return lambda: B.solve_mixed_batch(mats, [b.data_ptr() for b in bs],
+                                           [x.data_ptr() for x in xs], l=2,
+                                           target=TOL_TRUE, precond=B.PRECOND_LEARNED,
+                                           model=model, workers=workers)
+
+    def plain():
+        return B.solve_batch(scaled, B.BICGSTABL_FAST, [b.data_ptr() for b in bs],
+                             [x.data_ptr() for x in xs], TOL_TRUE, 20000, l=2)
+
+    def worst_true_res(scale):
+        w = 0.0
+        for (rp, c, v, n, b), x, di in zip(systems, xs, dinv):
+            xh = (x * di if scale else x).cpu().numpy()
+            r = b - P.csr_matvec(rp, c, v, xh)
+            w = max(w, float(np.linalg.norm(r) / np.linalg.norm(b)))
+        return w
+
+    res = {}
+    for name, fn, k, scale in (("plain_fp64", plain, a.steps, True),
+                               ("mixed_learned_sequential", learned(1), 1, False),
+                               ("mixed_learned", learned(), a.steps, False)):
+        for _ in range(a.warmup if k > 1 else 0):
+            for x in xs:
+                x.zero_()
+            fn()
+        if name == "mixed_learned":
+            with Clocks(0) as clk:
+                ms, (ret, st) = timed(fn, k)
+        else:
+            ms, (ret, st) = timed(fn, k)
+        its = [s["hist_len"] for s in st]
+        res[name] = {"s": ms / 1e3, "ret": ret, "worst_true_residual": worst_true_res(scale),
+                     "iters_min": min(its), "iters_max": max(its),
+                     "iters_mean": float(np.mean(its)),
+                     "launches": int(sum(s["launches"] for s in st))}
+    line = {
+        "metric": "time to 1e-8 FP64 true residual on every system of the batch",
+        "value": res["mixed_learned"]["s"], "unit": "s", "n_gpus": 1,
+        "steps": a.steps, "warmup": a.warmup,
+        "ms_per_step": res["mixed_learned"]["s"] * 1e3, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+        "config": {"workload": f"kappa_batch_{a.batch_count}", "systems": a.batch_count,
+                   "rows": ntot, "nnz": nnz, "l": 2, "edge": "U{32..96} seed 4",
+                   "kappa": "exp(GRF), corr 0.1, var 1", "rhs": "N(0,1)",
+                   "l2": "inputs larger than L2 (FP64 CSR %.0f MB)" % ((nnz * 12 + 4 * ntot) / 1e6)},
+        "plain_fp64_s": res["plain_fp64"]["s"],
+        "speedup_vs_plain_fp64": res["plain_fp64"]["s"] / res["mixed_learned"]["s"],
+        "modes": res,
+        "spai_training": {"s": train_s, "final_loss": loss, "systems": "64 kappa, L U{16..32}",
+                          "epochs": 100, "probes": 8},
+        "setup_s": {"generate": gen_s, "upload": upload_s},
+        "clocks": clk.summary(),
+        "gpu_launches": res["mixed_learned"]["launches"],
+    }
+    print(json.dumps(line), flush=True)
+    for m in mats + scaled:
+        m.close()
+    model.close()
+    return 0
+
+
 def main():
     a = args_()
     if a.impl == "reference":
         return run_reference(a)
+    if a.workload == "kappa_batch":
+        return run_batch(a)
     return run_ours(a)
 
 

@@ -100,12 +100,20 @@ def _load():
     L.bksp_gpu_solve.argtypes = [vp, i, i, vp, vp, d, i, vp, C.POINTER(Stats)]
     L.bksp_gpu_spmv.argtypes = [vp, i, vp, vp, vp]
     L.bksp_gpu_matrix_variant.argtypes = [vp, i]
+    L.bksp_gpu_matrix_diagonals.argtypes = [vp, C.POINTER(C.c_int)]
     L.bksp_gpu_true_residual.argtypes = [vp, vp, vp, vp]
     L.bksp_gpu_true_residual.restype = d
     L.bksp_gpu_device_count.restype = i
     L.bksp_gpu_solve_mixed.argtypes = [vp, vp, vp, C.POINTER(MixedOpts), vp,
                                        C.POINTER(Stats)]
     L.bksp_dbicgstabl_mixed.argtypes = [sp, _dp, C.POINTER(MixedOpts), _dp]
+    L.bksp_gpu_solve_mixed_batch.argtypes = [C.POINTER(vp), C.POINTER(vp),
+                                             C.POINTER(vp), i,
+                                             C.POINTER(MixedOpts), i,
+                                             C.POINTER(Stats)]
+    L.bksp_gpu_solve_batch.argtypes = [C.POINTER(vp), i, i, C.POINTER(vp),
+                                       C.POINTER(vp), i, d, i, i,
+                                       C.POINTER(Stats)]
     L.bksp_gpu_spai_create.argtypes = [C.c_uint, C.POINTER(vp)]
     L.bksp_gpu_spai_destroy.argtypes = [vp]
     L.bksp_gpu_spai_params.argtypes = [vp, C.POINTER(C.c_float), i]
@@ -344,7 +352,15 @@ class GpuMatrix:
                      "inner_iters": st.inner_iters, "sweeps": st.sweeps}
 
     SPMV_VARIANTS = {0: "tile", 1: "tma", 2: "vec4", 3: "vec8", 4: "vec16",
-                     5: "vec32", 6: "wtile"}
+                     5: "vec32", 6: "wtile", 7: "dia"}
+
+    def diagonals(self):
+        """Column offsets of the operator's diagonal form ([] when none)."""
+        off = (C.c_int * 8)()
+        nd = lib.bksp_gpu_matrix_diagonals(self.h, off)
+        if nd < 0:
+            raise RuntimeError("bksp_gpu_matrix_diagonals failed")
+        return list(off[:nd])
 
     def variant(self, v=-1):
         """Query (v < 0) or set the SpMV kernel variant; returns it."""
@@ -436,3 +452,44 @@ def dbicgstabl_mixed(A, b, x, l=4, target=1e-8, max_iter=10000, precond=0,
                   model.h if model is not None else None, 0.0, 0, fallback)
     return lib.bksp_dbicgstabl_mixed(A.ptr, b.ctypes.data_as(_dp), C.byref(o),
                                      _inplace(x))
+
+
+def _batch_args(mats, bs, xs):
+    n = len(mats)
+    if len(bs) != n or len(xs) != n:
+        raise ValueError("one b and one x per matrix")
+    A = (C.c_void_p * n)(*[m.h for m in mats])
+    B = (C.c_void_p * n)(*[int(p) for p in bs])
+    X = (C.c_void_p * n)(*[int(p) for p in xs])
+    st = (Stats * n)()
+    return n, A, B, X, st
+
+
+def _batch_stats(st):
+    return [{"ret": s.ret, "hist_len": s.hist_len, "true_res": s.true_res,
+             "launches": s.launches, "iters": s.hist_len,
+             "inner_iters": s.inner_iters, "sweeps": s.sweeps,
+             "solve_ms": s.solve_ms} for s in st]
+
+
+def solve_mixed_batch(mats, bs, xs, l=4, target=1e-8, max_iter=10000,
+                      precond=0, model=None, delta=0.0, period=0, fallback=1,
+                      workers=0):
+    """bksp_gpu_solve_mixed_batch: mixed-precision BiCGSTAB(l) on every
+    (GpuMatrix, b, x) of the lists (device pointers, ready before the call,
+    x in/out), several systems at once; returns (ret, per-system stats)."""
+    n, A, B, X, st = _batch_args(mats, bs, xs)
+    o = MixedOpts(l, target, max_iter, precond,
+                  model.h if model is not None else None, delta, period,
+                  fallback)
+    ret = lib.bksp_gpu_solve_mixed_batch(A, B, X, n, C.byref(o), int(workers), st)
+    return ret, _batch_stats(st)
+
+
+def solve_batch(mats, method, bs, xs, tol, max_iter, l=4, workers=0):
+    """bksp_gpu_solve_batch: an FP64 method (CG ... BICGSTABL_FAST) on every
+    system of the lists; returns (ret, per-system stats)."""
+    n, A, B, X, st = _batch_args(mats, bs, xs)
+    ret = lib.bksp_gpu_solve_batch(A, int(method), int(l), B, X, n, float(tol),
+                                   int(max_iter), int(workers), st)
+    return ret, _batch_stats(st)

@@ -104,12 +104,19 @@ int bksp_gpu_matrix_destroy(bksp_gpu_matrix* m) {
 
 int bksp_gpu_matrix_variant(bksp_gpu_matrix* m, int variant) {
   if (!m) return INVALID_PARAMETERS;
-  if (variant > 6) return INVALID_PARAMETERS;
+  if (variant > 7) return INVALID_PARAMETERS;
   if (variant >= 0) {
     m->A.variant = variant;
     m->At.variant = variant;
   }
   return m->A.variant;
+}
+
+int bksp_gpu_matrix_diagonals(const bksp_gpu_matrix* m, int* offsets) {
+  if (!m) return INVALID_PARAMETERS;
+  if (offsets)
+    for (int d = 0; d < m->A.ndia; ++d) offsets[d] = m->A.doff[d];
+  return m->A.ndia;
 }
 
 int bksp_gpu_matrix_info(const bksp_gpu_matrix* m, int* n, int* nnz) {

@@ -106,7 +106,7 @@ int bksp_gpu_solve_mixed(bksp_gpu_matrix* m, const double* b, double* x,
     double* dx = dalloc_n<double>(np, st);
     double* x0 = dalloc_n<double>(np, st);
     float* mv = o->precond == BKSP_GPU_PRECOND_LEARNED
-                    ? dalloc_n<float>((long long)m->A.nnz + 8, st) : nullptr;
+                    ? dalloc_n<float>(spai_scratch_floats(m), st) : nullptr;
     BK_CHECK(cudaMemsetAsync(db, 0, sizeof(double) * np, st));
     BK_CHECK(cudaMemsetAsync(dx, 0, sizeof(double) * np, st));
     tm.begin_solve();

@@ -7,8 +7,9 @@
 // Terms are applied in input order: the first present term is a rounded
 // product, every further term a fused multiply-add -- the rounding of a
 // dscal / dcopy followed by FMA-based daxpy calls on the reference's CPU.
-// Inputs stream through one at a time, so register use grows with the
-// number of outputs and dots, not with the number of inputs.
+// Inputs stream through one at a time with the next two loads in flight,
+// so register use grows with the number of outputs and dots, not with the
+// number of inputs.
 // Operands are streamed as 16-byte packets (double2 / float4); lengths are
 // padded to a multiple of 64 and padding entries are zero in every vector.
 #pragma once
@@ -16,12 +17,21 @@
 
 namespace bk {
 
+// Input i's packet q (advanced by `off` when i repeats per batch rep).
+template <typename T>
+__device__ __forceinline__ void load_in(const LcH<T>& d, int i, long long off,
+                                        long long q, T* v) {
+  const T* p = d.in[i] + ((d.in_rep_mask >> i) & 1u ? off : 0);
+  unpack<T>(reinterpret_cast<const typename Pack<T>::V*>(p)[q], v);
+}
+
 template <typename T, int MI, int MO, int ND>
-__global__ void __launch_bounds__(kThreads, (MI > 4 ? 4 : 6))
+__global__ void __launch_bounds__(kThreads, 4)
 k_lincomb(const LcH<T> d, Red rd) {
   if (skip(rd)) return;
   using PV = typename Pack<T>::V;
   constexpr int P = Pack<T>::N;
+  constexpr int D = 3;   // input packets in flight per thread
   __shared__ T cs[MO][MI];
   __shared__ unsigned pres[MO];
   if (threadIdx.x < MO) {
@@ -49,25 +59,31 @@ k_lincomb(const LcH<T> d, Red rd) {
     const long long off = (long long)rep * d.stride;
     for (long long q = (long long)blockIdx.x * kThreads + threadIdx.x; q < npk;
          q += gstride) {
-      // Inputs are streamed one at a time into the output accumulators, so
-      // only the outputs and the dot operands stay live.
+      // Inputs are folded into the output accumulators one at a time, in
+      // input order, while the loads of the next D - 1 inputs are already
+      // in flight (a ring of D packets), so only the outputs, the dot
+      // operands and D packets stay live.
       T r[MO][P], da[ND > 0 ? ND : 1][P], db[ND > 0 ? ND : 1][P];
       bool first[MO];
 #pragma unroll
       for (int o = 0; o < MO; ++o) first[o] = true;
+      T ring[D][P];
+#pragma unroll
+      for (int i = 0; i < D - 1; ++i)
+        if (i < MI && i < d.nin) load_in(d, i, off, q, ring[i]);
 #pragma unroll
       for (int i = 0; i < MI; ++i) {
         if (i < d.nin) {
-          const T* p = d.in[i] + ((d.in_rep_mask >> i) & 1u ? off : 0);
-          T v[P];
-          unpack<T>(reinterpret_cast<const PV*>(p)[q], v);
+          const int ahead = i + D - 1;
+          if (ahead < MI && ahead < d.nin) load_in(d, ahead, off, q, ring[ahead % D]);
+          const T* v = ring[i % D];
 #pragma unroll
           for (int o = 0; o < MO; ++o) {
             if ((pm[o] >> i) & 1u) {
-              const T c = cs[o][i];
+              const T cf = cs[o][i];
 #pragma unroll
               for (int e = 0; e < P; ++e)
-                r[o][e] = first[o] ? mul_rn(c, v[e]) : fma_rn(c, v[e], r[o][e]);
+                r[o][e] = first[o] ? mul_rn(cf, v[e]) : fma_rn(cf, v[e], r[o][e]);
               first[o] = false;
             }
           }
@@ -121,7 +137,7 @@ k_lincomb(const LcH<T> d, Red rd) {
 // running over i, then j >= i.  The one-pass minimal-residual step of
 // BiCGSTAB(l) (its Gram matrix of r_0..r_l).
 template <typename T, int M>
-__global__ void __launch_bounds__(kThreads, (M > 5 ? 2 : 4))
+__global__ void __launch_bounds__(kThreads, (M > 2 ? 2 : 4))
 k_gram_vec(const GramH<T> g, Red rd) {
   if (skip(rd)) return;
   using PV = typename Pack<T>::V;
@@ -131,11 +147,24 @@ k_gram_vec(const GramH<T> g, Red rd) {
 #pragma unroll
   for (int q = 0; q < NP; ++q) acc[q] = 0.0;
   const long long npk = g.n / P;
+  const long long stride = (long long)gridDim.x * kThreads;
+  // Two packets per thread and sweep: 2 M independent 16-byte loads in
+  // flight before the dot products consume them.
   for (long long q = (long long)blockIdx.x * kThreads + threadIdx.x; q < npk;
-       q += (long long)gridDim.x * kThreads) {
-    T v[M][P];
+       q += 2 * stride) {
+    const long long q2 = q + stride;
+    T v[2][M][P];
 #pragma unroll
-    for (int i = 0; i < M; ++i) unpack<T>(reinterpret_cast<const PV*>(g.v[i])[q], v[i]);
+    for (int i = 0; i < M; ++i) unpack<T>(reinterpret_cast<const PV*>(g.v[i])[q], v[0][i]);
+#pragma unroll
+    for (int i = 0; i < M; ++i) {
+      if (q2 < npk) {
+        unpack<T>(reinterpret_cast<const PV*>(g.v[i])[q2], v[1][i]);
+      } else {
+#pragma unroll
+        for (int e = 0; e < P; ++e) v[1][i][e] = T(0);
+      }
+    }
     int idx = 0;
 #pragma unroll
     for (int i = 0; i < M; ++i)
@@ -143,7 +172,9 @@ k_gram_vec(const GramH<T> g, Red rd) {
       for (int j = i; j < M; ++j) {
         double s = 0.0;
 #pragma unroll
-        for (int e = 0; e < P; ++e) s += (double)v[i][e] * (double)v[j][e];
+        for (int h = 0; h < 2; ++h)
+#pragma unroll
+          for (int e = 0; e < P; ++e) s += (double)v[h][i][e] * (double)v[h][j][e];
         acc[idx++] += s;
       }
   }

@@ -53,6 +53,18 @@ struct RedH {
   short guard;   // > 0: the kernel runs only while S[guard] != 0
 };
 
+// Diagonal form of a CSR operator whose stored entries lie on at most
+// kDiaMax diagonals and whose rows list their columns in ascending order
+// (k_spmv_dia.cuh).  nd = 0: the operator has no diagonal form.
+constexpr int kDiaMax = 8;
+struct DiaH {
+  const void* val;             // nd x stride values, diagonal-major, 0 where absent
+  const unsigned char* mask;   // per row (stride bytes): bit d = entry on diagonal d stored
+  long long stride;            // pad64(n)
+  int nd;                      // diagonals in use
+  int off[kDiaMax];            // their column offsets j - i, ascending
+};
+
 // Device CSR matrix (one value precision).
 struct CsrH {
   const int* rowptr;
@@ -62,6 +74,7 @@ struct CsrH {
   int n;
   int nrb;
   int variant;   // SpMV kernel variant (kernels.cu: spmv_dispatch)
+  DiaH dia;
 };
 
 // One linear-combination launch: out[o] = sum_i c[o][i] * in[i], terms
@@ -123,6 +136,12 @@ void launch_gram_f(const GramH<float>& g, const RedH& rd, cudaStream_t st);
 // Element-wise precision conversions / mixed-precision updates.
 void launch_convert_d2f(const double* a, float* b, long long n, cudaStream_t st);
 void launch_convert_f2d(const float* a, double* b, long long n, cudaStream_t st);
+// Scatter CSR values into the diagonal form (dval zero-filled beforehand);
+// mask != nullptr: also write the row masks.
+void launch_csr2dia_d(const CsrH& A, const double* val, double* dval,
+                      unsigned char* mask, cudaStream_t st);
+void launch_csr2dia_f(const CsrH& A, const float* val, float* dval,
+                      unsigned char* mask, cudaStream_t st);
 // Mixed precision: o0 (= o1 = o2 when given) = fl32(in), with the dot
 // (w, o0) when nd = 1 (w == nullptr: (o0, o0)); and x64 += t32, y32 = 0.
 void launch_mx_d2f(const double* in, float* o0, float* o1, float* o2,

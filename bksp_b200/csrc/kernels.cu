@@ -1,21 +1,19 @@
-// Single translation unit holding every device kernel of the library (the
-// scalar epilogues are one device function shared by all reductions) and
-// the host-callable launch wrappers declared in kernel_api.h.
+// Kernels and launch wrappers (kernel_api.h) of the precision conversions,
+// the mixed-precision steps and the scalar / control nodes of a solve, plus
+// the shared launch bookkeeping.  The other kernels live in kernels_spmv.cu,
+// kernels_vec.cu and kernels_block.cu; every translation unit compiles its
+// own copy of the scalar epilogues (epilogues.cuh).
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
+#include <unordered_map>
 
 #include "dev_common.cuh"
 #include "epilogues.cuh"
-#include "k_spmv.cuh"
-#include "k_spmv_tma.cuh"
-#include "k_spmv_vec.cuh"
-#include "k_spmv_wtile.cuh"
-#include "k_vec.cuh"
-#include "k_shift.cuh"
-#include "k_block.cuh"
 #include "kernel_api.h"
+#include "launch_util.h"
 
 namespace bk {
 
@@ -24,175 +22,27 @@ long long& launch_count() {
   return n;
 }
 
-static inline int grid_for(long long work_items) {
-  long long g = (work_items + kThreads - 1) / kThreads;
-  if (g < 1) g = 1;
-  if (g > kMaxBlocks) g = kMaxBlocks;
-  return (int)g;
-}
-
-// ------------------------------------------------------------------ SpMV
-
-// SpMV kernel variants (every one sums a row in the reference's order):
-//   0 tile (register-staged products), 1 tile with TMA bulk copies,
-//   2..5 vector CSR with 4, 8, 16, 32 lanes per row, 6 warp tile.
-// CsrH.variant carries the choice made for the operator (autotuner);
-// BKSP_GPU_SPMV=tile|tma|vec4|vec8|vec16|vec32 overrides it.
-static int spmv_override() {
-  static int v = -2;
-  if (v == -2) {
-    const char* e = std::getenv("BKSP_GPU_SPMV");
-    v = -1;
-    if (e) {
-      const std::string s(e);
-      if (s == "tile") v = 0;
-      else if (s == "tma") v = 1;
-      else if (s == "vec4") v = 2;
-      else if (s == "vec8") v = 3;
-      else if (s == "vec16") v = 4;
-      else if (s == "vec32") v = 5;
-      else if (s == "wtile") v = 6;
-    }
-  }
-  return v;
-}
-
-template <typename VT, typename XT, int L>
-static void spmv_vec_launch(const CsrH& A, const SpmvH<XT>& io, const RedH& rd,
-                            cudaStream_t st) {
-  long long g = ((long long)A.n * L + kThreads - 1) / kThreads;
-  if (g > kMaxBlocks) g = kMaxBlocks;
-  if (g < 1) g = 1;
-  switch (io.nd) {
-    case 0: k_spmv_vec<VT, XT, 0, L><<<(int)g, kThreads, 0, st>>>(A, io, rd); break;
-    case 1: k_spmv_vec<VT, XT, 1, L><<<(int)g, kThreads, 0, st>>>(A, io, rd); break;
-    case 2: k_spmv_vec<VT, XT, 2, L><<<(int)g, kThreads, 0, st>>>(A, io, rd); break;
-    default: k_spmv_vec<VT, XT, 3, L><<<(int)g, kThreads, 0, st>>>(A, io, rd); break;
-  }
-}
-
-template <typename VT, typename XT, int ND>
-static void spmv_tma_launch(const CsrH& A, const SpmvH<XT>& io, const RedH& rd,
-                            cudaStream_t st) {
-  const size_t sm = 2 * (size_t)kStageEnt * (sizeof(int) + sizeof(VT));
-  static int attr_dev = -1, per_sm = 1;
-  int dev = 0;
+// Blocks of `kernel` (kThreads threads, no dynamic shared memory) that are
+// resident on the whole GPU at once, cached per kernel.
+int resident_grid(const void* kernel) {
+  static std::mutex mu;
+  static std::unordered_map<const void*, int> cache;
+  std::lock_guard<std::mutex> lk(mu);
+  const auto it = cache.find(kernel);
+  if (it != cache.end()) return it->second;
+  int dev = 0, sms = kSMs, per_sm = 0;
   cudaGetDevice(&dev);
-  if (attr_dev != dev) {
-    cudaFuncSetAttribute(k_spmv_tma<VT, XT, ND>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_spmv_tma<VT, XT, ND>,
-                                                  kThreads, sm);
-    if (per_sm < 1) per_sm = 1;
-    attr_dev = dev;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, 0) !=
+          cudaSuccess ||
+      per_sm < 1) {
+    cudaGetLastError();
+    per_sm = 1;
   }
-  int g = kSMs * per_sm;
+  long long g = (long long)per_sm * sms;
   if (g > kMaxBlocks) g = kMaxBlocks;
-  if (g > A.nrb) g = A.nrb > 0 ? A.nrb : 1;
-  k_spmv_tma<VT, XT, ND><<<g, kThreads, sm, st>>>(A, io, rd);
-}
-
-template <typename VT, typename XT>
-static void spmv_dispatch(const CsrH& A, const SpmvH<XT>& io, const RedH& rd,
-                          cudaStream_t st) {
-  int var = spmv_override();
-  if (var < 0) var = A.variant;
-  switch (var) {
-    case 1:
-      switch (io.nd) {
-        case 0: spmv_tma_launch<VT, XT, 0>(A, io, rd, st); return;
-        case 1: spmv_tma_launch<VT, XT, 1>(A, io, rd, st); return;
-        case 2: spmv_tma_launch<VT, XT, 2>(A, io, rd, st); return;
-        default: spmv_tma_launch<VT, XT, 3>(A, io, rd, st); return;
-      }
-    case 2: spmv_vec_launch<VT, XT, 4>(A, io, rd, st); return;
-    case 3: spmv_vec_launch<VT, XT, 8>(A, io, rd, st); return;
-    case 4: spmv_vec_launch<VT, XT, 16>(A, io, rd, st); return;
-    case 5: spmv_vec_launch<VT, XT, 32>(A, io, rd, st); return;
-    case 6: {
-      const int g = A.nrb < kMaxBlocks ? (A.nrb > 0 ? A.nrb : 1) : kMaxBlocks;
-      switch (io.nd) {
-        case 0: k_spmv_wtile<VT, XT, 0><<<g, kThreads, 0, st>>>(A, io, rd); return;
-        case 1: k_spmv_wtile<VT, XT, 1><<<g, kThreads, 0, st>>>(A, io, rd); return;
-        case 2: k_spmv_wtile<VT, XT, 2><<<g, kThreads, 0, st>>>(A, io, rd); return;
-        default: k_spmv_wtile<VT, XT, 3><<<g, kThreads, 0, st>>>(A, io, rd); return;
-      }
-    }
-    default: break;
-  }
-  const int g = A.nrb < kMaxBlocks ? (A.nrb > 0 ? A.nrb : 1) : kMaxBlocks;
-  switch (io.nd) {
-    case 0: k_spmv<VT, XT, 0><<<g, kThreads, 0, st>>>(A, io, rd); break;
-    case 1: k_spmv<VT, XT, 1><<<g, kThreads, 0, st>>>(A, io, rd); break;
-    case 2: k_spmv<VT, XT, 2><<<g, kThreads, 0, st>>>(A, io, rd); break;
-    default: k_spmv<VT, XT, 3><<<g, kThreads, 0, st>>>(A, io, rd); break;
-  }
-}
-
-void launch_spmv_d(const CsrH& A, const SpmvH<double>& io, const RedH& rd,
-                   cudaStream_t st) {
-  ++launch_count();
-  spmv_dispatch<double, double>(A, io, rd, st);
-}
-void launch_spmv_f(const CsrH& A, const SpmvH<float>& io, const RedH& rd,
-                   cudaStream_t st) {
-  ++launch_count();
-  spmv_dispatch<float, float>(A, io, rd, st);
-}
-
-// ------------------------------------------------------ linear combination
-
-template <typename T, int MI, int MO>
-static void lc_nd(const LcH<T>& d, const RedH& rd, cudaStream_t st) {
-  const int g = grid_for(d.n / Pack<T>::N);
-  switch (d.nd) {
-    case 0: k_lincomb<T, MI, MO, 0><<<g, kThreads, 0, st>>>(d, rd); break;
-    case 1: k_lincomb<T, MI, MO, 1><<<g, kThreads, 0, st>>>(d, rd); break;
-    case 2: k_lincomb<T, MI, MO, 2><<<g, kThreads, 0, st>>>(d, rd); break;
-    default: k_lincomb<T, MI, MO, 3><<<g, kThreads, 0, st>>>(d, rd); break;
-  }
-}
-
-template <typename T>
-static void lc_dispatch(const LcH<T>& d, const RedH& rd, cudaStream_t st) {
-  if (d.nin <= 4 && d.nout <= 2) lc_nd<T, 4, 2>(d, rd, st);
-  else if (d.nin <= 8 && d.nout <= 4) lc_nd<T, 8, 4>(d, rd, st);
-  else if (d.nout <= 4) lc_nd<T, 24, 4>(d, rd, st);
-  else if (d.nin <= 16) lc_nd<T, 16, 6>(d, rd, st);
-  else lc_nd<T, 24, 6>(d, rd, st);
-}
-
-void launch_lincomb_d(const LcH<double>& d, const RedH& rd, cudaStream_t st) {
-  ++launch_count();
-  lc_dispatch<double>(d, rd, st);
-}
-void launch_lincomb_f(const LcH<float>& d, const RedH& rd, cudaStream_t st) {
-  ++launch_count();
-  lc_dispatch<float>(d, rd, st);
-}
-
-// ------------------------------------------------------ pairwise Gram
-
-template <typename T>
-static void gram_dispatch(const GramH<T>& g, const RedH& rd, cudaStream_t st) {
-  ++launch_count();
-  const int gr = grid_for(g.n / Pack<T>::N);
-  switch (g.m) {
-    case 2: k_gram_vec<T, 2><<<gr, kThreads, 0, st>>>(g, rd); break;
-    case 3: k_gram_vec<T, 3><<<gr, kThreads, 0, st>>>(g, rd); break;
-    case 4: k_gram_vec<T, 4><<<gr, kThreads, 0, st>>>(g, rd); break;
-    case 5: k_gram_vec<T, 5><<<gr, kThreads, 0, st>>>(g, rd); break;
-    case 6: k_gram_vec<T, 6><<<gr, kThreads, 0, st>>>(g, rd); break;
-    case 7: k_gram_vec<T, 7><<<gr, kThreads, 0, st>>>(g, rd); break;
-    case 8: k_gram_vec<T, 8><<<gr, kThreads, 0, st>>>(g, rd); break;
-    default: k_gram_vec<T, 9><<<gr, kThreads, 0, st>>>(g, rd); break;
-  }
-}
-void launch_gram_d(const GramH<double>& g, const RedH& rd, cudaStream_t st) {
-  gram_dispatch<double>(g, rd, st);
-}
-void launch_gram_f(const GramH<float>& g, const RedH& rd, cudaStream_t st) {
-  gram_dispatch<float>(g, rd, st);
+  cache[kernel] = (int)g;
+  return (int)g;
 }
 
 // ----------------------------------------------------------- conversions
@@ -216,72 +66,6 @@ void launch_convert_d2f(const double* a, float* b, long long n, cudaStream_t st)
 void launch_convert_f2d(const float* a, double* b, long long n, cudaStream_t st) {
   ++launch_count();
   k_convert_f2d<<<grid_for(n), kThreads, 0, st>>>(a, b, n);
-}
-
-// ------------------------------------------------------- shifted methods
-
-void launch_shift(const ShiftArgsH& a, const RedH& rd, cudaStream_t st) {
-  ++launch_count();
-  ShiftArgs s{a.r, a.p, a.x, a.xs, a.ps, a.np, a.ns, a.l, a.j, a.mode};
-  const int g = grid_for(a.np);
-  switch (a.mode) {
-    case 0: k_shift<0><<<g, kThreads, 0, st>>>(s, rd); break;
-    case 1: k_shift<1><<<g, kThreads, 0, st>>>(s, rd); break;
-    case 2: k_shift<2><<<g, kThreads, 0, st>>>(s, rd); break;
-    default: k_shift<3><<<g, kThreads, 0, st>>>(s, rd); break;
-  }
-}
-
-// --------------------------------------------------------- block methods
-
-void launch_spmm(const CsrH& A, const SpmmH& a, const RedH& rd, cudaStream_t st) {
-  ++launch_count();
-  SpmmArgs s{a.X, a.Y, a.C, a.W, a.alpha, a.mode, a.s, a.nd};
-  const int g = grid_for((long long)A.n * kBlkS);
-  switch (a.nd) {
-    case 0: k_spmm<0><<<g, kThreads, 0, st>>>(A, s, rd); break;
-    case 1: k_spmm<1><<<g, kThreads, 0, st>>>(A, s, rd); break;
-    default: k_spmm<2><<<g, kThreads, 0, st>>>(A, s, rd); break;
-  }
-}
-
-void launch_block(const BlkH& a, const RedH& rd, cudaStream_t st) {
-  ++launch_count();
-  BlkArgs b;
-  static_assert(sizeof(BlkArgs) == sizeof(BlkH), "BlkArgs layout");
-  memcpy(&b, &a, sizeof(b));
-  const long long tiles = (a.n + kBlkTileRows - 1) / kBlkTileRows;
-  int g = (int)(tiles < kMaxBlocks ? tiles : kMaxBlocks);
-  if (g < 1) g = 1;
-  k_block<<<g, kThreads, 0, st>>>(b, rd);
-}
-
-// Column-major n x s (leading dimension n) <-> row-major np x s.
-__global__ void k_cm2rm(const double* __restrict__ cm, double* __restrict__ rm,
-                        int n, int s) {
-  const long long tot = (long long)n * s;
-  for (long long q = (long long)blockIdx.x * kThreads + threadIdx.x; q < tot;
-       q += (long long)gridDim.x * kThreads) {
-    const long long i = q / s, c = q % s;
-    rm[q] = cm[c * n + i];
-  }
-}
-__global__ void k_rm2cm(const double* __restrict__ rm, double* __restrict__ cm,
-                        int n, int s) {
-  const long long tot = (long long)n * s;
-  for (long long q = (long long)blockIdx.x * kThreads + threadIdx.x; q < tot;
-       q += (long long)gridDim.x * kThreads) {
-    const long long c = q / n, i = q % n;
-    cm[q] = rm[i * s + c];
-  }
-}
-void launch_cm2rm(const double* cm, double* rm, int n, int s, cudaStream_t st) {
-  ++launch_count();
-  k_cm2rm<<<grid_for((long long)n * s), kThreads, 0, st>>>(cm, rm, n, s);
-}
-void launch_rm2cm(const double* rm, double* cm, int n, int s, cudaStream_t st) {
-  ++launch_count();
-  k_rm2cm<<<grid_for((long long)n * s), kThreads, 0, st>>>(rm, cm, n, s);
 }
 
 // ------------------------------------------------- mixed-precision steps
@@ -311,11 +95,10 @@ void launch_mx_d2f(const double* in, float* o0, float* o1, float* o2,
                    const float* w, int nd, long long n, const RedH& rd,
                    cudaStream_t st) {
   ++launch_count();
-  const int g = grid_for(n);
   if (nd)
-    k_mx_d2f<1><<<g, kThreads, 0, st>>>(in, o0, o1, o2, w, n, rd);
+    k_mx_d2f<1><<<grid_wave(k_mx_d2f<1>, n), kThreads, 0, st>>>(in, o0, o1, o2, w, n, rd);
   else
-    k_mx_d2f<0><<<g, kThreads, 0, st>>>(in, o0, o1, o2, w, n, rd);
+    k_mx_d2f<0><<<grid_wave(k_mx_d2f<0>, n), kThreads, 0, st>>>(in, o0, o1, o2, w, n, rd);
 }
 
 // x64 += t32 (the preconditioned correction M y), then y32 = 0.
@@ -333,7 +116,7 @@ k_mx_accum(double* __restrict__ x, const float* __restrict__ t,
 void launch_mx_accum(double* x, const float* t, float* y, long long n,
                      const RedH& rd, cudaStream_t st) {
   ++launch_count();
-  k_mx_accum<<<grid_for(n), kThreads, 0, st>>>(x, t, y, n, rd);
+  k_mx_accum<<<grid_wave(k_mx_accum, n), kThreads, 0, st>>>(x, t, y, n, rd);
 }
 
 // ------------------------------------------------------- scalar / control

@@ -1,0 +1,83 @@
+// Shifted-method and block-method kernels and their launch wrappers
+// (kernel_api.h).
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "dev_common.cuh"
+#include "epilogues.cuh"
+#include "k_shift.cuh"
+#include "k_block.cuh"
+#include "kernel_api.h"
+#include "launch_util.h"
+
+namespace bk {
+
+// ------------------------------------------------------- shifted methods
+
+void launch_shift(const ShiftArgsH& a, const RedH& rd, cudaStream_t st) {
+  ++launch_count();
+  ShiftArgs s{a.r, a.p, a.x, a.xs, a.ps, a.np, a.ns, a.l, a.j, a.mode};
+  switch (a.mode) {
+    case 0: k_shift<0><<<grid_wave(k_shift<0>, a.np), kThreads, 0, st>>>(s, rd); break;
+    case 1: k_shift<1><<<grid_wave(k_shift<1>, a.np), kThreads, 0, st>>>(s, rd); break;
+    case 2: k_shift<2><<<grid_wave(k_shift<2>, a.np), kThreads, 0, st>>>(s, rd); break;
+    default: k_shift<3><<<grid_wave(k_shift<3>, a.np), kThreads, 0, st>>>(s, rd); break;
+  }
+}
+
+// --------------------------------------------------------- block methods
+
+void launch_spmm(const CsrH& A, const SpmmH& a, const RedH& rd, cudaStream_t st) {
+  ++launch_count();
+  SpmmArgs s{a.X, a.Y, a.C, a.W, a.alpha, a.mode, a.s, a.nd};
+  const int g = grid_for((long long)A.n * kBlkS);
+  switch (a.nd) {
+    case 0: k_spmm<0><<<g, kThreads, 0, st>>>(A, s, rd); break;
+    case 1: k_spmm<1><<<g, kThreads, 0, st>>>(A, s, rd); break;
+    default: k_spmm<2><<<g, kThreads, 0, st>>>(A, s, rd); break;
+  }
+}
+
+void launch_block(const BlkH& a, const RedH& rd, cudaStream_t st) {
+  ++launch_count();
+  BlkArgs b;
+  static_assert(sizeof(BlkArgs) == sizeof(BlkH), "BlkArgs layout");
+  memcpy(&b, &a, sizeof(b));
+  const long long tiles = (a.n + kBlkTileRows - 1) / kBlkTileRows;
+  int g = (int)(tiles < kMaxBlocks ? tiles : kMaxBlocks);
+  if (g < 1) g = 1;
+  k_block<<<g, kThreads, 0, st>>>(b, rd);
+}
+
+// Column-major n x s (leading dimension n) <-> row-major np x s.
+__global__ void k_cm2rm(const double* __restrict__ cm, double* __restrict__ rm,
+                        int n, int s) {
+  const long long tot = (long long)n * s;
+  for (long long q = (long long)blockIdx.x * kThreads + threadIdx.x; q < tot;
+       q += (long long)gridDim.x * kThreads) {
+    const long long i = q / s, c = q % s;
+    rm[q] = cm[c * n + i];
+  }
+}
+__global__ void k_rm2cm(const double* __restrict__ rm, double* __restrict__ cm,
+                        int n, int s) {
+  const long long tot = (long long)n * s;
+  for (long long q = (long long)blockIdx.x * kThreads + threadIdx.x; q < tot;
+       q += (long long)gridDim.x * kThreads) {
+    const long long c = q / n, i = q % n;
+    cm[q] = rm[i * s + c];
+  }
+}
+void launch_cm2rm(const double* cm, double* rm, int n, int s, cudaStream_t st) {
+  ++launch_count();
+  k_cm2rm<<<grid_for((long long)n * s), kThreads, 0, st>>>(cm, rm, n, s);
+}
+void launch_rm2cm(const double* rm, double* cm, int n, int s, cudaStream_t st) {
+  ++launch_count();
+  k_rm2cm<<<grid_for((long long)n * s), kThreads, 0, st>>>(rm, cm, n, s);
+}
+
+}  // namespace bk

@@ -1,0 +1,182 @@
+// SpMV kernels (every variant) and their launch wrappers (kernel_api.h),
+// plus the CSR -> diagonal-form scatter.
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "dev_common.cuh"
+#include "epilogues.cuh"
+#include "k_spmv.cuh"
+#include "k_spmv_tma.cuh"
+#include "k_spmv_vec.cuh"
+#include "k_spmv_wtile.cuh"
+#include "k_spmv_dia.cuh"
+#include "kernel_api.h"
+#include "launch_util.h"
+
+namespace bk {
+
+// ------------------------------------------------------------------ SpMV
+
+// SpMV kernel variants (every one sums a row in the reference's order):
+//   0 tile (register-staged products), 1 tile with TMA bulk copies,
+//   2..5 vector CSR with 4, 8, 16, 32 lanes per row, 6 warp tile,
+//   7 diagonal form (operators that have one; else the tile kernel).
+// CsrH.variant carries the choice made for the operator (autotuner);
+// BKSP_GPU_SPMV=tile|tma|vec4|vec8|vec16|vec32|wtile|dia overrides it.
+static int parse_spmv_override() {
+  const char* e = std::getenv("BKSP_GPU_SPMV");
+  if (!e) return -1;
+  const std::string s(e);
+  if (s == "tile") return 0;
+  if (s == "tma") return 1;
+  if (s == "vec4") return 2;
+  if (s == "vec8") return 3;
+  if (s == "vec16") return 4;
+  if (s == "vec32") return 5;
+  if (s == "wtile") return 6;
+  if (s == "dia") return 7;
+  return -1;
+}
+static int spmv_override() {
+  static const int v = parse_spmv_override();   // thread-safe initialisation
+  return v;
+}
+
+template <typename VT, typename XT, int L>
+static void spmv_vec_launch(const CsrH& A, const SpmvH<XT>& io, const RedH& rd,
+                            cudaStream_t st) {
+  long long g = ((long long)A.n * L + kThreads - 1) / kThreads;
+  if (g > kMaxBlocks) g = kMaxBlocks;
+  if (g < 1) g = 1;
+  switch (io.nd) {
+    case 0: k_spmv_vec<VT, XT, 0, L><<<(int)g, kThreads, 0, st>>>(A, io, rd); break;
+    case 1: k_spmv_vec<VT, XT, 1, L><<<(int)g, kThreads, 0, st>>>(A, io, rd); break;
+    case 2: k_spmv_vec<VT, XT, 2, L><<<(int)g, kThreads, 0, st>>>(A, io, rd); break;
+    default: k_spmv_vec<VT, XT, 3, L><<<(int)g, kThreads, 0, st>>>(A, io, rd); break;
+  }
+}
+
+template <typename VT, typename XT, int ND>
+static void spmv_tma_launch(const CsrH& A, const SpmvH<XT>& io, const RedH& rd,
+                            cudaStream_t st) {
+  const size_t sm = 2 * (size_t)kStageEnt * (sizeof(int) + sizeof(VT));
+  // The shared-memory attribute is per device: set it once on each.
+  static std::mutex mu;
+  static unsigned long long devs_set = 0;
+  static int per_sm = 1;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  int blocks_per_sm = 1;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    if (dev < 64 && !((devs_set >> dev) & 1ull)) {
+      cudaFuncSetAttribute(k_spmv_tma<VT, XT, ND>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+      int b = 0;
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_spmv_tma<VT, XT, ND>,
+                                                    kThreads, sm);
+      per_sm = b < 1 ? 1 : b;
+      devs_set |= 1ull << dev;
+    }
+    blocks_per_sm = per_sm;
+  }
+  int g = kSMs * blocks_per_sm;
+  if (g > kMaxBlocks) g = kMaxBlocks;
+  if (g > A.nrb) g = A.nrb > 0 ? A.nrb : 1;
+  k_spmv_tma<VT, XT, ND><<<g, kThreads, sm, st>>>(A, io, rd);
+}
+
+static inline bool aligned16(const void* p) {
+  return ((uintptr_t)p & 15u) == 0;
+}
+
+// The diagonal kernel stores y and loads x, b, w0, w1 as 16-byte packets.
+template <typename XT>
+static bool dia_usable(const CsrH& A, const SpmvH<XT>& io) {
+  return A.dia.nd > 0 && aligned16(io.x) && aligned16(io.y) &&
+         aligned16(io.y2) && aligned16(io.b) && aligned16(io.w0) &&
+         aligned16(io.w1);
+}
+
+template <typename VT, typename XT>
+static void spmv_dia_launch(const CsrH& A, const SpmvH<XT>& io, const RedH& rd,
+                            cudaStream_t st) {
+  const long long groups = ((long long)A.n + 3) / 4;   // 4 rows per thread
+  switch (io.nd) {
+    case 0: k_spmv_dia<VT, XT, 0><<<grid_wave(k_spmv_dia<VT, XT, 0>, groups), kThreads, 0, st>>>(A, io, rd); break;
+    case 1: k_spmv_dia<VT, XT, 1><<<grid_wave(k_spmv_dia<VT, XT, 1>, groups), kThreads, 0, st>>>(A, io, rd); break;
+    case 2: k_spmv_dia<VT, XT, 2><<<grid_wave(k_spmv_dia<VT, XT, 2>, groups), kThreads, 0, st>>>(A, io, rd); break;
+    default: k_spmv_dia<VT, XT, 3><<<grid_wave(k_spmv_dia<VT, XT, 3>, groups), kThreads, 0, st>>>(A, io, rd); break;
+  }
+}
+
+template <typename VT, typename XT>
+static void spmv_dispatch(const CsrH& A, const SpmvH<XT>& io, const RedH& rd,
+                          cudaStream_t st) {
+  int var = spmv_override();
+  if (var < 0) var = A.variant;
+  if (var == 7) {
+    if (dia_usable(A, io)) {
+      spmv_dia_launch<VT, XT>(A, io, rd, st);
+      return;
+    }
+    var = 0;
+  }
+  switch (var) {
+    case 1:
+      switch (io.nd) {
+        case 0: spmv_tma_launch<VT, XT, 0>(A, io, rd, st); return;
+        case 1: spmv_tma_launch<VT, XT, 1>(A, io, rd, st); return;
+        case 2: spmv_tma_launch<VT, XT, 2>(A, io, rd, st); return;
+        default: spmv_tma_launch<VT, XT, 3>(A, io, rd, st); return;
+      }
+    case 2: spmv_vec_launch<VT, XT, 4>(A, io, rd, st); return;
+    case 3: spmv_vec_launch<VT, XT, 8>(A, io, rd, st); return;
+    case 4: spmv_vec_launch<VT, XT, 16>(A, io, rd, st); return;
+    case 5: spmv_vec_launch<VT, XT, 32>(A, io, rd, st); return;
+    case 6: {
+      const int g = A.nrb < kMaxBlocks ? (A.nrb > 0 ? A.nrb : 1) : kMaxBlocks;
+      switch (io.nd) {
+        case 0: k_spmv_wtile<VT, XT, 0><<<g, kThreads, 0, st>>>(A, io, rd); return;
+        case 1: k_spmv_wtile<VT, XT, 1><<<g, kThreads, 0, st>>>(A, io, rd); return;
+        case 2: k_spmv_wtile<VT, XT, 2><<<g, kThreads, 0, st>>>(A, io, rd); return;
+        default: k_spmv_wtile<VT, XT, 3><<<g, kThreads, 0, st>>>(A, io, rd); return;
+      }
+    }
+    default: break;
+  }
+  const int g = A.nrb < kMaxBlocks ? (A.nrb > 0 ? A.nrb : 1) : kMaxBlocks;
+  switch (io.nd) {
+    case 0: k_spmv<VT, XT, 0><<<g, kThreads, 0, st>>>(A, io, rd); break;
+    case 1: k_spmv<VT, XT, 1><<<g, kThreads, 0, st>>>(A, io, rd); break;
+    case 2: k_spmv<VT, XT, 2><<<g, kThreads, 0, st>>>(A, io, rd); break;
+    default: k_spmv<VT, XT, 3><<<g, kThreads, 0, st>>>(A, io, rd); break;
+  }
+}
+
+void launch_spmv_d(const CsrH& A, const SpmvH<double>& io, const RedH& rd,
+                   cudaStream_t st) {
+  ++launch_count();
+  spmv_dispatch<double, double>(A, io, rd, st);
+}
+void launch_spmv_f(const CsrH& A, const SpmvH<float>& io, const RedH& rd,
+                   cudaStream_t st) {
+  ++launch_count();
+  spmv_dispatch<float, float>(A, io, rd, st);
+}
+
+void launch_csr2dia_d(const CsrH& A, const double* val, double* dval,
+                      unsigned char* mask, cudaStream_t st) {
+  ++launch_count();
+  k_csr2dia<double><<<(A.n + 255) / 256, 256, 0, st>>>(A, val, dval, mask);
+}
+void launch_csr2dia_f(const CsrH& A, const float* val, float* dval,
+                      unsigned char* mask, cudaStream_t st) {
+  ++launch_count();
+  k_csr2dia<float><<<(A.n + 255) / 256, 256, 0, st>>>(A, val, dval, mask);
+}
+
+}  // namespace bk

@@ -1,0 +1,73 @@
+// Fused level-1 kernels (linear combinations with dots, pairwise Gram
+// products) and their launch wrappers (kernel_api.h).
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "dev_common.cuh"
+#include "epilogues.cuh"
+#include "k_vec.cuh"
+#include "kernel_api.h"
+#include "launch_util.h"
+
+namespace bk {
+
+// ------------------------------------------------------ linear combination
+
+template <typename T, int MI, int MO>
+static void lc_nd(const LcH<T>& d, const RedH& rd, cudaStream_t st) {
+  const long long q = d.n / Pack<T>::N;
+  switch (d.nd) {
+    case 0: k_lincomb<T, MI, MO, 0><<<grid_wave(k_lincomb<T, MI, MO, 0>, q), kThreads, 0, st>>>(d, rd); break;
+    case 1: k_lincomb<T, MI, MO, 1><<<grid_wave(k_lincomb<T, MI, MO, 1>, q), kThreads, 0, st>>>(d, rd); break;
+    case 2: k_lincomb<T, MI, MO, 2><<<grid_wave(k_lincomb<T, MI, MO, 2>, q), kThreads, 0, st>>>(d, rd); break;
+    default: k_lincomb<T, MI, MO, 3><<<grid_wave(k_lincomb<T, MI, MO, 3>, q), kThreads, 0, st>>>(d, rd); break;
+  }
+}
+
+template <typename T>
+static void lc_dispatch(const LcH<T>& d, const RedH& rd, cudaStream_t st) {
+  if (d.nin <= 4 && d.nout <= 2) lc_nd<T, 4, 2>(d, rd, st);
+  else if (d.nin <= 8 && d.nout <= 4) lc_nd<T, 8, 4>(d, rd, st);
+  else if (d.nout <= 4) lc_nd<T, 24, 4>(d, rd, st);
+  else if (d.nin <= 16) lc_nd<T, 16, 6>(d, rd, st);
+  else lc_nd<T, 24, 6>(d, rd, st);
+}
+
+void launch_lincomb_d(const LcH<double>& d, const RedH& rd, cudaStream_t st) {
+  ++launch_count();
+  lc_dispatch<double>(d, rd, st);
+}
+void launch_lincomb_f(const LcH<float>& d, const RedH& rd, cudaStream_t st) {
+  ++launch_count();
+  lc_dispatch<float>(d, rd, st);
+}
+
+// ------------------------------------------------------ pairwise Gram
+
+template <typename T>
+static void gram_dispatch(const GramH<T>& g, const RedH& rd, cudaStream_t st) {
+  ++launch_count();
+  const long long q = (g.n / Pack<T>::N + 1) / 2;   // two packets per thread
+  switch (g.m) {
+#define BK_GRAM(M)                                                        \
+  case M:                                                                 \
+    k_gram_vec<T, M><<<grid_wave(k_gram_vec<T, M>, q), kThreads, 0, st>>>(g, rd); \
+    break;
+    BK_GRAM(2) BK_GRAM(3) BK_GRAM(4) BK_GRAM(5) BK_GRAM(6) BK_GRAM(7) BK_GRAM(8)
+    default:
+      k_gram_vec<T, 9><<<grid_wave(k_gram_vec<T, 9>, q), kThreads, 0, st>>>(g, rd);
+      break;
+#undef BK_GRAM
+  }
+}
+void launch_gram_d(const GramH<double>& g, const RedH& rd, cudaStream_t st) {
+  gram_dispatch<double>(g, rd, st);
+}
+void launch_gram_f(const GramH<float>& g, const RedH& rd, cudaStream_t st) {
+  gram_dispatch<float>(g, rd, st);
+}
+
+}  // namespace bk

@@ -1,6 +1,7 @@
 #include "runtime.h"
 
 #include <algorithm>
+#include <climits>
 #include <cstdio>
 #include <cstdlib>
 #include <mutex>
@@ -50,9 +51,16 @@ void DevCsr::release(cudaStream_t st) {
   dfree(v64, st);
   dfree(v32, st);
   dfree(rb, st);
+  dfree(d64, st);
+  dfree(d32, st);
+  if (owns_dmask) dfree(dmask, st);
   rowptr = col = rb = nullptr;
   v64 = nullptr;
   v32 = nullptr;
+  d64 = nullptr;
+  d32 = nullptr;
+  dmask = nullptr;
+  ndia = 0;
 }
 
 HostCsr expand_symmetric(int n, const int* rowptr, const int* col,
@@ -151,9 +159,63 @@ std::vector<int> make_row_blocks(int n, const int* rowptr) {
   return rb;
 }
 
-// SpMV variant from the mean row length: vector CSR with the smallest lane
-// count that covers a typical row.
-static int heuristic_variant(int n, int nnz) {
+// Diagonal offsets of an operator, or false when it has no useful diagonal
+// form: more than kDiaMax diagonals, a row whose columns do not strictly
+// ascend (its CSR summation order would not be the diagonal order), or a
+// form moving more bytes than CSR in FP64 (nd * 8 n + n >= 12 nnz + 4 n).
+// off comes out ascending.  One pass: a row's offsets ascend, so the
+// pointer into the sorted list only moves forward within a row.
+static bool dia_offsets(int n, const int* rowptr, const int* col, int& nd,
+                        int off[kDiaMax]) {
+  nd = 0;
+  for (int i = 0; i < n; ++i) {
+    int q = 0;
+    long long prev = LLONG_MIN;
+    for (int k = rowptr[i]; k < rowptr[i + 1]; ++k) {
+      const long long o = (long long)col[k] - i;
+      if (o <= prev) return false;
+      prev = o;
+      while (q < nd && off[q] < o) ++q;
+      if (q == nd || off[q] != o) {
+        if (nd == kDiaMax) return false;
+        for (int t = nd; t > q; --t) off[t] = off[t - 1];
+        off[q] = (int)o;
+        ++nd;
+      }
+    }
+  }
+  const double nnz = rowptr[n];
+  return nd > 0 && (double)nd * 8.0 * n + n < 12.0 * nnz + 4.0 * n;
+}
+
+// Build the diagonal form of an uploaded operator (values of both
+// precisions present, row masks) when it has one.
+static void build_dia(int n, const int* rowptr, const int* col, DevCsr& A,
+                      cudaStream_t st) {
+  int nd = 0, off[kDiaMax] = {};
+  if (!dia_offsets(n, rowptr, col, nd, off)) return;
+  const long long stride = pad64(n);
+  A.ndia = nd;
+  for (int d = 0; d < kDiaMax; ++d) A.doff[d] = d < nd ? off[d] : 0;
+  A.dmask = dalloc_n<unsigned char>(stride, st);
+  A.owns_dmask = true;
+  A.d64 = dalloc_n<double>(nd * stride, st);
+  BK_CHECK(cudaMemsetAsync(A.dmask, 0, stride, st));
+  BK_CHECK(cudaMemsetAsync(A.d64, 0, sizeof(double) * nd * stride, st));
+  CsrH h = A.hview(A.v64, A.d64);
+  launch_csr2dia_d(h, A.v64, A.d64, A.dmask, st);
+  BK_CHECK(cudaGetLastError());
+  if (A.v32) {
+    A.d32 = dalloc_n<float>(nd * stride, st);
+    launch_convert_d2f(A.d64, A.d32, nd * stride, st);
+    BK_CHECK(cudaGetLastError());
+  }
+}
+
+// SpMV variant without timing: the diagonal form when there is one, else
+// vector CSR with the smallest lane count that covers a typical row.
+static int heuristic_variant(int n, int nnz, bool dia) {
+  if (dia) return 7;
   const double avg = n > 0 ? (double)nnz / n : 0.0;
   if (avg <= 4.5) return 2;
   if (avg <= 9.0) return 3;
@@ -164,15 +226,16 @@ static int heuristic_variant(int n, int nnz) {
 namespace {
 struct TuneKey {
   int n, nnz, dev;
-  bool fp32;
+  bool fp32, dia;
   bool operator==(const TuneKey& o) const {
-    return n == o.n && nnz == o.nnz && dev == o.dev && fp32 == o.fp32;
+    return n == o.n && nnz == o.nnz && dev == o.dev && fp32 == o.fp32 &&
+           dia == o.dia;
   }
 };
 struct TuneHash {
   size_t operator()(const TuneKey& k) const {
     return ((size_t)k.n * 1000003u) ^ ((size_t)k.nnz * 7919u) ^
-           ((size_t)k.dev << 1) ^ (size_t)k.fp32;
+           ((size_t)k.dev << 2) ^ (size_t)k.fp32 ^ ((size_t)k.dia << 1);
   }
 };
 std::mutex g_tune_mu;
@@ -180,15 +243,16 @@ std::unordered_map<TuneKey, int, TuneHash> g_tune_cache;
 }  // namespace
 
 // Autotuner: time every SpMV variant on this operator (FP32 values when
-// present, else FP64), keep the fastest; cached per (n, nnz, device).
-// BKSP_GPU_AUTOTUNE=0 keeps the mean-row-length heuristic.
+// present, else FP64), keep the fastest; cached per (n, nnz, device,
+// precision, diagonal form present).  BKSP_GPU_AUTOTUNE=0 keeps the
+// heuristic choice.
 void autotune_spmv(DevCsr& A, cudaStream_t st) {
   const char* e = std::getenv("BKSP_GPU_AUTOTUNE");
   if (e && std::string(e) == "0") return;
   int dev = 0;
   cudaGetDevice(&dev);
   const bool f32 = A.v32 != nullptr;
-  const TuneKey key{A.n, A.nnz, dev, f32};
+  const TuneKey key{A.n, A.nnz, dev, f32, A.ndia > 0};
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tune_cache.find(key);
@@ -210,9 +274,10 @@ void autotune_spmv(DevCsr& A, cudaStream_t st) {
   BK_CHECK(cudaEventCreate(&e1));
   // Three interleaved rounds of 8 launches per candidate; a candidate's
   // time is its best round, so one noisy round cannot decide the choice.
-  const int cands[] = {0, 6, 1, 2, 3, 4};
-  constexpr int kC = sizeof(cands) / sizeof(cands[0]);
-  float best_of[kC];
+  int cands[8] = {0, 6, 1, 2, 3, 4};
+  int kC = 6;
+  if (A.ndia > 0) cands[kC++] = 7;
+  float best_of[8];
   for (int c = 0; c < kC; ++c) best_of[c] = 1e30f;
   for (int round = 0; round < 3; ++round) {
     for (int c = 0; c < kC; ++c) {
@@ -287,7 +352,8 @@ void upload_csr(int n, const int* rowptr, const int* col, const double* val,
     launch_convert_d2f(out.v64, out.v32, padn, st);
     BK_CHECK(cudaGetLastError());
   }
-  out.variant = heuristic_variant(n, nnz);
+  build_dia(n, rowptr, col, out, st);
+  out.variant = heuristic_variant(n, nnz, out.ndia > 0);
   if (n >= (1 << 16)) autotune_spmv(out, st);
 }
 

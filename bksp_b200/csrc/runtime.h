@@ -56,8 +56,26 @@ struct DevCsr {
   float* v32 = nullptr;
   int* rb = nullptr;
   int variant = 3;   // SpMV kernel variant chosen for this operator
-  CsrH h64() const { return CsrH{rowptr, col, v64, rb, n, nrb, variant}; }
-  CsrH h32() const { return CsrH{rowptr, col, v32, rb, n, nrb, variant}; }
+  // Diagonal form (ndia = 0: none): values per precision, shared row masks.
+  int ndia = 0;
+  int doff[kDiaMax] = {};
+  unsigned char* dmask = nullptr;
+  double* d64 = nullptr;
+  float* d32 = nullptr;
+  bool owns_dmask = true;   // false for views sharing another operator's masks
+  CsrH h64() const { return hview(v64, d64); }
+  CsrH h32() const { return hview(v32, d32); }
+  CsrH hview(const void* v, const void* dv) const {
+    CsrH h{rowptr, col, v, rb, n, nrb, variant, DiaH{}};
+    if (ndia > 0 && dv) {
+      h.dia.val = dv;
+      h.dia.mask = dmask;
+      h.dia.stride = pad64(n);
+      h.dia.nd = ndia;
+      for (int d = 0; d < kDiaMax; ++d) h.dia.off[d] = doff[d];
+    }
+    return h;
+  }
   void release(cudaStream_t st);
 };
 

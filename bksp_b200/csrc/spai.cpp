@@ -88,6 +88,10 @@ static void ensure_features(bksp_gpu_matrix* m, cudaStream_t st) {
   BK_CHECK(cudaGetLastError());
 }
 
+long long spai_scratch_floats(const bksp_gpu_matrix* m) {
+  return pad64((long long)m->A.nnz + 8) + (long long)m->A.ndia * pad64(m->A.n);
+}
+
 DevCsr spai_apply(bksp_gpu_spai_model* model, bksp_gpu_matrix* m, float* mvals,
                   cudaStream_t st) {
   ensure_features(m, st);
@@ -105,6 +109,18 @@ DevCsr spai_apply(bksp_gpu_spai_model* model, bksp_gpu_matrix* m, float* mvals,
   v.rb = m->A.rb;
   v.variant = m->A.variant;
   v.v32 = mvals;
+  if (m->A.ndia > 0) {
+    // M has A's pattern: A's diagonals and row masks, M's values.
+    v.ndia = m->A.ndia;
+    for (int d = 0; d < kDiaMax; ++d) v.doff[d] = m->A.doff[d];
+    v.dmask = m->A.dmask;
+    v.owns_dmask = false;
+    const long long dn = (long long)v.ndia * pad64(n);
+    v.d32 = mvals + pad64((long long)m->A.nnz + 8);
+    BK_CHECK(cudaMemsetAsync(v.d32, 0, sizeof(float) * dn, st));
+    launch_csr2dia_f(v.hview(v.v32, v.d32), v.v32, v.d32, nullptr, st);
+    BK_CHECK(cudaGetLastError());
+  }
   return v;
 }
 

@@ -35,8 +35,12 @@ struct SpaiSlots {
 // Host analysis of the uploaded CSR (rows as on the device).
 void spai_build_slots(int n, const int* rowptr, const int* col, SpaiSlots& s,
                       cudaStream_t st);
-// M (FP32 values in mvals, nnz + 8 floats) on A's pattern from the model;
-// returns a CSR view sharing A's index arrays.
+// Scratch floats spai_apply needs: M's CSR values (nnz + 8, padded to 64)
+// then, when A has a diagonal form, M's diagonal form.
+long long spai_scratch_floats(const bksp_gpu_matrix* m);
+// M (FP32 values in mvals, spai_scratch_floats floats) on A's pattern from
+// the model; returns a view sharing A's index arrays and row masks (never
+// released).
 DevCsr spai_apply(bksp_gpu_spai_model* model, bksp_gpu_matrix* m,
                   float* mvals, cudaStream_t st);
 

@@ -14,6 +14,7 @@
 // (forward, residual, backward) and a CTA reduces its rows' weight
 // gradients through shared memory into per-CTA partials, which the Adam
 // kernel sums in a fixed order (deterministic).
+#include <mutex>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -338,11 +339,18 @@ void launch_spai_grad(int n, const float* w, const float* feat,
                       cudaStream_t st) {
   ++launch_count();
   const size_t sm = sizeof(float) * (kP + kTrainThreads * kStage);
-  static bool attr = false;
-  if (!attr) {
-    cudaFuncSetAttribute(k_spai_grad, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)sm);
-    attr = true;
+  // The shared-memory attribute is per device: set it once on each.
+  static std::mutex mu;
+  static unsigned long long devs_set = 0;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    if (dev < 64 && !((devs_set >> dev) & 1ull)) {
+      cudaFuncSetAttribute(k_spai_grad, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)sm);
+      devs_set |= 1ull << dev;
+    }
   }
   k_spai_grad<<<spai_grad_blocks(n), kTrainThreads, sm, st>>>(
       n, w, feat, dinv, slot_entry, col, Z, AZ, probes, ldz, scale, gpart, lpart);

@@ -95,3 +95,72 @@ def uniform(n, seed):
 def log_shifts(count=32, lo=-3.0, hi=0.0):
     """sigma_k = 10^(lo + (hi-lo) k/(count-1)), k = 0..count-1."""
     return 10.0 ** (lo + (hi - lo) * np.arange(count) / (count - 1))
+
+
+def gaussian_random_field(L, seed, corr=0.1, var=1.0):
+    """Stationary Gaussian random field on the L^3 cell centres of the unit
+    cube with covariance var * exp(-r^2 / (2 corr^2)), by spectral sampling:
+    white noise filtered in Fourier space with the square root of the
+    covariance's spectral density (periodic FFT, then normalised to zero
+    mean and variance `var`)."""
+    rng = np.random.default_rng(seed)
+    noise = rng.standard_normal((L, L, L))
+    k = 2.0 * np.pi * np.fft.fftfreq(L, d=1.0 / L)
+    kz = 2.0 * np.pi * np.fft.rfftfreq(L, d=1.0 / L)
+    k2 = k[:, None, None] ** 2 + k[None, :, None] ** 2 + kz[None, None, :] ** 2
+    filt = np.exp(-0.25 * corr * corr * k2)   # sqrt of exp(-corr^2 k^2 / 2)
+    g = np.fft.irfftn(np.fft.rfftn(noise) * filt, s=(L, L, L))
+    g -= g.mean()
+    s = g.std()
+    return g * (np.sqrt(var) / s if s > 0 else 0.0)
+
+
+def kappa_diffusion3d(L, seed):
+    """-div(kappa grad u) = f on an L^3 cell-centred grid of the unit cube,
+    Dirichlet u = 0 on the boundary, 7-point finite volumes (h^2-scaled):
+    face coefficient = harmonic mean 2 k_i k_j / (k_i + k_j) between
+    neighbouring cells, 2 k_i on a boundary face; kappa = exp(g) with g a
+    Gaussian random field (correlation length 0.1, variance 1, seed).
+    Symmetric positive definite.  Returns (rowptr, col, val, n)."""
+    kap = np.exp(gaussian_random_field(L, seed)).reshape(-1)   # index x + L(y + L z)
+    n = L ** 3
+    idx = np.arange(n, dtype=np.int64)
+    x = idx % L
+    y = (idx // L) % L
+    z = idx // (L * L)
+    # neighbours in ascending linear-offset order: z-, y-, x-, (diag), x+, y+, z+
+    nbr = [(0, 0, -1), (0, -1, 0), (-1, 0, 0), (1, 0, 0), (0, 1, 0), (0, 0, 1)]
+    cols = np.empty((n, 7), dtype=np.int64)
+    vals = np.zeros((n, 7), dtype=np.float64)
+    mask = np.ones((n, 7), dtype=bool)
+    diag = np.zeros(n)
+    slot = [0, 1, 2, 4, 5, 6]
+    for (dx, dy, dz), s in zip(nbr, slot):
+        xx, yy, zz = x + dx, y + dy, z + dz
+        inside = (xx >= 0) & (xx < L) & (yy >= 0) & (yy < L) & (zz >= 0) & (zz < L)
+        j = np.where(inside, xx + L * (yy + L * zz), 0)
+        kf = np.where(inside, 2.0 * kap * kap[j] / (kap + kap[j]), 2.0 * kap)
+        diag += kf
+        cols[:, s] = j
+        vals[:, s] = -kf
+        mask[:, s] = inside
+    cols[:, 3] = idx
+    vals[:, 3] = diag
+    counts = mask.sum(axis=1)
+    rowptr = np.zeros(n + 1, dtype=np.int64)
+    np.cumsum(counts, out=rowptr[1:])
+    return rowptr.astype(np.int32), cols[mask].astype(np.int32), vals[mask], n
+
+
+def kappa_batch(count=64, seed=4, lo=32, hi=96, field_seed0=5):
+    """The batched workload: `count` kappa-diffusion systems with edge
+    lengths L ~ U{lo..hi} (seed), field seeds field_seed0 + i, right-hand
+    sides f ~ N(0, 1) (seed field_seed0 + i + 10000).  Returns a list of
+    (rowptr, col, val, n, b)."""
+    Ls = np.random.default_rng(seed).integers(lo, hi + 1, count)
+    out = []
+    for i, L in enumerate(Ls):
+        rp, c, v, n = kappa_diffusion3d(int(L), field_seed0 + i)
+        b = np.random.default_rng(field_seed0 + i + 10000).standard_normal(n)
+        out.append((rp, c, v, n, b))
+    return out

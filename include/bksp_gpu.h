@@ -88,11 +88,21 @@ int bksp_gpu_solve(bksp_gpu_matrix *A, int method, int l, const double *b,
 
 /* SpMV kernel variant of the operator: 0 tile, 1 tile with TMA bulk
  * copies, 2..5 vector CSR with 4, 8, 16, 32 lanes per row, 6 warp tile
- * (each warp streams and sums its own 32 rows).  variant < 0
- * queries, otherwise sets.  Returns the variant in use.  The library picks
- * one by timing all of them when it uploads an operator of >= 65,536
- * rows (by mean row length below that). */
+ * (each warp streams and sums its own 32 rows), 7 diagonal form (operators
+ * without one, and calls whose result / operand vectors are not 16-byte
+ * aligned, run the tile kernel).  variant < 0 queries, otherwise sets.
+ * Returns the variant set.  The library picks one by timing all of them
+ * when it uploads an operator of >= 65,536 rows (below that: the diagonal
+ * form when there is one, else by mean row length). */
 int bksp_gpu_matrix_variant(bksp_gpu_matrix *A, int variant);
+
+/* Diagonal form of the operator: an operator whose stored entries lie on at
+ * most 8 diagonals, whose rows list their columns in strictly ascending
+ * order, and whose diagonal storage is smaller than its CSR storage, is
+ * also kept diagonal by diagonal.  Returns the number of diagonals (0: no
+ * diagonal form) and writes their column offsets j - i, ascending, to
+ * offsets (8 ints, or NULL). */
+int bksp_gpu_matrix_diagonals(const bksp_gpu_matrix *A, int *offsets);
 
 /* y = A x on the device, FP64 (fp32 = 0) or FP32 vectors and values
  * (fp32 = 1, needs BKSP_GPU_FP32); x and y hold n elements.  Asynchronous
@@ -168,19 +178,42 @@ int bksp_gpu_solve_mixed(bksp_gpu_matrix *A, const double *b, double *x,
 int bksp_dbicgstabl_mixed(dspmat *A, double *b, const bksp_gpu_mixed_opts *opts,
                           double *x);
 
-/* The same FP64 relative true residual, computed without allocating any
- * memory, for callers that cannot allocate device memory where they need it
- * (a host application whose memory pool already owns the GPU's memory;
- * latency-critical loops that cannot take the device-wide synchronisation of
- * cudaMalloc/cudaFree).  No counterpart in the reference.  Its scratch is a
- * static device array of about 8 MiB that every GPU loading the library
- * holds until exit; operators with more than 1,048,576 rows are rejected
- * with INVALID_PARAMETERS and a message on stderr.  The first call on each
- * device looks up that array's device address (make it before any stream
- * capture).  All calls on a device share the array: calls whose GPU work
- * overlaps race and must be serialised by the caller.  b, x: device
- * pointers to n doubles; *res receives the residual; returns 0 or
- * INVALID_PARAMETERS; synchronous on `stream` (NULL: library stream). */
+/* ------------------------------------------------------------ batches */
+
+/* Many independent systems in one call: `workers` host threads (0: 8; at
+ * most count), each with its own CUDA stream, take the systems in turn and
+ * solve each exactly as bksp_gpu_solve_mixed / bksp_gpu_solve would, so the
+ * GPU runs several systems' solves at once and every result equals the
+ * single-system call's.  A[i], b[i], x[i]: system i's operator and device
+ * vectors (x in/out); they must be ready when the call is made, and every
+ * x[i] holds its result when it returns.  stats: NULL or count entries
+ * (stats[i].ret = system i's return code).  Returns 0 when every system
+ * converged, NOT_CONVERGED when at least one did not (or diverged),
+ * INVALID_PARAMETERS on bad arguments or a failed system. */
+int bksp_gpu_solve_mixed_batch(bksp_gpu_matrix *const *A, const double *const *b,
+                               double *const *x, int count,
+                               const bksp_gpu_mixed_opts *opts, int workers,
+                               bksp_gpu_stats *stats);
+int bksp_gpu_solve_batch(bksp_gpu_matrix *const *A, int method, int l,
+                         const double *const *b, double *const *x, int count,
+                         double tol, int max_iter, int workers,
+                         bksp_gpu_stats *stats);
+
+/* The FP64 relative true residual of bksp_gpu_true_residual, computed
+ * without allocating any memory, for callers that cannot allocate device
+ * memory where they need it (a host application whose memory pool already
+ * owns the GPU's memory; latency-critical loops that cannot take the
+ * device-wide synchronisation of cudaMalloc/cudaFree).  No counterpart in
+ * the reference.  Its scratch is a static device array of about 8 MiB that
+ * every GPU loading the library holds until exit; operators with more than
+ * 1,048,576 rows are rejected with INVALID_PARAMETERS and a message on
+ * stderr.  The first call on each device looks up that array's device
+ * address (make it before any stream capture).  All calls on a device share
+ * the array: calls whose GPU work overlaps race and must be serialised by
+ * the caller.  b, x: device pointers to n doubles; *res receives the
+ * residual; returns 0 or INVALID_PARAMETERS; synchronous on `stream` (NULL:
+ * library stream).
+ */
 int bksp_gpu_true_residual_noalloc(bksp_gpu_matrix *A, const double *b,
                                    const double *x, void *stream,
                                    double *res);

@@ -165,3 +165,27 @@ def test_one_pass_mr_matches_mgs(gpu, torch_cuda, golden, fast):
         np.testing.assert_allclose(st["hist"][:k], gk["hist"][:k], rtol=1e-6)
         assert S.true_residual(A, b, xd.cpu().numpy()) < 1e-9
     G.close()
+
+
+@pytest.mark.parametrize("precond", [0, 1, 2])
+def test_mixed_solve_same_with_diagonal_form(gpu, torch_cuda, trained, precond):
+    """The diagonal-form SpMV sums each row in the CSR order, so a mixed
+    solve (A and M products) gives bit-identical results with either kernel."""
+    B, torch = gpu, torch_cuda
+    model = trained[0]
+    rp, c, v, n, A, b = _system(P.convdiff3d, 20)
+    G = B.GpuMatrix(B.CsrMatrix(rp, c, v), B.FP32)
+    assert len(G.diagonals()) == 7
+    bd = _dev(torch, b)
+    out = []
+    for variant in (0, 7):
+        G.variant(variant)
+        xd = torch.zeros(n, dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        ret, st = G.solve_mixed(bd.data_ptr(), xd.data_ptr(), l=4, target=1e-8,
+                                precond=precond, model=model)
+        out.append((ret, st["true_res"], xd.cpu().numpy()))
+    assert out[0][0] == out[1][0] >= 0
+    assert out[0][1] == out[1][1] <= 1e-8
+    assert np.array_equal(out[0][2], out[1][2])
+    G.close()

@@ -60,7 +60,7 @@ def test_spmv_bit_exact_vs_reference_order(gpu, testmats):
                                atol=1e-20)
 
 
-@pytest.mark.parametrize("variant", range(7))
+@pytest.mark.parametrize("variant", range(8))
 def test_spmv_variants_bit_exact(gpu, testmats, variant):
     """Every SpMV kernel variant sums rows in the reference's order."""
     import torch
@@ -100,6 +100,61 @@ def test_spmv_variants_bit_exact(gpu, testmats, variant):
         ref32 = sp.csr_matrix((v.astype(np.float32), c, rp), shape=(G.n, G.n)) @ x.astype(np.float32)
         np.testing.assert_allclose(y32.cpu().numpy(), ref32, rtol=2e-5, atol=2e-4)
         G.close()
+
+
+def test_diagonal_form_detection(gpu, testmats):
+    """Operators on <= 8 diagonals with ascending rows get a diagonal form."""
+    G = gpu.GpuMatrix(gpu.CsrMatrix(testmats["pde_rowptr"], testmats["pde_col"],
+                                    testmats["pde_val"]))
+    assert G.diagonals() == [-47, -1, 0, 1, 47]
+    assert G.variant() == 7          # small operator with a diagonal form
+    G.close()
+    rp, c, v, n = P.convdiff3d(12)
+    G = gpu.GpuMatrix(gpu.CsrMatrix(rp, c, v), gpu.FP32)
+    assert G.diagonals() == [-144, -12, -1, 0, 1, 12, 144]
+    G.close()
+    # 165 diagonals: none.
+    G = gpu.GpuMatrix(gpu.CsrMatrix(testmats["bfwb_rowptr"], testmats["bfwb_col"],
+                                    testmats["bfwb_val"]))
+    assert G.diagonals() == []
+    G.close()
+    # A row listing its columns out of order: none (the diagonal order would
+    # not be the row's summation order).
+    rp2, c2, v2 = rp.copy(), c.copy(), v.copy()
+    k = rp2[100]
+    c2[k], c2[k + 1] = c2[k + 1], c2[k]
+    v2[k], v2[k + 1] = v2[k + 1], v2[k]
+    G = gpu.GpuMatrix(gpu.CsrMatrix(rp2, c2, v2))
+    assert G.diagonals() == []
+    G.close()
+
+
+def test_dia_tail_unaligned_and_missing_entries(gpu):
+    """Diagonal kernel: odd n (tail rows), rows missing diagonals, an
+    explicitly stored zero, and result vectors that are not 16-byte aligned
+    (which fall back to the tile kernel) -- all bit-exact."""
+    import torch
+    rp, c, v, n = P.convdiff2d(37)          # n = 1369, odd
+    rng = np.random.default_rng(11)
+    v = v.copy()
+    v[rng.integers(0, v.size, 50)] = 0.0    # stored zeros stay stored
+    G = gpu.GpuMatrix(gpu.CsrMatrix(rp, c, v), gpu.FP32)
+    assert len(G.diagonals()) == 5
+    G.variant(7)
+    x = rng.uniform(-1, 1, n)
+    ref = _row_sums_sequential(rp, c, v, x)
+    xd = torch.from_numpy(x).cuda()
+    for shift in (0, 1):
+        yb = torch.full((n + 1,), 7.0, dtype=torch.float64, device="cuda")
+        y = yb[shift:shift + n]
+        torch.cuda.synchronize()
+        G.spmv(xd.data_ptr(), y.data_ptr(), False)
+        torch.cuda.synchronize()
+        assert np.array_equal(y.cpu().numpy(), ref)
+        # Nothing written outside the n results.
+        out = yb.cpu().numpy()
+        assert out[n if shift == 0 else 0] == 7.0
+    G.close()
 
 
 @pytest.mark.parametrize("nrows,rowlen", [(1, 5000), (3, 2049), (700, 0), (1000, 1)])
