@@ -40,6 +40,14 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+T0 = time.perf_counter()
+
+
+def log(msg):
+    """Progress on stderr (stdout carries only the JSON line)."""
+    print(f"[bench {time.perf_counter() - T0:7.1f} s] {msg}", file=sys.stderr, flush=True)
+
+
 METRIC = "time to 1e-8 FP64 true residual: learned-precond mixed vs plain FP64, same B200"
 TOL_TRUE = 1e-8
 L_DEG = 4
@@ -59,12 +67,72 @@ def args_():
                    help="kappa_batch: the batched workload (64 kappa-diffusion "
                         "systems, BiCGSTAB(2)), one JSON line of its own")
     p.add_argument("--batch-count", type=int, default=64)
+    p.add_argument("--reference-solve-worker", action="store_true",
+                   help=argparse.SUPPRESS)
     p.add_argument("--profile", default=None,
                    choices=["plain_fp64", "mixed_none", "mixed_learned", "spmv"],
                    help="profiling driver: set up, run one warm solve, then "
                         "one solve (or SpMV launches) between "
                         "cudaProfilerStart/Stop, print nothing else")
     return p.parse_args()
+
+
+def usable_cores():
+    """Host cores this process may run on: its CPU affinity, capped by a
+    cgroup CPU quota (containers often see every core of the machine but
+    may use only a share; more OpenMP/BLAS threads than that thrash)."""
+    try:
+        n = len(os.sched_getaffinity(0))
+    except (AttributeError, OSError):
+        n = os.cpu_count() or 1
+    quota = None
+    try:
+        with open("/sys/fs/cgroup/cpu.max") as f:
+            q, per = f.read().split()[:2]
+            if q != "max":
+                quota = float(q) / float(per)
+    except (OSError, ValueError):
+        try:
+            with open("/sys/fs/cgroup/cpu/cpu.cfs_quota_us") as f:
+                q = float(f.read())
+            with open("/sys/fs/cgroup/cpu/cpu.cfs_period_us") as f:
+                per = float(f.read())
+            if q > 0:
+                quota = q / per
+        except (OSError, ValueError):
+            quota = None
+    if quota is not None:
+        n = min(n, max(1, int(quota)))
+    return max(1, n)
+
+
+def reference_full_solve(nx, timeout):
+    """One full reference dbicgstabl solve (oracle/_ref) on usable_cores()
+    threads, in a child process bounded by `timeout` seconds.  Returns
+    (seconds, ret, cores) or (None, reason, cores)."""
+    cores = usable_cores()
+    env = dict(os.environ, OPENBLAS_NUM_THREADS=str(cores), OMP_NUM_THREADS=str(cores))
+    try:
+        out = subprocess.run([sys.executable, os.path.abspath(__file__),
+                              "--reference-solve-worker", "--nx", str(nx)],
+                             env=env, capture_output=True, text=True,
+                             timeout=timeout)
+        d = json.loads(out.stdout.strip().splitlines()[-1])
+        return d["s"], d["ret"], cores
+    except subprocess.TimeoutExpired:
+        return None, f"timed out after {timeout} s", cores
+    except (ValueError, IndexError, KeyError) as e:
+        return None, f"failed: {e}", cores
+
+
+def reference_solve_worker(nx):
+    from oracle import ref as R
+    rp, c, v, n, b = problem(nx)
+    A = R.Matrix(rp, c, v, n)
+    t0 = time.perf_counter()
+    ret, _, _ = R.call("dbicgstabl", A, b, L_DEG, TOL_TRUE, 10000, np.zeros(n))
+    print(json.dumps({"s": time.perf_counter() - t0, "ret": int(ret)}), flush=True)
+    return 0
 
 
 def problem(nx):
@@ -89,17 +157,21 @@ def run_reference(a):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    cores = os.cpu_count() or 1
+    cores = usable_cores()
     os.environ["OPENBLAS_NUM_THREADS"] = str(cores)
     os.environ["OMP_NUM_THREADS"] = str(cores)
+    # Full solve once (warm-up, untimed, child process bounded in time): the
+    # reference's iteration count.
+    full_s, ret_full, cores = reference_full_solve(a.nx, timeout=420)
+    if full_s is None:
+        print(json.dumps({"impl": "reference",
+                          "unavailable": f"reference full solve {ret_full} "
+                                         f"on {cores} host threads"}), flush=True)
+        return 0
+    iters_full = ret_full + 1 if ret_full >= 0 else 10000
     from oracle import ref as R
     rp, c, v, n, b = problem(a.nx)
     A = R.Matrix(rp, c, v, n)
-    # Full solve once (warm-up, untimed): the reference's iteration count.
-    t0 = time.perf_counter()
-    ret_full, outs, _ = R.call("dbicgstabl", A, b, L_DEG, TOL_TRUE, 10000, np.zeros(n))
-    full_s = time.perf_counter() - t0
-    iters_full = ret_full + 1 if ret_full >= 0 else 10000
     sample = 8
     for _ in range(max(a.warmup - 1, 0)):
         R.call("dbicgstabl", A, b, L_DEG, 1e-300, sample, np.zeros(n))
@@ -213,6 +285,7 @@ def run_ours(a):
     nnz = int(rp[-1])
     Ah = B.CsrMatrix(rp, c, v)
     G = B.GpuMatrix(Ah, B.FP32)
+    log(f"operator uploaded (n={n}, nnz={nnz}, variant {G.variant()})")
     dev = torch.device("cuda", local)
     b = torch.from_numpy(b_h).to(dev)
     x = torch.zeros(n, dtype=torch.float64, device=dev)
@@ -266,6 +339,7 @@ def run_ours(a):
     for m_ in train_mats:
         m_.close()
     train_s = time.perf_counter() - t0
+    log(f"preconditioner trained ({train_s:.2f} s)")
 
     def mixed_step(precond, mdl=None):
         def f():
@@ -295,6 +369,7 @@ def run_ours(a):
             ms, (ret_m, st_m) = timed(step, a.steps)
         barrier()
         tr = G.true_residual(b.data_ptr(), x.data_ptr(), sp)
+        log(f"mode {name}: {np.mean(ms):.2f} ms, ret {ret_m}")
         modes[name] = {"s": max_over_ranks(float(np.mean(ms))) / 1e3,
                        "ret": ret_m, "true_residual": tr,
                        "iters": st_m.get("iters", st_m.get("hist_len")),
@@ -356,15 +431,11 @@ def run_ours(a):
     except (OSError, ValueError):
         traffic = None
 
-    # End to end through bksp.h with host arrays (pinned).
-    def pinned(arr):
-        t = torch.from_numpy(np.ascontiguousarray(arr)).pin_memory()
-        return t, t.numpy()
-    _, rp_p = pinned(rp)
-    _, c_p = pinned(c)
-    _, v_p = pinned(v)
-    _, b_p = pinned(b_h)
-    xt_, x_p = pinned(np.zeros(n))
+    # End to end through bksp.h with host arrays (pinned).  The pinned
+    # tensors are kept referenced for as long as their NumPy views are used.
+    pinned_keep = [torch.from_numpy(np.ascontiguousarray(arr)).pin_memory()
+                   for arr in (rp, c, v, b_h, np.zeros(n))]
+    rp_p, c_p, v_p, b_p, x_p = [t.numpy() for t in pinned_keep]
     Ap = B.CsrMatrix(rp_p, c_p, v_p)
     e2e_ms, e2e_rets = [], []
     for i in range(a.warmup + a.steps):
@@ -380,16 +451,19 @@ def run_ours(a):
         if i >= a.warmup:
             e2e_ms.append(dt * 1e3)
     e2e_s = max_over_ranks(float(np.mean(e2e_ms))) / 1e3
+    log(f"e2e: {e2e_s * 1e3:.1f} ms, rets {e2e_rets}")
     e2e_true = float(np.linalg.norm(b_h - P.csr_matvec(rp, c, v, x_p)) /
                      np.linalg.norm(b_h))
-    # CSR operator (FP64 values), b, x0, and the learned preconditioner's
-    # per-row slot map (8 int32 per row) built on the host at upload.
-    h2d = 4 * (n + 1) + 12 * nnz + 16 * n + 32 * n
+    # CSR operator (FP64 values), b and x0; everything else (structure scan,
+    # diagonal form, the learned preconditioner's slot map) is built on the
+    # GPU.
+    h2d = 4 * (n + 1) + 12 * nnz + 16 * n
     d2h = 8 * n
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
-        cpu = cpu_baseline(rp, c, v, n, b_h)
+        cpu = cpu_baseline(a.nx)
+        log(f"cpu baseline: {cpu}")
 
     if rank == 0:
         line = {
@@ -409,7 +483,8 @@ def run_ours(a):
                               "epochs": 200, "probes": 8},
             "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ret": r_e2e, "rets": e2e_rets,
-                    "iters": st_e.get("hist_len"), "true_residual": e2e_true},
+                    "iters": st_e.get("hist_len"), "true_residual": e2e_true,
+                    "call_ms": st_e.get("total_ms"), "solve_ms": st_e.get("solve_ms")},
             "roofline": {"bound": "hbm", "kernel": kname,
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
@@ -462,26 +537,18 @@ def profile_run(a, torch, G, b, x, sp, plain_step, mixed_step, B, n, model):
     return 0
 
 
-def cpu_baseline(rp, c, v, n, b):
-    """One full reference solve on this host (oracle/_ref), all cores."""
-    cores = os.cpu_count() or 1
-    os.environ["OPENBLAS_NUM_THREADS"] = str(cores)
-    os.environ["OMP_NUM_THREADS"] = str(cores)
-    try:
-        from oracle import ref as R
-        if not R.available():
-            return {"value": None, "unit": "s", "cores": cores,
-                    "kind": "reference", "sample": "oracle/_ref not built"}
-        A = R.Matrix(rp, c, v, n)
-        t0 = time.perf_counter()
-        ret, outs, _ = R.call("dbicgstabl", A, b, L_DEG, TOL_TRUE, 10000, np.zeros(n))
-        dt = time.perf_counter() - t0
-        return {"value": dt, "unit": "s", "cores": cores, "kind": "reference",
-                "sample": f"one full dbicgstabl(l={L_DEG}) solve to tol "
-                          f"{TOL_TRUE} (ret {ret})"}
-    except Exception as e:  # the baseline is reported, never required
+def cpu_baseline(nx):
+    """One full reference solve on this host (oracle/_ref), on every usable
+    core, bounded to a few minutes."""
+    from oracle import ref as R
+    cores = usable_cores()
+    if not R.available():
         return {"value": None, "unit": "s", "cores": cores, "kind": "reference",
-                "sample": f"failed: {e}"}
+                "sample": "oracle/_ref not built"}
+    dt, ret, cores = reference_full_solve(nx, timeout=300)
+    return {"value": dt, "unit": "s", "cores": cores, "kind": "reference",
+            "sample": f"one full dbicgstabl(l={L_DEG}) solve to tol {TOL_TRUE} "
+                      f"(ret {ret}), {cores} threads"}
 
 
 def run_batch(a):
@@ -607,6 +674,8 @@ def run_batch(a):
 
 def main():
     a = args_()
+    if a.reference_solve_worker:
+        return reference_solve_worker(a.nx)
     if a.impl == "reference":
         return run_reference(a)
     if a.workload == "kappa_batch":

@@ -77,9 +77,7 @@ void upload_operator(const dspmat* A, bool expand, bool want_fp32, DevCsr& out,
     upload_csr(n, h.rowptr.data(), h.col.data(), h.val.data(), want_fp32, out,
                st);
   } else {
-    for (int k = 0; k < *A->nnz; ++k)
-      if (A->col[k] < 0 || A->col[k] >= n)
-        throw CudaError("matrix: column index out of range");
+    // Column indices are checked by the structure scan on the GPU.
     upload_csr(n, A->row, A->col, A->value, want_fp32, out, st);
   }
 }

@@ -69,12 +69,11 @@ int bksp_gpu_matrix_create(dspmat* A, int flags, bksp_gpu_matrix** out) {
     if (flags & BKSP_GPU_MIRROR) {
       HostCsr h = expand_symmetric(n, A->row, A->col, A->value);
       upload_csr(n, h.rowptr.data(), h.col.data(), h.val.data(), f32, m->A, st);
-      if (f32) spai_build_slots(n, h.rowptr.data(), h.col.data(), m->spai, st);
     } else {
       upload_operator(A, false, f32, m->A, st);
-      if (f32) spai_build_slots(n, A->row, A->col, m->spai, st);
     }
-    host_diag(A, m);
+    if (f32) spai_build_slots(m->A, m->spai, st);
+    m->diag_ok = !(m->A.scan.flags & kScanNoDiag);
     if (flags & BKSP_GPU_TRANSPOSE) {
       HostCsr t = transpose(n, A->row, A->col, A->value);
       upload_csr(n, t.rowptr.data(), t.col.data(), t.val.data(),

@@ -22,7 +22,6 @@ struct bksp_gpu_matrix {
   bk::DevCsr jacobi;
   bool has_jacobi = false;
   bool diag_ok = false;       // every diagonal entry present and non-zero
-  std::vector<double> diag;   // host copy of diag(A)
   bk::SpaiSlots spai;         // learned-preconditioner slot map / features
 };
 
@@ -38,7 +37,6 @@ void download_vec(double* h, const double* d, int n, long long cols,
 void upload_operator(const dspmat* A, bool expand, bool want_fp32, DevCsr& out,
                      cudaStream_t st);
 int hist_cap_for(int max_iter);
-void host_diag(const dspmat* A, bksp_gpu_matrix* m);
 
 // Device + wall timing of one call, reported into the recorded stats.
 struct Timer {

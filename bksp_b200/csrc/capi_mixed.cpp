@@ -14,31 +14,20 @@ using namespace bk;
 
 namespace bk {
 
-// diag(A) on the host (first stored diagonal entry of each row).
-void host_diag(const dspmat* A, bksp_gpu_matrix* m) {
-  const int n = *A->row_size;
-  m->diag.assign(n, 0.0);
-  std::vector<char> seen(n, 0);
-  for (int i = 0; i < n; ++i)
-    for (int k = A->row[i]; k < A->row[i + 1]; ++k)
-      if (A->col[k] == i && !seen[i]) {
-        m->diag[i] = A->value[k];
-        seen[i] = 1;
-      }
-  m->diag_ok = true;
-  for (int i = 0; i < n; ++i)
-    if (m->diag[i] == 0.0) { m->diag_ok = false; break; }
-}
-
+// M = diag(A)^-1 (first stored diagonal entry of each row, from the
+// operator's structure scan) as a one-entry-per-row CSR.
 void build_jacobi(bksp_gpu_matrix* m, cudaStream_t st) {
   if (m->has_jacobi || !m->diag_ok) return;
   const int n = m->A.n;
   std::vector<int> rp(n + 1), col(n);
   std::vector<double> v(n);
+  BK_CHECK(cudaMemcpyAsync(v.data(), m->A.ddiag, sizeof(double) * n,
+                           cudaMemcpyDeviceToHost, st));
+  BK_CHECK(cudaStreamSynchronize(st));
   for (int i = 0; i < n; ++i) {
     rp[i] = i;
     col[i] = i;
-    v[i] = 1.0 / m->diag[i];
+    v[i] = 1.0 / v[i];
   }
   rp[n] = n;
   upload_csr(n, rp.data(), col.data(), v.data(), true, m->jacobi, st);

@@ -67,6 +67,10 @@ __device__ __forceinline__ float warp_sumf(float v) {
 
 // Scalar epilogue dispatcher (epilogues.cuh).
 static __device__ __noinline__ void run_epilogue(const Red& rd);
+// Epilogues touching only S[0 .. kEpiStage) (epilogues.cuh): the last block
+// runs them on a shared-memory copy of those slots.
+constexpr int kEpiStage = 384;
+static __device__ __forceinline__ bool epi_staged(short epi);
 
 // Block-reduce ND per-thread accumulators, publish the block's partials and
 // let the last-arriving block finish the sums into S[out..] and run the
@@ -106,6 +110,15 @@ __device__ __forceinline__ void finish_reduction(const double* acc,
       v += __ldcg(rd.part + d * kMaxBlocks + b);
     tot[d] = warp_sum(v);
   }
+  // The scalar epilogue is a chain of dependent reads and writes of S by
+  // one thread; for the methods whose slots all lie below kEpiStage the
+  // block first copies those slots to shared memory, the thread works on
+  // the copy (shared-memory instead of L2 latency per access), and the
+  // block writes the copy back.
+  __shared__ double Ssh[kEpiStage];
+  const bool stage = epi_staged(rd.epi) && rd.out + ND <= kEpiStage;
+  if (stage)
+    for (int i = threadIdx.x; i < kEpiStage; i += kThreads) Ssh[i] = __ldcg(rd.S + i);
   __syncthreads();
   if (lane == 0) {
 #pragma unroll
@@ -113,16 +126,25 @@ __device__ __forceinline__ void finish_reduction(const double* acc,
   }
   __syncthreads();
   if (threadIdx.x == 0) {
+    double* S = stage ? Ssh : rd.S;
 #pragma unroll
     for (int d = 0; d < ND; ++d) {
       double s = 0.0;
 #pragma unroll
       for (int w = 0; w < kWarps; ++w) s += sh[d][w];
-      rd.S[rd.out + d] = s;
+      S[rd.out + d] = s;
     }
     *rd.ticket = 0u;
     __threadfence();
-    if (rd.epi) run_epilogue(rd);
+    if (rd.epi) {
+      Red r = rd;
+      r.S = S;
+      run_epilogue(r);
+    }
+  }
+  if (stage) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < kEpiStage; i += kThreads) rd.S[i] = Ssh[i];
   }
 }
 

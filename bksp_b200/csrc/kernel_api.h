@@ -136,6 +136,23 @@ void launch_gram_f(const GramH<float>& g, const RedH& rd, cudaStream_t st);
 // Element-wise precision conversions / mixed-precision updates.
 void launch_convert_d2f(const double* a, float* b, long long n, cudaStream_t st);
 void launch_convert_f2d(const float* a, double* b, long long n, cudaStream_t st);
+// Structure scan of an uploaded CSR operator (one thread per row, rows with
+// valid row pointers): flags |= kScanBadCol (a column outside [0, n)),
+// kScanUnsorted (a row whose columns do not strictly ascend), kScanManyOffs
+// (more than kScanOffs distinct column offsets j - i), kScanNoDiag (a row
+// without a non-zero stored diagonal entry); the distinct offsets (up to
+// kScanOffs, unordered, in off[0..noff)); diag[i] = the row's first stored
+// diagonal entry (0 when none).
+constexpr int kScanOffs = 9;
+enum : int { kScanBadCol = 1, kScanUnsorted = 2, kScanManyOffs = 4, kScanNoDiag = 8 };
+struct CsrScanH {
+  int flags;
+  int noff;
+  int off[kScanOffs];
+};
+// scan: device CsrScanH, initialised by the launch.
+void launch_csr_scan(const int* rowptr, const int* col, const double* val, int n,
+                     double* diag, CsrScanH* scan, cudaStream_t st);
 // Scatter CSR values into the diagonal form (dval zero-filled beforehand);
 // mask != nullptr: also write the row masks.
 void launch_csr2dia_d(const CsrH& A, const double* val, double* dval,

@@ -3,6 +3,7 @@
 // the shared launch bookkeeping.  The other kernels live in kernels_spmv.cu,
 // kernels_vec.cu and kernels_block.cu; every translation unit compiles its
 // own copy of the scalar epilogues (epilogues.cuh).
+#include <climits>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -66,6 +67,88 @@ void launch_convert_d2f(const double* a, float* b, long long n, cudaStream_t st)
 void launch_convert_f2d(const float* a, double* b, long long n, cudaStream_t st) {
   ++launch_count();
   k_convert_f2d<<<grid_for(n), kThreads, 0, st>>>(a, b, n);
+}
+
+// ---------------------------------------------------- operator analysis
+
+constexpr int kEmptyOff = INT_MIN;   // never a column offset (|j - i| < n)
+
+// Insert offset o into a table of kScanOffs slots filled front to back
+// (shared or global memory); false when the table is full of other offsets.
+__device__ __forceinline__ bool offset_insert(int* tab, int o) {
+  for (int s = 0; s < kScanOffs; ++s) {
+    const int v = *(volatile int*)(tab + s);
+    if (v == o) return true;
+    if (v == kEmptyOff) {
+      const int prev = atomicCAS(tab + s, kEmptyOff, o);
+      if (prev == kEmptyOff || prev == o) return true;
+    }
+  }
+  return false;
+}
+
+__global__ void __launch_bounds__(kThreads)
+k_csr_scan(const int* __restrict__ rowptr, const int* __restrict__ col,
+           const double* __restrict__ val, int n, double* __restrict__ diag,
+           CsrScanH* scan) {
+  __shared__ int tab[kScanOffs];
+  __shared__ int sflags;
+  if (threadIdx.x < kScanOffs) tab[threadIdx.x] = kEmptyOff;
+  if (threadIdx.x == 0) sflags = 0;
+  __syncthreads();
+  const int i = blockIdx.x * kThreads + threadIdx.x;
+  int fl = 0;
+  if (i < n) {
+    const int k0 = rowptr[i], k1 = rowptr[i + 1];
+    int prev = -1;
+    double d = 0.0;
+    bool has_d = false;
+    for (int k = k0; k < k1; ++k) {
+      const int c = col[k];
+      if (c < 0 || c >= n) {
+        fl |= kScanBadCol;
+        continue;
+      }
+      if (c <= prev) fl |= kScanUnsorted;
+      prev = c;
+      if (c == i && !has_d) {
+        d = val[k];
+        has_d = true;
+      }
+      if (!offset_insert(tab, c - i)) fl |= kScanManyOffs;
+    }
+    if (!has_d || d == 0.0) fl |= kScanNoDiag;
+    diag[i] = d;
+  }
+  if (fl) atomicOr(&sflags, fl);
+  __syncthreads();
+  if (threadIdx.x == 0 && sflags) atomicOr(&scan->flags, sflags);
+  if (threadIdx.x < kScanOffs) {
+    const int o = tab[threadIdx.x];
+    if (o != kEmptyOff && !offset_insert(scan->off, o))
+      atomicOr(&scan->flags, (int)kScanManyOffs);
+  }
+}
+
+__global__ void k_scan_init(CsrScanH* scan) {
+  scan->flags = 0;
+  scan->noff = 0;
+  for (int s = 0; s < kScanOffs; ++s) scan->off[s] = kEmptyOff;
+}
+
+__global__ void k_scan_count(CsrScanH* scan) {
+  int c = 0;
+  for (int s = 0; s < kScanOffs; ++s) c += scan->off[s] != kEmptyOff;
+  scan->noff = c;
+}
+
+void launch_csr_scan(const int* rowptr, const int* col, const double* val, int n,
+                     double* diag, CsrScanH* scan, cudaStream_t st) {
+  launch_count() += 3;
+  k_scan_init<<<1, 1, 0, st>>>(scan);
+  k_csr_scan<<<(n + kThreads - 1) / kThreads, kThreads, 0, st>>>(rowptr, col, val, n,
+                                                                  diag, scan);
+  k_scan_count<<<1, 1, 0, st>>>(scan);
 }
 
 // ------------------------------------------------- mixed-precision steps

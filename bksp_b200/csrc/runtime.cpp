@@ -53,6 +53,8 @@ void DevCsr::release(cudaStream_t st) {
   dfree(rb, st);
   dfree(d64, st);
   dfree(d32, st);
+  dfree(ddiag, st);
+  ddiag = nullptr;
   if (owns_dmask) dfree(dmask, st);
   rowptr = col = rb = nullptr;
   v64 = nullptr;
@@ -159,44 +161,24 @@ std::vector<int> make_row_blocks(int n, const int* rowptr) {
   return rb;
 }
 
-// Diagonal offsets of an operator, or false when it has no useful diagonal
-// form: more than kDiaMax diagonals, a row whose columns do not strictly
-// ascend (its CSR summation order would not be the diagonal order), or a
-// form moving more bytes than CSR in FP64 (nd * 8 n + n >= 12 nnz + 4 n).
-// off comes out ascending.  One pass: a row's offsets ascend, so the
-// pointer into the sorted list only moves forward within a row.
-static bool dia_offsets(int n, const int* rowptr, const int* col, int& nd,
-                        int off[kDiaMax]) {
-  nd = 0;
-  for (int i = 0; i < n; ++i) {
-    int q = 0;
-    long long prev = LLONG_MIN;
-    for (int k = rowptr[i]; k < rowptr[i + 1]; ++k) {
-      const long long o = (long long)col[k] - i;
-      if (o <= prev) return false;
-      prev = o;
-      while (q < nd && off[q] < o) ++q;
-      if (q == nd || off[q] != o) {
-        if (nd == kDiaMax) return false;
-        for (int t = nd; t > q; --t) off[t] = off[t - 1];
-        off[q] = (int)o;
-        ++nd;
-      }
-    }
-  }
-  const double nnz = rowptr[n];
-  return nd > 0 && (double)nd * 8.0 * n + n < 12.0 * nnz + 4.0 * n;
+// The diagonal form is worth keeping when the rows' columns strictly ascend
+// (the diagonal order is then each row's CSR summation order), the entries
+// lie on at most kDiaMax diagonals and the form moves fewer bytes than CSR
+// in FP64 (nd * 8 n + n < 12 nnz + 4 n).
+static bool dia_wanted(const CsrScanH& sc, int n, int nnz) {
+  if (sc.flags & (kScanUnsorted | kScanManyOffs | kScanBadCol)) return false;
+  const int nd = sc.noff;
+  return nd > 0 && nd <= kDiaMax &&
+         (double)nd * 8.0 * n + n < 12.0 * nnz + 4.0 * n;
 }
 
-// Build the diagonal form of an uploaded operator (values of both
-// precisions present, row masks) when it has one.
-static void build_dia(int n, const int* rowptr, const int* col, DevCsr& A,
-                      cudaStream_t st) {
-  int nd = 0, off[kDiaMax] = {};
-  if (!dia_offsets(n, rowptr, col, nd, off)) return;
-  const long long stride = pad64(n);
+// Build the diagonal form of an uploaded, scanned operator (values of both
+// precisions present, row masks).
+static void build_dia(DevCsr& A, cudaStream_t st) {
+  const int nd = A.scan.noff;
+  const long long stride = pad64(A.n);
   A.ndia = nd;
-  for (int d = 0; d < kDiaMax; ++d) A.doff[d] = d < nd ? off[d] : 0;
+  for (int d = 0; d < kDiaMax; ++d) A.doff[d] = d < nd ? A.scan.off[d] : 0;
   A.dmask = dalloc_n<unsigned char>(stride, st);
   A.owns_dmask = true;
   A.d64 = dalloc_n<double>(nd * stride, st);
@@ -352,7 +334,17 @@ void upload_csr(int n, const int* rowptr, const int* col, const double* val,
     launch_convert_d2f(out.v64, out.v32, padn, st);
     BK_CHECK(cudaGetLastError());
   }
-  build_dia(n, rowptr, col, out, st);
+  // Structure scan on the GPU (one small read-back).
+  out.ddiag = dalloc_n<double>(pad64(n), st);
+  CsrScanH* dscan = dalloc_n<CsrScanH>(1, st);
+  launch_csr_scan(out.rowptr, out.col, out.v64, n, out.ddiag, dscan, st);
+  BK_CHECK(cudaGetLastError());
+  BK_CHECK(cudaMemcpyAsync(&out.scan, dscan, sizeof(CsrScanH), cudaMemcpyDeviceToHost, st));
+  dfree(dscan, st);
+  BK_CHECK(cudaStreamSynchronize(st));
+  if (out.scan.flags & kScanBadCol) throw CudaError("matrix: column index out of range");
+  std::sort(out.scan.off, out.scan.off + std::min(out.scan.noff, kScanOffs));
+  if (dia_wanted(out.scan, n, nnz)) build_dia(out, st);
   out.variant = heuristic_variant(n, nnz, out.ndia > 0);
   if (n >= (1 << 16)) autotune_spmv(out, st);
 }

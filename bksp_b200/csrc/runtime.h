@@ -63,6 +63,10 @@ struct DevCsr {
   double* d64 = nullptr;
   float* d32 = nullptr;
   bool owns_dmask = true;   // false for views sharing another operator's masks
+  // Structure scan at upload (kernel_api.h: CsrScanH), offsets ascending,
+  // and the first stored diagonal entry of every row (device, n doubles).
+  CsrScanH scan{};
+  double* ddiag = nullptr;
   CsrH h64() const { return hview(v64, d64); }
   CsrH h32() const { return hview(v32, d32); }
   CsrH hview(const void* v, const void* dv) const {
@@ -96,7 +100,9 @@ HostCsr expand_symmetric(int n, const int* rowptr, const int* col,
 // (src/matvec.c:29-45).
 HostCsr transpose(int n, const int* rowptr, const int* col, const double* val);
 
-// Upload a host CSR (rows in the caller's order) and build its row blocks.
+// Upload a host CSR (rows in the caller's order), scan its structure on the
+// GPU (columns in range -- else CudaError --, diagonal offsets, diagonal),
+// build its row blocks and, when it has one, its diagonal form.
 void upload_csr(int n, const int* rowptr, const int* col, const double* val,
                 bool want_fp32, DevCsr& out, cudaStream_t st);
 

@@ -27,53 +27,32 @@ void SpaiSlots::release(cudaStream_t st) {
   ok = false;
 }
 
-void spai_build_slots(int n, const int* rowptr, const int* col, SpaiSlots& s,
-                      cudaStream_t st) {
+void spai_build_slots(const DevCsr& A, SpaiSlots& s, cudaStream_t st) {
   s.ok = false;
-  // Distinct diagonal offsets; a stencil has few, so a linear table beats
-  // hashing (most entries hit one of the first few offsets).
-  long long offs[kSlots + 1];
-  int noff = 0;
-  for (int i = 0; i < n; ++i)
-    for (int k = rowptr[i]; k < rowptr[i + 1]; ++k) {
-      const long long o = (long long)col[k] - i;
-      int q = 0;
-      while (q < noff && offs[q] != o) ++q;
-      if (q == noff) {
-        if (noff == kSlots) return;   // more diagonals than slots
-        offs[noff++] = o;
-      }
-    }
-  std::vector<long long> neg, pos;
+  // The operator's distinct diagonal offsets come from its structure scan.
+  if (A.scan.flags & (kScanManyOffs | kScanBadCol)) return;
+  const int noff = A.scan.noff;
+  if (noff > kSlots) return;   // more diagonals than slots
+  std::vector<int> neg, pos;
   bool has0 = false;
   for (int q = 0; q < noff; ++q) {
-    if (offs[q] < 0) neg.push_back(offs[q]);
-    else if (offs[q] > 0) pos.push_back(offs[q]);
+    const int o = A.scan.off[q];
+    if (o < 0) neg.push_back(o);
+    else if (o > 0) pos.push_back(o);
     else has0 = true;
   }
   if (!has0 || neg.size() > (size_t)kCenterSlot ||
       pos.size() > (size_t)(kSlots - 1 - kCenterSlot))
     return;
-  std::sort(neg.begin(), neg.end(), [](long long a, long long b) { return a > b; });
+  std::sort(neg.begin(), neg.end(), [](int a, int b) { return a > b; });
   std::sort(pos.begin(), pos.end());
-  long long so[kSlots];
-  int sl[kSlots], ns = 0;
+  int so[kSlots] = {}, sl[kSlots] = {}, ns = 0;
   so[ns] = 0; sl[ns++] = kCenterSlot;
   for (size_t r = 0; r < neg.size(); ++r) { so[ns] = neg[r]; sl[ns++] = kCenterSlot - 1 - (int)r; }
   for (size_t r = 0; r < pos.size(); ++r) { so[ns] = pos[r]; sl[ns++] = kCenterSlot + 1 + (int)r; }
-  std::vector<int> se((size_t)n * kSlots, -1);
-  for (int i = 0; i < n; ++i)
-    for (int k = rowptr[i]; k < rowptr[i + 1]; ++k) {
-      const long long o = (long long)col[k] - i;
-      int q = 0;
-      while (so[q] != o) ++q;
-      int& e = se[(size_t)i * kSlots + sl[q]];
-      if (e < 0) e = k;
-    }
-  s.slot_entry = dalloc_n<int>((long long)n * kSlots, st);
-  BK_CHECK(cudaMemcpyAsync(s.slot_entry, se.data(), sizeof(int) * se.size(),
-                           cudaMemcpyHostToDevice, st));
-  BK_CHECK(cudaStreamSynchronize(st));
+  s.slot_entry = dalloc_n<int>((long long)A.n * kSlots, st);
+  launch_spai_slot_map(A.n, A.rowptr, A.col, so, sl, ns, s.slot_entry, st);
+  BK_CHECK(cudaGetLastError());
   s.ok = true;
 }
 

@@ -32,9 +32,9 @@ struct SpaiSlots {
   void release(cudaStream_t st);
 };
 
-// Host analysis of the uploaded CSR (rows as on the device).
-void spai_build_slots(int n, const int* rowptr, const int* col, SpaiSlots& s,
-                      cudaStream_t st);
+// Slot map of an uploaded, scanned operator (built on the GPU); leaves
+// s.ok false when the operator is not stencil-like.
+void spai_build_slots(const DevCsr& A, SpaiSlots& s, cudaStream_t st);
 // Scratch floats spai_apply needs: M's CSR values (nnz + 8, padded to 64)
 // then, when A has a diagonal form, M's diagonal form.
 long long spai_scratch_floats(const bksp_gpu_matrix* m);

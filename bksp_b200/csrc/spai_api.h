@@ -15,6 +15,11 @@ constexpr int kHidden = 64;      // two hidden layers of this width
 constexpr int kSpaiParams = kHidden * kSlots + kHidden + kHidden * kHidden +
                             kHidden + kSlots * kHidden + kSlots;   // 5256
 
+// slot_entry[i * kSlots + sl[q]] = index of row i's first entry with column
+// offset so[q] (q < ns), -1 where the row has none.
+void launch_spai_slot_map(int n, const int* rowptr, const int* col,
+                          const int* so, const int* sl, int ns, int* slot_entry,
+                          cudaStream_t st);
 void launch_spai_features(int n, const int* rowptr, const double* val,
                           const int* slot_entry, float* feat, float* dinv,
                           cudaStream_t st);

@@ -322,6 +322,42 @@ void launch_spai_features(int n, const int* rowptr, const double* val,
                                                   feat, dinv);
 }
 
+struct SlotTable {
+  int so[kSlots], sl[kSlots];
+  int ns;
+};
+
+__global__ void __launch_bounds__(256)
+k_spai_slot_map(int n, const int* __restrict__ rowptr, const int* __restrict__ col,
+                SlotTable t, int* __restrict__ slot_entry) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int e[kSlots];
+#pragma unroll
+  for (int s = 0; s < kSlots; ++s) e[s] = -1;
+  for (int k = rowptr[i]; k < rowptr[i + 1]; ++k) {
+    const int o = col[k] - i;
+#pragma unroll
+    for (int q = 0; q < kSlots; ++q)
+      if (q < t.ns && t.so[q] == o && e[t.sl[q]] < 0) e[t.sl[q]] = k;
+  }
+#pragma unroll
+  for (int s = 0; s < kSlots; ++s) slot_entry[(long long)i * kSlots + s] = e[s];
+}
+
+void launch_spai_slot_map(int n, const int* rowptr, const int* col,
+                          const int* so, const int* sl, int ns, int* slot_entry,
+                          cudaStream_t st) {
+  ++launch_count();
+  SlotTable t{};
+  for (int q = 0; q < ns && q < kSlots; ++q) {
+    t.so[q] = so[q];
+    t.sl[q] = sl[q];
+  }
+  t.ns = ns < kSlots ? ns : kSlots;
+  k_spai_slot_map<<<(n + 255) / 256, 256, 0, st>>>(n, rowptr, col, t, slot_entry);
+}
+
 void launch_spai_infer(int n, const float* w, const float* feat,
                        const float* dinv, const int* slot_entry, float* mval,
                        cudaStream_t st) {
