@@ -401,8 +401,8 @@ def run_ours(a):
         return e0.elapsed_time(e1) / reps
 
     variants = {}
-    for v, vname in G.SPMV_VARIANTS.items():
-        G.variant(v)
+    for var_id, vname in G.SPMV_VARIANTS.items():
+        G.variant(var_id)
         variants[vname] = {"fp64_ms": time_spmv(xs64, ys64, False),
                            "fp32_ms": time_spmv(xs32, ys32, True)}
     G.variant(tuned)

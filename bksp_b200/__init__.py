@@ -141,6 +141,12 @@ class CsrMatrix:
         self.rowptr = np.ascontiguousarray(rowptr, dtype=np.int32)
         self.col = np.ascontiguousarray(col, dtype=np.int32)
         self.val = np.ascontiguousarray(val, dtype=np.float64)
+        nnz = int(self.rowptr[-1]) if self.rowptr.size else 0
+        if self.rowptr.ndim != 1 or self.rowptr.size < 2:
+            raise ValueError("rowptr must hold n + 1 >= 2 entries")
+        if self.col.shape != (nnz,) or self.val.shape != (nnz,):
+            raise ValueError(f"col and val must hold rowptr[-1] = {nnz} entries "
+                             f"(got {self.col.shape}, {self.val.shape})")
         n = self.rowptr.size - 1 if n is None else int(n)
         self.n = n
         self.symmetric = bool(symmetric)

@@ -210,42 +210,93 @@ static __device__ void fail_divergence(const Red& rd) {
 // arithmetic), the omega / omega'' back substitution, and the update
 // coefficients mapped from the orthogonalised r'_j back onto r_j
 // (r' = r U^-1 with U unit upper, U_ij = tau_ij).
-static __device__ void blf_mr(double* S, int l) {
-  const int M = l + 1;
-  auto G = [&](int i, int j) {
-    if (i > j) { const int t = i; i = j; j = t; }
-    return S[kGramOut + i * M - i * (i - 1) / 2 + (j - i)];
-  };
-  double* tau = S + kBlTau;
-  double* sig = S + kBlSigma;
-  double* omd = S + kBlOmegaD;
-  double h[kBlMaxL + 1];
-  for (int j = 1; j <= l; ++j) {
-    for (int i = 1; i < j; ++i) {
-      double t = G(i, j);
-      for (int k = 1; k < i; ++k) t -= tau[k * l + i] * sig[k] * tau[k * l + j];
-      tau[i * l + j] = t / sig[i];
+// Compile-time degree L: the Gram entries are loaded once (independent
+// loads) and the whole recurrence runs in registers, so the one thread's
+// dependent chain pays register latency, not a memory round trip per step.
+template <int L>
+static __device__ __noinline__ void blf_mr_t(double* S) {
+  constexpr int M = L + 1;
+  double g[M][M];
+#pragma unroll
+  for (int i = 0; i < M; ++i)
+#pragma unroll
+    for (int j = i; j < M; ++j) {
+      const double v = S[kGramOut + i * M - i * (i - 1) / 2 + (j - i)];
+      g[i][j] = v;
+      g[j][i] = v;
     }
-    double sj = G(j, j);
-    for (int k = 1; k < j; ++k) sj -= tau[k * l + j] * tau[k * l + j] * sig[k];
+  double tau[M][M], sig[M], h[M], omd[M], om[M], omdd[M], cr[M], cx[M];
+#pragma unroll
+  for (int j = 1; j <= L; ++j) {
+#pragma unroll
+    for (int i = 1; i < j; ++i) {
+      double t = g[i][j];
+#pragma unroll
+      for (int k = 1; k < i; ++k) t -= tau[k][i] * sig[k] * tau[k][j];
+      tau[i][j] = t / sig[i];
+    }
+    double sj = g[j][j];
+#pragma unroll
+    for (int k = 1; k < j; ++k) sj -= tau[k][j] * tau[k][j] * sig[k];
     sig[j] = sj;
-    double hj = G(0, j);
-    for (int i = 1; i < j; ++i) hj -= tau[i * l + j] * h[i];
+    double hj = g[0][j];
+#pragma unroll
+    for (int i = 1; i < j; ++i) hj -= tau[i][j] * h[i];
     h[j] = hj;
     omd[j] = hj / sj;
   }
-  bl_back_substitution(S, l);
-  double* cr = S + kBlfCr;
-  double* cx = S + kBlfCx;
-  for (int j = 1; j <= l; ++j) {
-    cr[j] = omd[j];
-    cx[j] = j < l ? S[kBlOmegaDD + j] : 0.0;
+  // src/bicgstabl.c:93-109 (bl_back_substitution) on the register copies.
+  om[L] = omd[L];
+#pragma unroll
+  for (int j = L - 1; j > 0; --j) {
+    double t = 0.0;
+#pragma unroll
+    for (int i = j + 1; i <= L; ++i) t += tau[j][i] * om[i];
+    om[j] = omd[j] - t;
   }
-  for (int i = l - 1; i >= 1; --i)
-    for (int j = i + 1; j <= l; ++j) {
-      cr[i] -= tau[i * l + j] * cr[j];
-      cx[i] -= tau[i * l + j] * cx[j];
+#pragma unroll
+  for (int j = 1; j < L; ++j) {
+    double t = 0.0;
+#pragma unroll
+    for (int i = j + 1; i < L; ++i) t += tau[j][i] * om[i + 1];
+    omdd[j] = om[j + 1] + t;
+  }
+#pragma unroll
+  for (int j = 1; j <= L; ++j) {
+    cr[j] = omd[j];
+    cx[j] = j < L ? omdd[j] : 0.0;
+  }
+#pragma unroll
+  for (int i = L - 1; i >= 1; --i)
+#pragma unroll
+    for (int j = i + 1; j <= L; ++j) {
+      cr[i] -= tau[i][j] * cr[j];
+      cx[i] -= tau[i][j] * cx[j];
     }
+#pragma unroll
+  for (int j = 1; j <= L; ++j) {
+#pragma unroll
+    for (int i = 1; i < j; ++i) S[kBlTau + i * L + j] = tau[i][j];
+    S[kBlSigma + j] = sig[j];
+    S[kBlOmegaD + j] = omd[j];
+    S[kBlOmega + j] = om[j];
+    if (j < L) S[kBlOmegaDD + j] = omdd[j];
+    S[kBlfCr + j] = cr[j];
+    S[kBlfCx + j] = cx[j];
+  }
+}
+
+static __device__ void blf_mr(double* S, int l) {
+  switch (l) {
+    case 1: blf_mr_t<1>(S); break;
+    case 2: blf_mr_t<2>(S); break;
+    case 3: blf_mr_t<3>(S); break;
+    case 4: blf_mr_t<4>(S); break;
+    case 5: blf_mr_t<5>(S); break;
+    case 6: blf_mr_t<6>(S); break;
+    case 7: blf_mr_t<7>(S); break;
+    default: blf_mr_t<8>(S); break;
+  }
 }
 
 __device__ __forceinline__ void bl_beta0(double* S, int l, double g1) {

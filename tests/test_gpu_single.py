@@ -280,3 +280,30 @@ def test_nan_breakdown_is_divergence(gpu):
     A = gpu.CsrMatrix(rp, np.arange(n, dtype=np.int32), np.zeros(n))
     x = np.zeros(n)
     assert gpu.dbicgstab(A, np.ones(n), 1e-10, 50, x) == gpu.DIVERGENCE
+
+
+def test_structure_scan_rejects_bad_columns(gpu, testmats):
+    """Column indices outside [0, n) are found by the GPU structure scan and
+    rejected with INVALID_PARAMETERS, by the handle API and by bksp.h calls;
+    a zero diagonal entry makes a Jacobi-preconditioned solve unavailable."""
+    import torch
+    rp, c, v = testmats["pde_rowptr"], testmats["pde_col"], testmats["pde_val"]
+    n = rp.size - 1
+    for bad in (-1, n, n + 1000):
+        c2 = c.copy()
+        c2[rp[n // 2] + 1] = bad
+        A = gpu.CsrMatrix(rp, c2, v)
+        with pytest.raises(RuntimeError):
+            gpu.GpuMatrix(A)
+        x = np.zeros(n)
+        assert gpu.dbicgstab(A, np.ones(n), 1e-10, 100, x) == -3
+    rows = np.repeat(np.arange(n), np.diff(rp))
+    v2 = v.copy()
+    v2[np.flatnonzero(c == rows)[7]] = 0.0
+    G = gpu.GpuMatrix(gpu.CsrMatrix(rp, c, v2), gpu.FP32)
+    bd = torch.ones(n, dtype=torch.float64, device="cuda")
+    xd = torch.zeros(n, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    ret, _ = G.solve_mixed(bd.data_ptr(), xd.data_ptr(), l=2, target=1e-8, precond=1)
+    assert ret == -3
+    G.close()
