@@ -45,10 +45,23 @@ __device__ __forceinline__ bool finished(const Ctl* c) {
   return *(volatile const int*)&c->done != 0;
 }
 
+// Programmatic dependent launch: the solve-loop kernels are launched
+// allowed to start while their predecessor in the stream is still running
+// (its last CTA's scalar epilogue, typically).  A kernel waits here until
+// the predecessor has completed and its memory is visible -- before its
+// first access to anything the predecessor may write -- and then lets its
+// own successor be scheduled.  Both instructions are no-ops for a launch
+// without the attribute.
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // Entry test of every kernel: the solve has finished, or the launch is
 // guarded by a scalar slot that is currently zero (conditional steps such
 // as a residual replacement inside a captured iteration).
 __device__ __forceinline__ bool skip(const Red& rd) {
+  pdl_enter();
   if (finished(rd.ctl)) return true;
   return rd.guard > 0 && *(volatile const double*)(rd.S + rd.guard) == 0.0;
 }

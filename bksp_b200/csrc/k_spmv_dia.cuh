@@ -175,6 +175,7 @@ k_spmv_dia(CsrH A, SpmvH<XT> io, Red rd) {
 template <typename T>
 __global__ void k_csr2dia(CsrH A, const T* __restrict__ val, T* __restrict__ dval,
                           unsigned char* __restrict__ mask) {
+  pdl_enter();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= A.n) return;
   const int k0 = A.rowptr[i], k1 = A.rowptr[i + 1];

@@ -179,9 +179,9 @@ void launch_mx_d2f(const double* in, float* o0, float* o1, float* o2,
                    cudaStream_t st) {
   ++launch_count();
   if (nd)
-    k_mx_d2f<1><<<grid_wave(k_mx_d2f<1>, n), kThreads, 0, st>>>(in, o0, o1, o2, w, n, rd);
+    launch_k(k_mx_d2f<1>, grid_wave(k_mx_d2f<1>, n), kThreads, 0, st, in, o0, o1, o2, w, n, rd);
   else
-    k_mx_d2f<0><<<grid_wave(k_mx_d2f<0>, n), kThreads, 0, st>>>(in, o0, o1, o2, w, n, rd);
+    launch_k(k_mx_d2f<0>, grid_wave(k_mx_d2f<0>, n), kThreads, 0, st, in, o0, o1, o2, w, n, rd);
 }
 
 // x64 += t32 (the preconditioned correction M y), then y32 = 0.
@@ -199,7 +199,7 @@ k_mx_accum(double* __restrict__ x, const float* __restrict__ t,
 void launch_mx_accum(double* x, const float* t, float* y, long long n,
                      const RedH& rd, cudaStream_t st) {
   ++launch_count();
-  k_mx_accum<<<grid_wave(k_mx_accum, n), kThreads, 0, st>>>(x, t, y, n, rd);
+  launch_k(k_mx_accum, grid_wave(k_mx_accum, n), kThreads, 0, st, x, t, y, n, rd);
 }
 
 // ------------------------------------------------------- scalar / control
@@ -231,11 +231,14 @@ void launch_ctl_init(CtlH* c, unsigned* ticket, double* S, int iter0,
                               hist_cap, slot, value);
 }
 
-__global__ void k_set_scalar(double* S, short slot, double v) { S[slot] = v; }
+__global__ void k_set_scalar(double* S, short slot, double v) {
+  pdl_enter();
+  S[slot] = v;
+}
 
 void launch_set_scalar(double* S, short slot, double v, cudaStream_t st) {
   ++launch_count();
-  k_set_scalar<<<1, 1, 0, st>>>(S, slot, v);
+  launch_k(k_set_scalar, 1, 1, 0, st, S, slot, v);
 }
 
 __global__ void k_epilogue(Red rd) {
@@ -245,7 +248,7 @@ __global__ void k_epilogue(Red rd) {
 
 void launch_epilogue(const RedH& rd, cudaStream_t st) {
   ++launch_count();
-  k_epilogue<<<1, 1, 0, st>>>(rd);
+  launch_k(k_epilogue, 1, 1, 0, st, rd);
 }
 
 // Body-final node of a solve's CUDA-graph while loop.  The loop ends when a
@@ -254,6 +257,7 @@ void launch_epilogue(const RedH& rd, cudaStream_t st) {
 // so a device-side loop can never outlive its iteration budget.
 __global__ void k_loop_control(Ctl* c, cudaGraphConditionalHandle h,
                                int use_handle) {
+  pdl_enter();
   const int trips = ++c->trips;
   bool keep = !c->done;
   if (keep && trips >= c->trip_cap) {
@@ -267,7 +271,7 @@ __global__ void k_loop_control(Ctl* c, cudaGraphConditionalHandle h,
 void launch_loop_control(CtlH* ctl, unsigned long long handle, int use_handle,
                          cudaStream_t st) {
   ++launch_count();
-  k_loop_control<<<1, 1, 0, st>>>(ctl, (cudaGraphConditionalHandle)handle,
+  launch_k(k_loop_control, 1, 1, 0, st, ctl, (cudaGraphConditionalHandle)handle,
                                   use_handle);
 }
 

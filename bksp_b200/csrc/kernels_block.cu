@@ -21,10 +21,10 @@ void launch_shift(const ShiftArgsH& a, const RedH& rd, cudaStream_t st) {
   ++launch_count();
   ShiftArgs s{a.r, a.p, a.x, a.xs, a.ps, a.np, a.ns, a.l, a.j, a.mode};
   switch (a.mode) {
-    case 0: k_shift<0><<<grid_wave(k_shift<0>, a.np), kThreads, 0, st>>>(s, rd); break;
-    case 1: k_shift<1><<<grid_wave(k_shift<1>, a.np), kThreads, 0, st>>>(s, rd); break;
-    case 2: k_shift<2><<<grid_wave(k_shift<2>, a.np), kThreads, 0, st>>>(s, rd); break;
-    default: k_shift<3><<<grid_wave(k_shift<3>, a.np), kThreads, 0, st>>>(s, rd); break;
+    case 0: launch_k(k_shift<0>, grid_wave(k_shift<0>, a.np), kThreads, 0, st, s, rd); break;
+    case 1: launch_k(k_shift<1>, grid_wave(k_shift<1>, a.np), kThreads, 0, st, s, rd); break;
+    case 2: launch_k(k_shift<2>, grid_wave(k_shift<2>, a.np), kThreads, 0, st, s, rd); break;
+    default: launch_k(k_shift<3>, grid_wave(k_shift<3>, a.np), kThreads, 0, st, s, rd); break;
   }
 }
 
@@ -35,9 +35,9 @@ void launch_spmm(const CsrH& A, const SpmmH& a, const RedH& rd, cudaStream_t st)
   SpmmArgs s{a.X, a.Y, a.C, a.W, a.alpha, a.mode, a.s, a.nd};
   const int g = grid_for((long long)A.n * kBlkS);
   switch (a.nd) {
-    case 0: k_spmm<0><<<g, kThreads, 0, st>>>(A, s, rd); break;
-    case 1: k_spmm<1><<<g, kThreads, 0, st>>>(A, s, rd); break;
-    default: k_spmm<2><<<g, kThreads, 0, st>>>(A, s, rd); break;
+    case 0: launch_k(k_spmm<0>, g, kThreads, 0, st, A, s, rd); break;
+    case 1: launch_k(k_spmm<1>, g, kThreads, 0, st, A, s, rd); break;
+    default: launch_k(k_spmm<2>, g, kThreads, 0, st, A, s, rd); break;
   }
 }
 
@@ -49,7 +49,7 @@ void launch_block(const BlkH& a, const RedH& rd, cudaStream_t st) {
   const long long tiles = (a.n + kBlkTileRows - 1) / kBlkTileRows;
   int g = (int)(tiles < kMaxBlocks ? tiles : kMaxBlocks);
   if (g < 1) g = 1;
-  k_block<<<g, kThreads, 0, st>>>(b, rd);
+  launch_k(k_block, g, kThreads, 0, st, b, rd);
 }
 
 // Column-major n x s (leading dimension n) <-> row-major np x s.

@@ -52,10 +52,10 @@ static void spmv_vec_launch(const CsrH& A, const SpmvH<XT>& io, const RedH& rd,
   if (g > kMaxBlocks) g = kMaxBlocks;
   if (g < 1) g = 1;
   switch (io.nd) {
-    case 0: k_spmv_vec<VT, XT, 0, L><<<(int)g, kThreads, 0, st>>>(A, io, rd); break;
-    case 1: k_spmv_vec<VT, XT, 1, L><<<(int)g, kThreads, 0, st>>>(A, io, rd); break;
-    case 2: k_spmv_vec<VT, XT, 2, L><<<(int)g, kThreads, 0, st>>>(A, io, rd); break;
-    default: k_spmv_vec<VT, XT, 3, L><<<(int)g, kThreads, 0, st>>>(A, io, rd); break;
+    case 0: launch_k(k_spmv_vec<VT, XT, 0, L>, (int)g, kThreads, 0, st, A, io, rd); break;
+    case 1: launch_k(k_spmv_vec<VT, XT, 1, L>, (int)g, kThreads, 0, st, A, io, rd); break;
+    case 2: launch_k(k_spmv_vec<VT, XT, 2, L>, (int)g, kThreads, 0, st, A, io, rd); break;
+    default: launch_k(k_spmv_vec<VT, XT, 3, L>, (int)g, kThreads, 0, st, A, io, rd); break;
   }
 }
 
@@ -86,7 +86,7 @@ static void spmv_tma_launch(const CsrH& A, const SpmvH<XT>& io, const RedH& rd,
   int g = kSMs * blocks_per_sm;
   if (g > kMaxBlocks) g = kMaxBlocks;
   if (g > A.nrb) g = A.nrb > 0 ? A.nrb : 1;
-  k_spmv_tma<VT, XT, ND><<<g, kThreads, sm, st>>>(A, io, rd);
+  launch_k(k_spmv_tma<VT, XT, ND>, g, kThreads, sm, st, A, io, rd);
 }
 
 static inline bool aligned16(const void* p) {
@@ -106,10 +106,10 @@ static void spmv_dia_launch(const CsrH& A, const SpmvH<XT>& io, const RedH& rd,
                             cudaStream_t st) {
   const long long groups = ((long long)A.n + 3) / 4;   // 4 rows per thread
   switch (io.nd) {
-    case 0: k_spmv_dia<VT, XT, 0><<<grid_wave(k_spmv_dia<VT, XT, 0>, groups), kThreads, 0, st>>>(A, io, rd); break;
-    case 1: k_spmv_dia<VT, XT, 1><<<grid_wave(k_spmv_dia<VT, XT, 1>, groups), kThreads, 0, st>>>(A, io, rd); break;
-    case 2: k_spmv_dia<VT, XT, 2><<<grid_wave(k_spmv_dia<VT, XT, 2>, groups), kThreads, 0, st>>>(A, io, rd); break;
-    default: k_spmv_dia<VT, XT, 3><<<grid_wave(k_spmv_dia<VT, XT, 3>, groups), kThreads, 0, st>>>(A, io, rd); break;
+    case 0: launch_k(k_spmv_dia<VT, XT, 0>, grid_wave(k_spmv_dia<VT, XT, 0>, groups), kThreads, 0, st, A, io, rd); break;
+    case 1: launch_k(k_spmv_dia<VT, XT, 1>, grid_wave(k_spmv_dia<VT, XT, 1>, groups), kThreads, 0, st, A, io, rd); break;
+    case 2: launch_k(k_spmv_dia<VT, XT, 2>, grid_wave(k_spmv_dia<VT, XT, 2>, groups), kThreads, 0, st, A, io, rd); break;
+    default: launch_k(k_spmv_dia<VT, XT, 3>, grid_wave(k_spmv_dia<VT, XT, 3>, groups), kThreads, 0, st, A, io, rd); break;
   }
 }
 
@@ -140,20 +140,20 @@ static void spmv_dispatch(const CsrH& A, const SpmvH<XT>& io, const RedH& rd,
     case 6: {
       const int g = A.nrb < kMaxBlocks ? (A.nrb > 0 ? A.nrb : 1) : kMaxBlocks;
       switch (io.nd) {
-        case 0: k_spmv_wtile<VT, XT, 0><<<g, kThreads, 0, st>>>(A, io, rd); return;
-        case 1: k_spmv_wtile<VT, XT, 1><<<g, kThreads, 0, st>>>(A, io, rd); return;
-        case 2: k_spmv_wtile<VT, XT, 2><<<g, kThreads, 0, st>>>(A, io, rd); return;
-        default: k_spmv_wtile<VT, XT, 3><<<g, kThreads, 0, st>>>(A, io, rd); return;
+        case 0: launch_k(k_spmv_wtile<VT, XT, 0>, g, kThreads, 0, st, A, io, rd); return;
+        case 1: launch_k(k_spmv_wtile<VT, XT, 1>, g, kThreads, 0, st, A, io, rd); return;
+        case 2: launch_k(k_spmv_wtile<VT, XT, 2>, g, kThreads, 0, st, A, io, rd); return;
+        default: launch_k(k_spmv_wtile<VT, XT, 3>, g, kThreads, 0, st, A, io, rd); return;
       }
     }
     default: break;
   }
   const int g = A.nrb < kMaxBlocks ? (A.nrb > 0 ? A.nrb : 1) : kMaxBlocks;
   switch (io.nd) {
-    case 0: k_spmv<VT, XT, 0><<<g, kThreads, 0, st>>>(A, io, rd); break;
-    case 1: k_spmv<VT, XT, 1><<<g, kThreads, 0, st>>>(A, io, rd); break;
-    case 2: k_spmv<VT, XT, 2><<<g, kThreads, 0, st>>>(A, io, rd); break;
-    default: k_spmv<VT, XT, 3><<<g, kThreads, 0, st>>>(A, io, rd); break;
+    case 0: launch_k(k_spmv<VT, XT, 0>, g, kThreads, 0, st, A, io, rd); break;
+    case 1: launch_k(k_spmv<VT, XT, 1>, g, kThreads, 0, st, A, io, rd); break;
+    case 2: launch_k(k_spmv<VT, XT, 2>, g, kThreads, 0, st, A, io, rd); break;
+    default: launch_k(k_spmv<VT, XT, 3>, g, kThreads, 0, st, A, io, rd); break;
   }
 }
 
@@ -171,12 +171,12 @@ void launch_spmv_f(const CsrH& A, const SpmvH<float>& io, const RedH& rd,
 void launch_csr2dia_d(const CsrH& A, const double* val, double* dval,
                       unsigned char* mask, cudaStream_t st) {
   ++launch_count();
-  k_csr2dia<double><<<(A.n + 255) / 256, 256, 0, st>>>(A, val, dval, mask);
+  launch_k(k_csr2dia<double>, (A.n + 255) / 256, 256, 0, st, A, val, dval, mask);
 }
 void launch_csr2dia_f(const CsrH& A, const float* val, float* dval,
                       unsigned char* mask, cudaStream_t st) {
   ++launch_count();
-  k_csr2dia<float><<<(A.n + 255) / 256, 256, 0, st>>>(A, val, dval, mask);
+  launch_k(k_csr2dia<float>, (A.n + 255) / 256, 256, 0, st, A, val, dval, mask);
 }
 
 }  // namespace bk

@@ -20,10 +20,10 @@ template <typename T, int MI, int MO>
 static void lc_nd(const LcH<T>& d, const RedH& rd, cudaStream_t st) {
   const long long q = d.n / Pack<T>::N;
   switch (d.nd) {
-    case 0: k_lincomb<T, MI, MO, 0><<<grid_wave(k_lincomb<T, MI, MO, 0>, q), kThreads, 0, st>>>(d, rd); break;
-    case 1: k_lincomb<T, MI, MO, 1><<<grid_wave(k_lincomb<T, MI, MO, 1>, q), kThreads, 0, st>>>(d, rd); break;
-    case 2: k_lincomb<T, MI, MO, 2><<<grid_wave(k_lincomb<T, MI, MO, 2>, q), kThreads, 0, st>>>(d, rd); break;
-    default: k_lincomb<T, MI, MO, 3><<<grid_wave(k_lincomb<T, MI, MO, 3>, q), kThreads, 0, st>>>(d, rd); break;
+    case 0: launch_k(k_lincomb<T, MI, MO, 0>, grid_wave(k_lincomb<T, MI, MO, 0>, q), kThreads, 0, st, d, rd); break;
+    case 1: launch_k(k_lincomb<T, MI, MO, 1>, grid_wave(k_lincomb<T, MI, MO, 1>, q), kThreads, 0, st, d, rd); break;
+    case 2: launch_k(k_lincomb<T, MI, MO, 2>, grid_wave(k_lincomb<T, MI, MO, 2>, q), kThreads, 0, st, d, rd); break;
+    default: launch_k(k_lincomb<T, MI, MO, 3>, grid_wave(k_lincomb<T, MI, MO, 3>, q), kThreads, 0, st, d, rd); break;
   }
 }
 
@@ -54,11 +54,11 @@ static void gram_dispatch(const GramH<T>& g, const RedH& rd, cudaStream_t st) {
   switch (g.m) {
 #define BK_GRAM(M)                                                        \
   case M:                                                                 \
-    k_gram_vec<T, M><<<grid_wave(k_gram_vec<T, M>, q), kThreads, 0, st>>>(g, rd); \
+    launch_k(k_gram_vec<T, M>, grid_wave(k_gram_vec<T, M>, q), kThreads, 0, st, g, rd); \
     break;
     BK_GRAM(2) BK_GRAM(3) BK_GRAM(4) BK_GRAM(5) BK_GRAM(6) BK_GRAM(7) BK_GRAM(8)
     default:
-      k_gram_vec<T, 9><<<grid_wave(k_gram_vec<T, 9>, q), kThreads, 0, st>>>(g, rd);
+      launch_k(k_gram_vec<T, 9>, grid_wave(k_gram_vec<T, 9>, q), kThreads, 0, st, g, rd);
       break;
 #undef BK_GRAM
   }

@@ -3,6 +3,10 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <cstdlib>
+#include <cstring>
+#include <utility>
+
 #include "dev_common.cuh"
 
 namespace bk {
@@ -30,6 +34,34 @@ static int grid_wave(K* kernel, long long items) {
   if (g < 1) g = 1;
   if (g > cap) g = cap;
   return (int)g;
+}
+
+// Launch with programmatic stream serialisation (dev_common.cuh:
+// pdl_enter): the kernel may be scheduled while its predecessor finishes.
+// BKSP_GPU_PDL=0 launches plainly.  Every kernel launched here calls
+// pdl_enter() (directly or through skip()) before touching memory.
+static inline bool pdl_enabled() {
+  static const bool on = [] {
+    const char* e = std::getenv("BKSP_GPU_PDL");
+    return !(e && std::strcmp(e, "0") == 0);
+  }();
+  return on;
+}
+
+template <typename... KArgs, typename... Args>
+static inline void launch_k(void (*kernel)(KArgs...), int grid, int block,
+                            size_t smem, cudaStream_t st, Args&&... args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3((unsigned)block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = pdl_enabled() ? 1 : 0;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
 
 }  // namespace bk

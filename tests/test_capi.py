@@ -51,9 +51,14 @@ def test_invalid_arguments_are_rejected_without_gpu_work():
     assert B.dcr(A, np.ones(2), 1e-8, 10, x) == B.INVALID_MATRIX_TYPE
     assert B.dbicgstabl(A, np.ones(2), 0, 1e-8, 10, x) == B.INVALID_PARAMETERS
     assert B.dbicgstabl(A, np.ones(2), 99, 1e-8, 10, x) == B.INVALID_PARAMETERS
-    # Row pointer inconsistent with nnz.
-    bad = B.CsrMatrix(np.array([0, 1, 3], np.int32), np.array([0, 1], np.int32),
-                      np.array([1.0, 1.0]))
+    # Row pointer inconsistent with the entry arrays: the Python wrapper
+    # refuses to build it; the C entry points reject a dspmat whose nnz
+    # disagrees with row[n].
+    with pytest.raises(ValueError):
+        B.CsrMatrix(np.array([0, 1, 3], np.int32), np.array([0, 1], np.int32),
+                    np.array([1.0, 1.0]))
+    bad = B.CsrMatrix(rp, np.array([0, 1], np.int32), np.array([1.0, 1.0]))
+    bad._nnz.value = 3
     assert B.dbicg(bad, np.ones(2), 1e-8, 10, x) == B.INVALID_PARAMETERS
 
 
