@@ -562,17 +562,31 @@ def run_batch(a):
     batched the same way; sequential_s: the learned solve one system at a
     time."""
     import torch
+    import torch.distributed as dist
     import bksp_b200 as B
     from bksp_b200 import problems as P
-    torch.cuda.set_device(0)
+    from bksp_b200 import shard
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=dev)
+    # Multi-GPU: the systems are independent, so each rank solves its share
+    # of the batch (balanced by stored entries, computed identically on every
+    # rank); only the timings are reduced (max over ranks).
+    edges = P.kappa_batch_edges(a.batch_count)
+    mine = shard.my_share([7.0 * float(L) ** 3 for L in edges], world, rank)
     t0 = time.perf_counter()
-    systems = P.kappa_batch(count=a.batch_count)
+    systems = P.kappa_batch(count=a.batch_count, indices=set(mine))
     gen_s = time.perf_counter() - t0
+    ntot_all = int(sum(int(L) ** 3 for L in edges))
     ntot = sum(s[3] for s in systems)
     nnz = sum(int(s[0][-1]) for s in systems)
     t0 = time.perf_counter()
     mats = [B.GpuMatrix(B.CsrMatrix(rp, c, v), B.FP32) for rp, c, v, n, b in systems]
-    dev = torch.device("cuda", 0)
     bs = [torch.from_numpy(s[4]).to(dev) for s in systems]
     xs = [torch.zeros_like(b) for b in bs]
     # Jacobi right-scaled copies for the FP64 comparator.
@@ -603,12 +617,19 @@ def run_batch(a):
             for x in xs:
                 x.zero_()
             torch.cuda.synchronize()
+            if world > 1:
+                dist.barrier()
             e0.record()
             last = fn()
             e1.record()
             e1.synchronize()
             ms.append(e0.elapsed_time(e1))
-        return float(np.mean(ms)), last
+        t = float(np.mean(ms))
+        if world > 1:
+            tt = torch.tensor([t], dtype=torch.float64, device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            t = float(tt.item())
+        return t, last
 
     def learned(workers=0):
         return lambda: B.solve_mixed_batch(mats, [b.data_ptr() for b in bs],
@@ -637,23 +658,45 @@ def run_batch(a):
                 x.zero_()
             fn()
         if name == "mixed_learned":
-            with Clocks(0) as clk:
+            with Clocks(local) as clk:
                 ms, (ret, st) = timed(fn, k)
         else:
             ms, (ret, st) = timed(fn, k)
         its = [s["hist_len"] for s in st]
-        res[name] = {"s": ms / 1e3, "ret": ret, "worst_true_residual": worst_true_res(scale),
-                     "iters_min": min(its), "iters_max": max(its),
-                     "iters_mean": float(np.mean(its)),
-                     "launches": int(sum(s["launches"] for s in st))}
+        stats = [worst_true_res(scale), -min(its), max(its), float(sum(its)),
+                 float(len(its)), float(sum(s["launches"] for s in st)),
+                 0.0 if ret == 0 else 1.0]
+        if world > 1:
+            t = torch.tensor(stats, dtype=torch.float64, device=dev)
+            for i, op in enumerate((dist.ReduceOp.MAX, dist.ReduceOp.MAX, dist.ReduceOp.MAX,
+                                    dist.ReduceOp.SUM, dist.ReduceOp.SUM, dist.ReduceOp.SUM,
+                                    dist.ReduceOp.MAX)):
+                ti = t[i:i + 1].clone()
+                dist.all_reduce(ti, op=op)
+                stats[i] = float(ti.item())
+        res[name] = {"s": ms / 1e3, "ret": ret if stats[6] == 0 else -1,
+                     "worst_true_residual": stats[0],
+                     "iters_min": int(-stats[1]), "iters_max": int(stats[2]),
+                     "iters_mean": stats[3] / stats[4],
+                     "launches": int(stats[5])}
+    if rank != 0:
+        for m in mats + scaled:
+            m.close()
+        model.close()
+        if world > 1:
+            dist.destroy_process_group()
+        return 0
     line = {
         "metric": "time to 1e-8 FP64 true residual on every system of the batch",
-        "value": res["mixed_learned"]["s"], "unit": "s", "n_gpus": 1,
+        "value": res["mixed_learned"]["s"], "unit": "s", "n_gpus": world,
         "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": res["mixed_learned"]["s"] * 1e3, "higher_is_better": False,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+        "scaling": "strong" if world > 1 else "weak", "vs_baseline": None,
+        "dtype": "f32+f64", "data": "synthetic",
         "config": {"workload": f"kappa_batch_{a.batch_count}", "systems": a.batch_count,
-                   "rows": ntot, "nnz": nnz, "l": 2, "edge": "U{32..96} seed 4",
+                   "rows": ntot_all, "rows_rank0": ntot, "nnz_rank0": nnz, "l": 2,
+                   "edge": "U{32..96} seed 4",
+                   "parallelism": f"systems sharded over {world} GPU(s), no exchange",
                    "kappa": "exp(GRF), corr 0.1, var 1", "rhs": "N(0,1)",
                    "l2": "inputs larger than L2 (FP64 CSR %.0f MB)" % ((nnz * 12 + 4 * ntot) / 1e6)},
         "plain_fp64_s": res["plain_fp64"]["s"],
@@ -669,6 +712,8 @@ def run_batch(a):
     for m in mats + scaled:
         m.close()
     model.close()
+    if world > 1:
+        dist.destroy_process_group()
     return 0
 
 

@@ -84,6 +84,12 @@ int bksp_gpu_matrix_create(dspmat* A, int flags, bksp_gpu_matrix** out) {
     *out = m;
     return 0;
   } catch (const std::exception& e) {
+    cudaStream_t st = Ctx::get().st;
+    cudaStreamSynchronize(st);
+    m->A.release(st);
+    m->At.release(st);
+    m->spai.release(st);
+    cudaStreamSynchronize(st);
     delete m;
     return fail(e);
   }

@@ -306,19 +306,17 @@ void upload_csr(int n, const int* rowptr, const int* col, const double* val,
   if (n <= 0) throw CudaError("matrix: empty");
   const int nnz = rowptr[n];
   if (rowptr[0] != 0 || nnz < 0) throw CudaError("matrix: bad row pointer");
-  for (int i = 0; i < n; ++i)
-    if (rowptr[i + 1] < rowptr[i]) throw CudaError("matrix: bad row pointer");
-  std::vector<int> rb = make_row_blocks(n, rowptr);
   const long long padn = (long long)(nnz + 3) / 4 * 4 + 4;
   out.n = n;
   out.nnz = nnz;
-  out.nrb = (int)rb.size() - 1;
   out.rowptr = dalloc_n<int>(n + 1, st);
   out.col = dalloc_n<int>(padn, st);
   out.v64 = dalloc_n<double>(padn, st);
-  out.rb = dalloc_n<int>((long long)rb.size(), st);
   BK_CHECK(cudaMemsetAsync(out.col, 0, sizeof(int) * padn, st));
   BK_CHECK(cudaMemsetAsync(out.v64, 0, sizeof(double) * padn, st));
+  // The copies run (asynchronously from pinned memory) while the host checks
+  // the row pointers and builds the row blocks below; nothing on the GPU
+  // reads the operator before the check has passed.
   BK_CHECK(cudaMemcpyAsync(out.rowptr, rowptr, sizeof(int) * (n + 1),
                            cudaMemcpyHostToDevice, st));
   if (nnz > 0) {
@@ -327,6 +325,16 @@ void upload_csr(int n, const int* rowptr, const int* col, const double* val,
     BK_CHECK(cudaMemcpyAsync(out.v64, val, sizeof(double) * nnz,
                              cudaMemcpyHostToDevice, st));
   }
+  bool monotone = true;
+  for (int i = 0; i < n && monotone; ++i) monotone = rowptr[i + 1] >= rowptr[i];
+  if (!monotone) {
+    cudaStreamSynchronize(st);   // the copies still read the caller's arrays
+    out.release(st);
+    throw CudaError("matrix: bad row pointer");
+  }
+  std::vector<int> rb = make_row_blocks(n, rowptr);
+  out.nrb = (int)rb.size() - 1;
+  out.rb = dalloc_n<int>((long long)rb.size(), st);
   BK_CHECK(cudaMemcpyAsync(out.rb, rb.data(), sizeof(int) * rb.size(),
                            cudaMemcpyHostToDevice, st));
   if (want_fp32) {
@@ -342,7 +350,10 @@ void upload_csr(int n, const int* rowptr, const int* col, const double* val,
   BK_CHECK(cudaMemcpyAsync(&out.scan, dscan, sizeof(CsrScanH), cudaMemcpyDeviceToHost, st));
   dfree(dscan, st);
   BK_CHECK(cudaStreamSynchronize(st));
-  if (out.scan.flags & kScanBadCol) throw CudaError("matrix: column index out of range");
+  if (out.scan.flags & kScanBadCol) {
+    out.release(st);
+    throw CudaError("matrix: column index out of range");
+  }
   std::sort(out.scan.off, out.scan.off + std::min(out.scan.noff, kScanOffs));
   if (dia_wanted(out.scan, n, nnz)) build_dia(out, st);
   out.variant = heuristic_variant(n, nnz, out.ndia > 0);

@@ -152,14 +152,22 @@ def kappa_diffusion3d(L, seed):
     return rowptr.astype(np.int32), cols[mask].astype(np.int32), vals[mask], n
 
 
-def kappa_batch(count=64, seed=4, lo=32, hi=96, field_seed0=5):
+def kappa_batch_edges(count=64, seed=4, lo=32, hi=96):
+    """Edge lengths L_i ~ U{lo..hi} (seed) of the batched workload."""
+    return np.random.default_rng(seed).integers(lo, hi + 1, count)
+
+
+def kappa_batch(count=64, seed=4, lo=32, hi=96, field_seed0=5, indices=None):
     """The batched workload: `count` kappa-diffusion systems with edge
     lengths L ~ U{lo..hi} (seed), field seeds field_seed0 + i, right-hand
     sides f ~ N(0, 1) (seed field_seed0 + i + 10000).  Returns a list of
-    (rowptr, col, val, n, b)."""
-    Ls = np.random.default_rng(seed).integers(lo, hi + 1, count)
+    (rowptr, col, val, n, b) for all systems, or for `indices` only (the
+    same systems as in the full batch)."""
+    Ls = kappa_batch_edges(count, seed, lo, hi)
     out = []
     for i, L in enumerate(Ls):
+        if indices is not None and i not in indices:
+            continue
         rp, c, v, n = kappa_diffusion3d(int(L), field_seed0 + i)
         b = np.random.default_rng(field_seed0 + i + 10000).standard_normal(n)
         out.append((rp, c, v, n, b))
