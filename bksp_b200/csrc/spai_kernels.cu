@@ -63,6 +63,33 @@ __device__ __forceinline__ void forward(const float* sw, const float (&f)[S],
   }
 }
 
+// Forward pass for inference: the second hidden layer's activations are
+// folded into the output as they are produced (o_s += W3[s][a] relu(z_a), a
+// ascending -- the same fused multiply-adds in the same order as forward()),
+// so h2 never needs registers and the kernel keeps two CTAs per SM.
+__device__ __forceinline__ void forward_infer(const float* sw, const float (&f)[S],
+                                              float (&o)[S]) {
+  float h1[H];
+#pragma unroll
+  for (int a = 0; a < H; ++a) {
+    float z = sw[ob1 + a];
+#pragma unroll
+    for (int s = 0; s < S; ++s) z = fmaf(sw[oW1 + a * S + s], f[s], z);
+    h1[a] = fmaxf(z, 0.0f);
+  }
+#pragma unroll
+  for (int s = 0; s < S; ++s) o[s] = sw[ob3 + s];
+#pragma unroll 4
+  for (int a = 0; a < H; ++a) {
+    float z = sw[ob2 + a];
+#pragma unroll
+    for (int b = 0; b < H; ++b) z = fmaf(sw[oW2 + a * H + b], h1[b], z);
+    const float r = fmaxf(z, 0.0f);
+#pragma unroll
+    for (int s = 0; s < S; ++s) o[s] = fmaf(sw[oW3 + s * H + a], r, o[s]);
+  }
+}
+
 // Forward pass writing the activations to a per-row stage `my` (f at 0,
 // h1 at S, h2 at S + H): bounded register use for the training kernel.
 __device__ __forceinline__ void forward_staged(const float* sw,
@@ -122,7 +149,7 @@ __global__ void k_spai_features(int n, const int* __restrict__ rowptr,
 }
 
 // Inference: M values on A's pattern (entries without a slot get 0).
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 2)
 k_spai_infer(int n, const float* __restrict__ w, const float* __restrict__ feat,
              const float* __restrict__ dinv, const int* __restrict__ slot_entry,
              float* __restrict__ mval) {
@@ -131,10 +158,10 @@ k_spai_infer(int n, const float* __restrict__ w, const float* __restrict__ feat,
   __syncthreads();
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  float f[S], h1[H], h2[H], o[S];
+  float f[S], o[S];
 #pragma unroll
   for (int s = 0; s < S; ++s) f[s] = feat[i * S + s];
-  forward(sw, f, h1, h2, o);
+  forward_infer(sw, f, o);
   const float di = dinv[i];
 #pragma unroll
   for (int s = 0; s < S; ++s) {
