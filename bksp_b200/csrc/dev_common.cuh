@@ -54,6 +54,11 @@ __device__ __forceinline__ bool finished(const Ctl* c) {
 // without the attribute.
 __device__ __forceinline__ void pdl_enter() {
   asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+// Let the successor be scheduled: kernels with a reduction call this when
+// their streaming work is done (finish_reduction), so the successor's launch
+// overlaps the last CTA's serial tail; others trigger implicitly at exit.
+__device__ __forceinline__ void pdl_trigger() {
   asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
@@ -80,10 +85,6 @@ __device__ __forceinline__ float warp_sumf(float v) {
 
 // Scalar epilogue dispatcher (epilogues.cuh).
 static __device__ __noinline__ void run_epilogue(const Red& rd);
-// Epilogues touching only S[0 .. kEpiStage) (epilogues.cuh): the last block
-// runs them on a shared-memory copy of those slots.
-constexpr int kEpiStage = 384;
-static __device__ __forceinline__ bool epi_staged(short epi);
 
 // Block-reduce ND per-thread accumulators, publish the block's partials and
 // let the last-arriving block finish the sums into S[out..] and run the
@@ -93,6 +94,7 @@ __device__ __forceinline__ void finish_reduction(const double* acc,
                                                  const Red& rd) {
   __shared__ double sh[ND > 0 ? ND : 1][kWarps];
   __shared__ int is_last;
+  pdl_trigger();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
   for (int d = 0; d < ND; ++d) {
@@ -100,7 +102,8 @@ __device__ __forceinline__ void finish_reduction(const double* acc,
     if (lane == 0) sh[d][warp] = v;
   }
   __syncthreads();
-  if (threadIdx.x == 0) {
+  const bool single = gridDim.x == 1;   // one CTA: its sums are the totals
+  if (threadIdx.x == 0 && !single) {
 #pragma unroll
     for (int d = 0; d < ND; ++d) {
       double s = 0.0;
@@ -108,30 +111,28 @@ __device__ __forceinline__ void finish_reduction(const double* acc,
       for (int w = 0; w < kWarps; ++w) s += sh[d][w];
       rd.part[d * kMaxBlocks + blockIdx.x] = s;
     }
-    __threadfence();
-    unsigned t = atomicAdd(rd.ticket, 1u);
+    // Release: the partials above are visible to whichever CTA sees this
+    // increment complete the count; acquire: the last CTA sees all of them.
+    unsigned t;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], 1;"
+                 : "=r"(t) : "l"(rd.ticket) : "memory");
     is_last = (t == gridDim.x - 1);
   }
   __syncthreads();
-  if (!is_last) return;
-  __threadfence();
+  if (!single && !is_last) return;
+  if (!single) __threadfence();
   double tot[ND > 0 ? ND : 1];
 #pragma unroll
   for (int d = 0; d < ND; ++d) {
     double v = 0.0;
-    for (int b = threadIdx.x; b < (int)gridDim.x; b += kThreads)
-      v += __ldcg(rd.part + d * kMaxBlocks + b);
+    if (single) {
+      if (threadIdx.x < kWarps) v = sh[d][threadIdx.x];
+    } else {
+      for (int b = threadIdx.x; b < (int)gridDim.x; b += kThreads)
+        v += __ldcg(rd.part + d * kMaxBlocks + b);
+    }
     tot[d] = warp_sum(v);
   }
-  // The scalar epilogue is a chain of dependent reads and writes of S by
-  // one thread; for the methods whose slots all lie below kEpiStage the
-  // block first copies those slots to shared memory, the thread works on
-  // the copy (shared-memory instead of L2 latency per access), and the
-  // block writes the copy back.
-  __shared__ double Ssh[kEpiStage];
-  const bool stage = epi_staged(rd.epi) && rd.out + ND <= kEpiStage;
-  if (stage)
-    for (int i = threadIdx.x; i < kEpiStage; i += kThreads) Ssh[i] = __ldcg(rd.S + i);
   __syncthreads();
   if (lane == 0) {
 #pragma unroll
@@ -139,25 +140,15 @@ __device__ __forceinline__ void finish_reduction(const double* acc,
   }
   __syncthreads();
   if (threadIdx.x == 0) {
-    double* S = stage ? Ssh : rd.S;
 #pragma unroll
     for (int d = 0; d < ND; ++d) {
       double s = 0.0;
 #pragma unroll
       for (int w = 0; w < kWarps; ++w) s += sh[d][w];
-      S[rd.out + d] = s;
+      rd.S[rd.out + d] = s;
     }
-    *rd.ticket = 0u;
-    __threadfence();
-    if (rd.epi) {
-      Red r = rd;
-      r.S = S;
-      run_epilogue(r);
-    }
-  }
-  if (stage) {
-    __syncthreads();
-    for (int i = threadIdx.x; i < kEpiStage; i += kThreads) rd.S[i] = Ssh[i];
+    if (!single) *rd.ticket = 0u;   // visible to the next kernel at exit
+    if (rd.epi) run_epilogue(rd);
   }
 }
 

@@ -307,15 +307,6 @@ __device__ __forceinline__ void bl_beta0(double* S, int l, double g1) {
   S[kBlG1] = g1;
 }
 
-// The single-vector methods (CG .. mixed BiCGSTAB(l)) keep every scalar
-// below kEpiStage (solver_defs.h: at most kGramOut + 45 = 345).
-static __device__ __forceinline__ bool epi_staged(short epi) {
-  return epi > E_NONE && epi < E_SHB_INIT;
-}
-static_assert(kGramOut + (kBlMaxL + 1) * (kBlMaxL + 2) / 2 <= kEpiStage &&
-                  kBlTau + (kBlMaxL + 1) * (kBlMaxL + 1) <= kEpiStage &&
-                  kBlfCx + kBlMaxL + 1 <= kEpiStage && kMxReps < kEpiStage,
-              "single-vector scalars must lie in the staged window");
 
 static __device__ __noinline__ void run_epilogue(const Red& rd) {
   double* S = rd.S;
