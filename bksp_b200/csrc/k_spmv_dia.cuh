@@ -3,23 +3,24 @@
 // convection-diffusion operators).  The values are stored diagonal by
 // diagonal (nd x stride, zero where a row has no entry on that diagonal)
 // with one mask byte per row, so the product streams values with 16-byte
-// coalesced loads and needs no column indices: 4 + w fewer bytes per entry
-// than CSR.
+// coalesced loads and needs no column indices (4 bytes fewer per stored
+// entry than CSR, against one mask byte per row and the zero fill).
 //
 // Each thread owns 4 consecutive rows (16-byte value packets per diagonal).
-// A row adds its products in ascending diagonal
-// order, which is its ascending column order, skipping diagonals its mask
-// does not hold: y = 0; y += a_k x_k over the stored entries, k ascending,
+// A row adds its products in ascending diagonal order, which is its
+// ascending column order, skipping diagonals its mask does not hold:
+// y = 0; y += a_k x_k over the stored entries, k ascending,
 // no FMA -- the CSR order of reference src/matvec.c:11-53 (dcsrgemm0), so
 // FP64 results are bit-identical to the tile kernel's and the reference's.
 // (Only operators whose rows list their columns in ascending order get a
-// diagonal form, see runtime.cpp: build_dia.)
+// diagonal form, see runtime.cpp: dia_wanted.)
 //
 // The x loads depend only on the row index and the offset (bounds checked
 // against n), not on the mask, so every load of a thread is independent
 // and in flight together; diagonals whose offset is a multiple of the
-// 16-byte packet (0, +-nx, +-nx*ny on a grid) read x with vector loads.  Epilogue as in k_spmv: y = A x or y = b - A x,
-// an optional second copy of y, up to three dot products.
+// 16-byte packet (0, +-nx, +-nx*ny on a grid) read x with vector loads.
+// Epilogue as in k_spmv: y = A x or y = b - A x, an optional second copy of
+// y, up to three dot products.
 #pragma once
 #include "dev_common.cuh"
 #include "k_spmv.cuh"

@@ -36,37 +36,11 @@ __device__ __forceinline__ void load_params(float* sw, const float* w) {
   for (int p = threadIdx.x; p < kP; p += blockDim.x) sw[p] = w[p];
 }
 
-// Forward pass of one row; returns o[S], keeps h1, h2.
-__device__ __forceinline__ void forward(const float* sw, const float (&f)[S],
-                                        float (&h1)[H], float (&h2)[H],
-                                        float (&o)[S]) {
-#pragma unroll
-  for (int a = 0; a < H; ++a) {
-    float z = sw[ob1 + a];
-#pragma unroll
-    for (int s = 0; s < S; ++s) z = fmaf(sw[oW1 + a * S + s], f[s], z);
-    h1[a] = fmaxf(z, 0.0f);
-  }
-#pragma unroll
-  for (int a = 0; a < H; ++a) {
-    float z = sw[ob2 + a];
-#pragma unroll
-    for (int b = 0; b < H; ++b) z = fmaf(sw[oW2 + a * H + b], h1[b], z);
-    h2[a] = fmaxf(z, 0.0f);
-  }
-#pragma unroll
-  for (int s = 0; s < S; ++s) {
-    float z = sw[ob3 + s];
-#pragma unroll
-    for (int b = 0; b < H; ++b) z = fmaf(sw[oW3 + s * H + b], h2[b], z);
-    o[s] = z;
-  }
-}
-
-// Forward pass for inference: the second hidden layer's activations are
-// folded into the output as they are produced (o_s += W3[s][a] relu(z_a), a
-// ascending -- the same fused multiply-adds in the same order as forward()),
-// so h2 never needs registers and the kernel keeps two CTAs per SM.
+// Forward pass of one row for inference: the second hidden layer's
+// activations are folded into the output as they are produced
+// (o_s += W3[s][a] relu(z_a), a ascending -- the same fused multiply-adds in
+// the same order as the training pass), so h2 needs no registers and the
+// kernel keeps two CTAs per SM.
 __device__ __forceinline__ void forward_infer(const float* sw, const float (&f)[S],
                                               float (&o)[S]) {
   float h1[H];
