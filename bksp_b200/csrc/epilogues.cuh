@@ -460,6 +460,10 @@ static __device__ __noinline__ void run_epilogue(const Red& rd) {
       const bool rep = rec <= S[kMxTarget] ||
                        rec < S[kMxDelta] * S[kMxLastRep] ||
                        S[kMxSinceRep] >= S[kMxPeriod];
+      // The replacement block runs as a conditional node of the captured
+      // iteration when there is one (only then are its kernels launched).
+      if (c->use_cond)
+        cudaGraphSetConditional((cudaGraphConditionalHandle)c->cond, rep ? 1u : 0u);
       if (rep) {
         S[kMxDoRep] = 1.0;   // the replacement block decides convergence
       } else {

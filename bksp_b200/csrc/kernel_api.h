@@ -42,6 +42,11 @@ struct CtlH {
   int done, iter, ret, max_iter, hist_cap, trips, trip_cap, hist_len;
   double tol;
   double* hist;
+  // Conditional IF node of the captured iteration (runtime.h: cond_block):
+  // its handle, set by the epilogue that decides the branch (use_cond != 0).
+  unsigned long long cond;
+  int use_cond;
+  int cond_pad;
 };
 
 struct RedH {
@@ -117,6 +122,13 @@ struct SpmvH {
   int nd;
   unsigned char dot[kMaxDotsApi][2];   // 0 = y, 1 = b, 2 = w0, 3 = w1
 };
+
+// Programmatic dependent launch is kept off for the kernels of a
+// conditional node's body and for the first launch after such a node (a
+// programmatic edge joins two kernels only): launch_k (launch_util.h)
+// honours these per-thread switches.
+inline thread_local bool g_plain_scope = false;   // every launch plain
+inline thread_local int g_plain_launches = 0;     // the next n launches plain
 
 // ---- launches (kernels.cu) ----
 // Kernel launches issued by this thread (graph replays are added by the

@@ -8,6 +8,7 @@
 #include <utility>
 
 #include "dev_common.cuh"
+#include "kernel_api.h"
 
 namespace bk {
 
@@ -58,7 +59,9 @@ static inline void launch_k(void (*kernel)(KArgs...), int grid, int block,
   cfg.stream = st;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  attr[0].val.programmaticStreamSerializationAllowed = pdl_enabled() ? 1 : 0;
+  const bool plain = g_plain_scope || g_plain_launches > 0;
+  if (g_plain_launches > 0) --g_plain_launches;
+  attr[0].val.programmaticStreamSerializationAllowed = (pdl_enabled() && !plain) ? 1 : 0;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);

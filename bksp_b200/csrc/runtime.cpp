@@ -373,12 +373,71 @@ void SolveState::create(int cap, cudaStream_t st) {
   BK_CHECK(cudaMemsetAsync(ctl, 0, 2 * sizeof(CtlH), st));
 }
 
+void cond_block(SolveState& ss, cudaStream_t st,
+                const std::function<void(cudaStream_t)>& inner) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cs) != cudaSuccess ||
+      cs != cudaStreamCaptureStatusActive) {
+    cudaGetLastError();
+    inner(st);
+    return;
+  }
+  // The capture's graph and its current dependencies (their edge types are
+  // dropped: the conditional node follows them with plain edges).
+  cudaGraph_t g = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  const cudaGraphEdgeData* edges = nullptr;
+  size_t nd = 0;
+  BK_CHECK(cudaStreamGetCaptureInfo_v3(st, &cs, nullptr, &g, &deps, &edges, &nd));
+  std::vector<cudaGraphNode_t> dv(deps, deps + nd);
+  cudaGraphConditionalHandle h;
+  BK_CHECK(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
+  alignas(cudaGraphNodeParams) unsigned char raw[sizeof(cudaGraphNodeParams)];
+  std::memset(raw, 0, sizeof(raw));
+  cudaGraphNodeParams& cp = *reinterpret_cast<cudaGraphNodeParams*>(raw);
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeIf;
+  cp.conditional.size = 1;
+  cudaGraphNode_t node;
+  BK_CHECK(cudaGraphAddNode(&node, g, dv.data(), dv.size(), &cp));
+  if (!ss.side) BK_CHECK(cudaStreamCreateWithFlags(&ss.side, cudaStreamNonBlocking));
+  BK_CHECK(cudaStreamBeginCaptureToGraph(ss.side, cp.conditional.phGraph_out[0], nullptr,
+                                         nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  const long long c0 = launch_count();
+  g_plain_scope = true;
+  try {
+    inner(ss.side);
+  } catch (...) {
+    g_plain_scope = false;
+    cudaGraph_t dropped = nullptr;
+    cudaStreamEndCapture(ss.side, &dropped);
+    if (dropped) cudaGraphDestroy(dropped);
+    throw;
+  }
+  g_plain_scope = false;
+  g_plain_launches = 1;   // the kernel after the node follows it plainly
+  ss.cond_kernels = launch_count() - c0;
+  cudaGraph_t captured = nullptr;
+  BK_CHECK(cudaStreamEndCapture(ss.side, &captured));
+  BK_CHECK(cudaStreamUpdateCaptureDependencies(st, &node, 1,
+                                               cudaStreamSetCaptureDependencies));
+  ss.cond_handle = (unsigned long long)h;
+  ss.has_cond = true;
+}
+
 void SolveState::release(cudaStream_t st) {
   dfree(S, st);
   dfree(ctl, st);
   dfree(part, st);
   dfree(ticket, st);
   dfree(hist, st);
+  if (side) {
+    cudaStreamSynchronize(side);
+    cudaStreamDestroy(side);
+    side = nullptr;
+  }
+  has_cond = false;
   S = nullptr;
   ctl = nullptr;
   ctl_free = nullptr;
@@ -474,14 +533,24 @@ static bool run_graph_while(SolveState& ss,
         cudaSuccess)
       break;
     const long long c0 = launch_count();
-    body(st);
-    launch_loop_control(ss.ctl, (unsigned long long)h, 1, st);
+    ss.has_cond = false;
+    ss.cond_kernels = 0;
+    bool body_ok = true;
+    try {
+      body(st);
+      launch_loop_control(ss.ctl, (unsigned long long)h, 1, st);
+    } catch (const std::exception&) {
+      body_ok = false;   // capture is ended below; the host-polled loop runs
+    }
+    g_plain_scope = false;
+    g_plain_launches = 0;
     body_kernels = launch_count() - c0;
     launch_count() = c0;   // captured, not launched
     cudaGraph_t captured = nullptr;
     const cudaError_t ce = cudaStreamEndCapture(st, &captured);
-    if (ce != cudaSuccess) {
+    if (ce != cudaSuccess || !body_ok) {
       cudaGetLastError();
+      ss.has_cond = false;
       break;
     }
     if (cudaGraphInstantiate(&ex, g, 0) != cudaSuccess) {
@@ -492,6 +561,11 @@ static bool run_graph_while(SolveState& ss,
     ok = true;
   } while (false);
   if (ok) {
+    if (ss.has_cond) {
+      // Hand the conditional node's handle to the device epilogues.
+      struct { unsigned long long cond; int use; int pad; } cc{ss.cond_handle, 1, 0};
+      BK_CHECK(cudaMemcpyAsync(&ss.ctl->cond, &cc, sizeof(cc), cudaMemcpyHostToDevice, st));
+    }
     BK_CHECK(cudaGraphLaunch(ex, st));
     BK_CHECK(cudaStreamSynchronize(st));
   }

@@ -123,6 +123,12 @@ struct SolveState {
   double* hist = nullptr;
   int hist_cap = 0;
   CtlH* ctl_free = nullptr;   // a control block that is never finished
+  // Conditional block of the captured iteration (cond_block): its handle
+  // and the kernels it holds, valid for the solve being captured.
+  bool has_cond = false;
+  unsigned long long cond_handle = 0;
+  long long cond_kernels = 0;
+  cudaStream_t side = nullptr;   // capture stream of the conditional body
   void create(int hist_cap, cudaStream_t st);
   void release(cudaStream_t st);
   // Reset control: iteration index starts at iter0, budget max_iter.
@@ -144,6 +150,14 @@ struct SolveState {
   void set_scalars(short slot, const double* host, int count, cudaStream_t st);
   double get_scalar(short slot, cudaStream_t st) const;
 };
+
+// Inside the body that run_loop captures: launch `inner`'s kernels in a
+// conditional IF node, so they run only in the iterations in which an
+// epilogue upstream sets the node's condition (through ctl->cond); in the
+// others no kernel is launched at all.  Outside a capture (host-polled
+// loop) inner runs directly and its kernels' own guards decide.
+void cond_block(SolveState& ss, cudaStream_t st,
+                const std::function<void(cudaStream_t)>& inner);
 
 // Builder for one fused linear-combination launch (LcH).
 template <typename T>

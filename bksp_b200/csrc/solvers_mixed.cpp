@@ -194,22 +194,26 @@ MixedOut bicgstabl_mixed(const DevCsr& A, const DevCsr* M, const double* b,
       u.dot(OUT + orr, OUT + orr).dot(irs, OUT + orr);
       u.launch(ss.red(kD, E_MX_CHECK), s);
     }
-    // Reliable update, guarded by S[kMxDoRep].
-    const float* corr = y;
-    if (M) {
-      spmv(*M, spmv_io<float>(y, t), ss.red_if(kMxDoRep, kD, E_NONE), s);
-      corr = t;
-    }
-    launch_mx_accum(x, corr, y, np, ss.red_if(kMxDoRep, kD, E_NONE), s);
-    {
-      SpmvH<double> io = spmv_io<double>(x, r64);
-      io.b = b;
-      io.mode = 1;
-      set_dot(io, 0, Y, Y);
-      spmv(A, io, ss.red_if(kMxDoRep, kD, E_MX_TRUE), s);
-    }
-    launch_mx_d2f(r64, R(0), nullptr, nullptr, rs, 1, np,
-                  ss.red_if(kMxDoRep, kD, E_MX_REBETA), s);
+    // Reliable update, guarded by S[kMxDoRep]; in the captured iteration
+    // these kernels sit in a conditional node that E_MX_CHECK opens only
+    // when a replacement is due.
+    cond_block(ss, s, [&](cudaStream_t s2) {
+      const float* corr = y;
+      if (M) {
+        spmv(*M, spmv_io<float>(y, t), ss.red_if(kMxDoRep, kD, E_NONE), s2);
+        corr = t;
+      }
+      launch_mx_accum(x, corr, y, np, ss.red_if(kMxDoRep, kD, E_NONE), s2);
+      {
+        SpmvH<double> io = spmv_io<double>(x, r64);
+        io.b = b;
+        io.mode = 1;
+        set_dot(io, 0, Y, Y);
+        spmv(A, io, ss.red_if(kMxDoRep, kD, E_MX_TRUE), s2);
+      }
+      launch_mx_d2f(r64, R(0), nullptr, nullptr, rs, 1, np,
+                    ss.red_if(kMxDoRep, kD, E_MX_REBETA), s2);
+    });
   };
   const CtlH c = run_loop(ss, body, st);
   // Fold any correction not yet accumulated (budget exhausted / breakdown).
@@ -223,6 +227,11 @@ MixedOut bicgstabl_mixed(const DevCsr& A, const DevCsr* M, const double* b,
   out.ret = c.ret;
   out.iters = c.hist_len;
   out.replacements = (int)ss.get_scalar(kMxReps, st);
+  // The conditional node's kernels ran only in the iterations with a
+  // replacement (run_loop counted them in every trip).
+  if (ss.has_cond)
+    launch_count() -= ss.cond_kernels * (long long)std::max(0, c.trips - out.replacements);
+  ss.has_cond = false;
   out.true_res = ss.get_scalar(kMxTrue, st);
   dfree(w, st);
   dfree(r64, st);
