@@ -1,0 +1,57 @@
+"""The execution modes of the device loop give the same numbers: the
+CUDA-graph while loop (with its conditional replacement node and
+programmatic dependent launch), the same with plain launches, and the
+host-polled loop run the same kernels in the same order, so the solutions
+must agree bit for bit.  Each mode runs in a child process (the switches
+are read once per process)."""
+import json
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+CHILD = r"""
+import json, sys
+import numpy as np, torch
+sys.path.insert(0, sys.argv[1])
+import bksp_b200 as B
+from bksp_b200 import problems as P
+rp, c, v, n = P.convdiff3d(16)
+b_h = P.csr_matvec(rp, c, v, P.uniform(n, 1))
+G = B.GpuMatrix(B.CsrMatrix(rp, c, v), B.FP32)
+b = torch.from_numpy(b_h).cuda()
+out = {}
+for name, fn in (
+        ("fp64", lambda x: G.solve(B.BICGSTABL_FAST, b.data_ptr(), x.data_ptr(), 1e-10, 500, l=4)),
+        ("mixed_none", lambda x: G.solve_mixed(b.data_ptr(), x.data_ptr(), l=4, target=1e-9, precond=0)),
+        ("mixed_jacobi", lambda x: G.solve_mixed(b.data_ptr(), x.data_ptr(), l=2, target=1e-9, precond=1))):
+    x = torch.zeros(n, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    ret, st = fn(x)
+    torch.cuda.synchronize()
+    out[name] = {"ret": ret, "x": x.cpu().numpy().tolist()}
+print(json.dumps(out))
+"""
+
+
+def _run(env_extra):
+    env = dict(os.environ, **env_extra)
+    r = subprocess.run([sys.executable, "-c", CHILD, ROOT], env=env,
+                       capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    return json.loads(r.stdout.strip().splitlines()[-1])
+
+
+def test_loop_modes_agree_bitwise():
+    base = _run({})
+    for extra in ({"BKSP_GPU_PDL": "0"}, {"BKSP_GPU_LOOP": "poll"}):
+        other = _run(extra)
+        for name in base:
+            assert base[name]["ret"] == other[name]["ret"] >= 0, (extra, name)
+            assert np.array_equal(np.array(base[name]["x"]), np.array(other[name]["x"])), (extra, name)
