@@ -101,6 +101,8 @@ def _load():
     L.bksp_gpu_spmv.argtypes = [vp, i, vp, vp, vp]
     L.bksp_gpu_matrix_variant.argtypes = [vp, i]
     L.bksp_gpu_matrix_diagonals.argtypes = [vp, C.POINTER(C.c_int)]
+    L.bksp_gpu_read_matrix_market.argtypes = [C.c_char_p, i, C.POINTER(vp)]
+    L.bksp_gpu_matrix_csr.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), _dp]
     L.bksp_gpu_true_residual.argtypes = [vp, vp, vp, vp]
     L.bksp_gpu_true_residual.restype = d
     L.bksp_gpu_device_count.restype = i
@@ -304,15 +306,39 @@ CG, CR, BICG, BICGSTAB, BICGSTABL, BICGSTABL_FAST = 1, 2, 3, 4, 5, 6
 class GpuMatrix:
     """``bksp_gpu_matrix``: an operator uploaded once and kept in HBM."""
 
-    def __init__(self, A, flags=0):
-        h = C.c_void_p()
-        rc = lib.bksp_gpu_matrix_create(A.ptr, int(flags), C.byref(h))
-        if rc != 0:
-            raise RuntimeError(f"bksp_gpu_matrix_create failed ({rc})")
+    def __init__(self, A, flags=0, _handle=None):
+        if _handle is not None:
+            h = _handle
+        else:
+            h = C.c_void_p()
+            rc = lib.bksp_gpu_matrix_create(A.ptr, int(flags), C.byref(h))
+            if rc != 0:
+                raise RuntimeError(f"bksp_gpu_matrix_create failed ({rc})")
         self.h = h
         n, nnz = C.c_int(), C.c_int()
         lib.bksp_gpu_matrix_info(h, C.byref(n), C.byref(nnz))
         self.n, self.nnz = n.value, nnz.value
+
+    @classmethod
+    def from_matrix_market(cls, path, flags=0):
+        """bksp_gpu_read_matrix_market: a .mtx file straight into GPU memory
+        (rows sorted and, with MIRROR, the triangle mirrored on the GPU)."""
+        h = C.c_void_p()
+        rc = lib.bksp_gpu_read_matrix_market(os.fsencode(path), int(flags), C.byref(h))
+        if rc != 0:
+            raise OSError(f"cannot load Matrix Market file {path} ({rc})")
+        return cls(None, _handle=h)
+
+    def csr(self):
+        """The operator's CSR as stored on the device: (rowptr, col, val)."""
+        rp = np.zeros(self.n + 1, np.int32)
+        col = np.zeros(max(self.nnz, 1), np.int32)
+        val = np.zeros(max(self.nnz, 1))
+        rc = lib.bksp_gpu_matrix_csr(self.h, rp.ctypes.data_as(_ip),
+                                     col.ctypes.data_as(_ip), val.ctypes.data_as(_dp))
+        if rc != 0:
+            raise RuntimeError("bksp_gpu_matrix_csr failed")
+        return rp, col[:self.nnz], val[:self.nnz]
 
     def close(self):
         if self.h:

@@ -165,6 +165,20 @@ struct CsrScanH {
 // scan: device CsrScanH, initialised by the launch.
 void launch_csr_scan(const int* rowptr, const int* col, const double* val, int n,
                      double* diag, CsrScanH* scan, cudaStream_t st);
+// Matrix Market file -> CSR on the GPU (kernels_mm.cu).  Coordinates are
+// 0-based and in file order; with `mirror`, every off-diagonal entry (i, j)
+// also goes to row j (one stored triangle of a symmetric file).
+// cnt[r] += entries of row r (cnt zero-filled beforehand).
+void launch_coo_count(const int* ri, const int* ci, long long nz, int mirror,
+                      int* cnt, cudaStream_t st);
+// Places the entries in their rows (any order within a row; key = source
+// row << 32 | file index); fill zero-filled beforehand.
+void launch_coo_scatter(const int* ri, const int* ci, const double* vv,
+                        long long nz, int mirror, const int* rowptr, int* fill,
+                        int* col, double* val, long long* key, cudaStream_t st);
+// Sorts each row by key (file order) or, with by_col, by (column, key).
+void launch_row_sort(const int* rowptr, int n, int by_col, int* col, double* val,
+                     long long* key, cudaStream_t st);
 // Scatter CSR values into the diagonal form (dval zero-filled beforehand);
 // mask != nullptr: also write the row masks.
 void launch_csr2dia_d(const CsrH& A, const double* val, double* dval,

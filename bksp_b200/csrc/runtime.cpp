@@ -302,7 +302,7 @@ void autotune_spmv(DevCsr& A, cudaStream_t st) {
 }
 
 void upload_csr(int n, const int* rowptr, const int* col, const double* val,
-                bool want_fp32, DevCsr& out, cudaStream_t st) {
+                bool want_fp32, DevCsr& out, cudaStream_t st, bool cv_on_device) {
   if (n <= 0) throw CudaError("matrix: empty");
   const int nnz = rowptr[n];
   if (rowptr[0] != 0 || nnz < 0) throw CudaError("matrix: bad row pointer");
@@ -320,10 +320,10 @@ void upload_csr(int n, const int* rowptr, const int* col, const double* val,
   BK_CHECK(cudaMemcpyAsync(out.rowptr, rowptr, sizeof(int) * (n + 1),
                            cudaMemcpyHostToDevice, st));
   if (nnz > 0) {
-    BK_CHECK(cudaMemcpyAsync(out.col, col, sizeof(int) * nnz,
-                             cudaMemcpyHostToDevice, st));
-    BK_CHECK(cudaMemcpyAsync(out.v64, val, sizeof(double) * nnz,
-                             cudaMemcpyHostToDevice, st));
+    const cudaMemcpyKind kind =
+        cv_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    BK_CHECK(cudaMemcpyAsync(out.col, col, sizeof(int) * nnz, kind, st));
+    BK_CHECK(cudaMemcpyAsync(out.v64, val, sizeof(double) * nnz, kind, st));
   }
   bool monotone = true;
   for (int i = 0; i < n && monotone; ++i) monotone = rowptr[i + 1] >= rowptr[i];

@@ -104,7 +104,8 @@ HostCsr transpose(int n, const int* rowptr, const int* col, const double* val);
 // GPU (columns in range -- else CudaError --, diagonal offsets, diagonal),
 // build its row blocks and, when it has one, its diagonal form.
 void upload_csr(int n, const int* rowptr, const int* col, const double* val,
-                bool want_fp32, DevCsr& out, cudaStream_t st);
+                bool want_fp32, DevCsr& out, cudaStream_t st,
+                bool cv_on_device = false);   // col, val already in GPU memory
 
 // Pick the fastest SpMV kernel variant for A by timing them (cached per
 // operator signature); called by upload_csr for large operators.

@@ -96,6 +96,24 @@ int bksp_gpu_solve(bksp_gpu_matrix *A, int method, int l, const double *b,
  * form when there is one, else by mean row length). */
 int bksp_gpu_matrix_variant(bksp_gpu_matrix *A, int variant);
 
+/* A Matrix Market file (coordinate real / integer / pattern, general or
+ * symmetric, square) straight into a device-resident operator: the text is
+ * parsed on the host by several threads; sorting the entries into rows --
+ * file order within a row, as read_matrix_market (and the reference's
+ * reader, src/read_matrix.c) leaves them -- and, with BKSP_GPU_MIRROR and a
+ * symmetric file, mirroring the stored triangle (rows then in ascending
+ * column order, as bksp_gpu_matrix_create builds them) run on the GPU.
+ * Flags: BKSP_GPU_FP32, BKSP_GPU_MIRROR (BKSP_GPU_TRANSPOSE is not
+ * accepted).  Returns 0 or INVALID_PARAMETERS (unreadable or malformed file,
+ * non-square matrix). */
+int bksp_gpu_read_matrix_market(const char *path, int flags,
+                                bksp_gpu_matrix **out);
+
+/* Copy the operator's CSR (n + 1 row pointers, nnz columns and FP64 values,
+ * as stored on the device; any pointer may be NULL) to host arrays. */
+int bksp_gpu_matrix_csr(const bksp_gpu_matrix *A, int *rowptr, int *col,
+                        double *val);
+
 /* Diagonal form of the operator: an operator whose stored entries lie on at
  * most 8 diagonals, whose rows list their columns in strictly ascending
  * order, and whose diagonal storage is smaller than its CSR storage, is

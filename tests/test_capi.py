@@ -98,3 +98,38 @@ def test_dense_helpers():
     B.lib.dvec2mat(x.ctypes.data_as(C.POINTER(C.c_double)), 1, C.byref(m))
     # reference src/util.c:57-67 writes value[i * col_size + m]
     assert [vals[i * 3 + 1] for i in range(5)] == list(x)
+
+
+def test_read_matrix_market_edge_cases(tmp_path):
+    """CRLF line ends, blank lines, signs and exponents parse; malformed entry
+    lines (bad index, extra token, wrong count) are rejected."""
+    ok = ("%%MatrixMarket matrix coordinate real general\r\n% c\r\n\r\n3 3 3\r\n"
+          "1 1 +2.5e0\r\n\r\n3 2 -1E-3\r\n2 3 4\r\n")
+    (tmp_path / "ok.mtx").write_text(ok)
+    rp, c, v, n, t = B.read_matrix_market(str(tmp_path / "ok.mtx"))
+    assert n == 3 and t == "unsymmetric"
+    assert list(rp) == [0, 1, 2, 3] and list(c) == [0, 2, 1]
+    assert list(v) == [2.5, 4.0, -1e-3]
+    pat = "%%MatrixMarket matrix coordinate pattern symmetric\n2 2 2\n1 1\n2 1\n"
+    (tmp_path / "pat.mtx").write_text(pat)
+    rp, c, v, n, t = B.read_matrix_market(str(tmp_path / "pat.mtx"))
+    assert t == "symmetric" and list(v) == [1.0, 1.0]
+    for body in ("3 3 1\n4 1 2.0\n", "3 3 1\n1 1 2.0 7\n", "3 3 2\n1 1 2.0\n",
+                 "3 3 1\n1 x 2.0\n"):
+        (tmp_path / "bad.mtx").write_text(
+            "%%MatrixMarket matrix coordinate real general\n" + body)
+        with pytest.raises(OSError):
+            B.read_matrix_market(str(tmp_path / "bad.mtx"))
+    # a file large enough to be parsed by several threads
+    rng = np.random.default_rng(0)
+    n = 60000
+    rows = rng.integers(0, n, 400000)
+    cols = rng.integers(0, n, 400000)
+    vals = rng.standard_normal(400000)
+    with open(tmp_path / "big.mtx", "w") as f:
+        f.write(f"%%MatrixMarket matrix coordinate real general\n{n} {n} {rows.size}\n")
+        f.writelines(f"{i + 1} {j + 1} {float(x)!r}\n" for i, j, x in zip(rows, cols, vals))
+    rp, c, v, n2, _ = B.read_matrix_market(str(tmp_path / "big.mtx"))
+    order = np.argsort(rows, kind="stable")
+    assert np.array_equal(c, cols[order]) and np.array_equal(v, vals[order])
+    assert np.array_equal(np.diff(rp), np.bincount(rows, minlength=n))
