@@ -36,31 +36,46 @@ __device__ __forceinline__ void load_params(float* sw, const float* w) {
   for (int p = threadIdx.x; p < kP; p += blockDim.x) sw[p] = w[p];
 }
 
-// Forward pass of one row for inference: the second hidden layer's
+// Forward pass of two rows for inference.  The second hidden layer's
 // activations are folded into the output as they are produced
 // (o_s += W3[s][a] relu(z_a), a ascending -- the same fused multiply-adds in
-// the same order as the training pass), so h2 needs no registers and the
-// kernel keeps two CTAs per SM.
-__device__ __forceinline__ void forward_infer(const float* sw, const float (&f)[S],
-                                              float (&o)[S]) {
-  float h1[H];
+// the same order as the training pass), so h2 needs no registers, and every
+// weight read from shared memory serves both rows (half the shared-memory
+// traffic per fused multiply-add).
+__device__ __forceinline__ void forward_infer2(const float* sw, const float (&f0)[S],
+                                               const float (&f1)[S], float (&o0)[S],
+                                               float (&o1)[S]) {
+  float h0[H], h1[H];
 #pragma unroll
   for (int a = 0; a < H; ++a) {
-    float z = sw[ob1 + a];
+    float z0 = sw[ob1 + a], z1 = z0;
 #pragma unroll
-    for (int s = 0; s < S; ++s) z = fmaf(sw[oW1 + a * S + s], f[s], z);
-    h1[a] = fmaxf(z, 0.0f);
+    for (int s = 0; s < S; ++s) {
+      const float wv = sw[oW1 + a * S + s];
+      z0 = fmaf(wv, f0[s], z0);
+      z1 = fmaf(wv, f1[s], z1);
+    }
+    h0[a] = fmaxf(z0, 0.0f);
+    h1[a] = fmaxf(z1, 0.0f);
   }
 #pragma unroll
-  for (int s = 0; s < S; ++s) o[s] = sw[ob3 + s];
-#pragma unroll 4
+  for (int s = 0; s < S; ++s) o0[s] = o1[s] = sw[ob3 + s];
+#pragma unroll 2
   for (int a = 0; a < H; ++a) {
-    float z = sw[ob2 + a];
+    float z0 = sw[ob2 + a], z1 = z0;
 #pragma unroll
-    for (int b = 0; b < H; ++b) z = fmaf(sw[oW2 + a * H + b], h1[b], z);
-    const float r = fmaxf(z, 0.0f);
+    for (int b = 0; b < H; ++b) {
+      const float wv = sw[oW2 + a * H + b];
+      z0 = fmaf(wv, h0[b], z0);
+      z1 = fmaf(wv, h1[b], z1);
+    }
+    const float r0 = fmaxf(z0, 0.0f), r1 = fmaxf(z1, 0.0f);
 #pragma unroll
-    for (int s = 0; s < S; ++s) o[s] = fmaf(sw[oW3 + s * H + a], r, o[s]);
+    for (int s = 0; s < S; ++s) {
+      const float wv = sw[oW3 + s * H + a];
+      o0[s] = fmaf(wv, r0, o0[s]);
+      o1[s] = fmaf(wv, r1, o1[s]);
+    }
   }
 }
 
@@ -122,25 +137,41 @@ __global__ void k_spai_features(int n, const int* __restrict__ rowptr,
   dinv[i] = (float)di;
 }
 
-// Inference: M values on A's pattern (entries without a slot get 0).
-__global__ void __launch_bounds__(256, 2)
+// Inference: M values on A's pattern (entries without a slot get 0).  Each
+// thread evaluates rows i and i + blockDim.x of its CTA's 2 * blockDim.x.
+constexpr int kInferThreads = 128;
+
+__global__ void __launch_bounds__(kInferThreads)
 k_spai_infer(int n, const float* __restrict__ w, const float* __restrict__ feat,
              const float* __restrict__ dinv, const int* __restrict__ slot_entry,
              float* __restrict__ mval) {
   __shared__ float sw[kP];
   load_params(sw, w);
   __syncthreads();
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  float f[S], o[S];
-#pragma unroll
-  for (int s = 0; s < S; ++s) f[s] = feat[i * S + s];
-  forward_infer(sw, f, o);
-  const float di = dinv[i];
+  const int i0 = blockIdx.x * (2 * kInferThreads) + threadIdx.x;
+  const int i1 = i0 + kInferThreads;
+  if (i0 >= n) return;
+  const bool two = i1 < n;
+  float f0[S], f1[S], o0[S], o1[S];
 #pragma unroll
   for (int s = 0; s < S; ++s) {
-    const int e = slot_entry[i * S + s];
-    if (e >= 0) mval[e] = o[s] * di;
+    f0[s] = feat[(long long)i0 * S + s];
+    f1[s] = two ? feat[(long long)i1 * S + s] : 0.0f;
+  }
+  forward_infer2(sw, f0, f1, o0, o1);
+  const float d0 = dinv[i0];
+#pragma unroll
+  for (int s = 0; s < S; ++s) {
+    const int e = slot_entry[(long long)i0 * S + s];
+    if (e >= 0) mval[e] = o0[s] * d0;
+  }
+  if (two) {
+    const float d1 = dinv[i1];
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+      const int e = slot_entry[(long long)i1 * S + s];
+      if (e >= 0) mval[e] = o1[s] * d1;
+    }
   }
 }
 
@@ -363,8 +394,9 @@ void launch_spai_infer(int n, const float* w, const float* feat,
                        const float* dinv, const int* slot_entry, float* mval,
                        cudaStream_t st) {
   ++launch_count();
-  k_spai_infer<<<(n + 255) / 256, 256, 0, st>>>(n, w, feat, dinv, slot_entry,
-                                               mval);
+  const int rows_per_cta = 2 * kInferThreads;
+  k_spai_infer<<<(n + rows_per_cta - 1) / rows_per_cta, kInferThreads, 0, st>>>(
+      n, w, feat, dinv, slot_entry, mval);
 }
 
 int spai_grad_blocks(int n) { return (n + kTrainThreads - 1) / kTrainThreads; }
