@@ -307,3 +307,24 @@ def test_structure_scan_rejects_bad_columns(gpu, testmats):
     ret, _ = G.solve_mixed(bd.data_ptr(), xd.data_ptr(), l=2, target=1e-8, precond=1)
     assert ret == -3
     G.close()
+
+
+def test_spmv_bit_exact_at_benchmark_size(gpu):
+    """The benchmark operator itself (3D convection-diffusion 128^3, 2.1 M
+    rows): every SpMV variant the autotuner may pick reproduces the
+    reference's row order bit for bit in FP64."""
+    import torch
+    rp, c, v, n = P.convdiff3d(128)
+    x = np.random.default_rng(9).uniform(-1, 1, n)
+    ref = _row_sums_sequential(rp, c, v, x)
+    G = gpu.GpuMatrix(gpu.CsrMatrix(rp, c, v))
+    assert len(G.diagonals()) == 7
+    xd = torch.from_numpy(x).cuda()
+    for variant in (7, 0, 6):
+        G.variant(variant)
+        yd = torch.zeros(n, dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        G.spmv(xd.data_ptr(), yd.data_ptr(), False)
+        torch.cuda.synchronize()
+        assert np.array_equal(yd.cpu().numpy(), ref), variant
+    G.close()
