@@ -63,9 +63,11 @@ def args_():
     p.add_argument("--nx", type=int, default=NX)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--workload", default="convdiff3d",
-                   choices=["convdiff3d", "kappa_batch"],
+                   choices=["convdiff3d", "kappa_batch", "configs"],
                    help="kappa_batch: the batched workload (64 kappa-diffusion "
-                        "systems, BiCGSTAB(2)), one JSON line of its own")
+                        "systems, BiCGSTAB(2)); configs: the other survey "
+                        "configurations through the bksp.h calls; each prints "
+                        "one JSON line of its own")
     p.add_argument("--batch-count", type=int, default=64)
     p.add_argument("--reference-solve-worker", action="store_true",
                    help=argparse.SUPPRESS)
@@ -717,6 +719,69 @@ def run_batch(a):
     return 0
 
 
+def run_configs(a):
+    """The survey's configurations 1, 3 and 4 through the drop-in bksp.h
+    calls (host arrays: upload, device solve, download), each timed on its
+    second call: CG on the 2D Poisson 64^2 operator in one-triangle storage
+    (tol 1e-10, also timed with the compiled reference); Block CG and Block
+    BiCGSTAB(2) with 16 right-hand sides on 3D Poisson 64^3 and 128^3 (tol
+    1e-8); shifted BiCGSTAB(4) with 32 shifts 10^-3..1 on the 2D
+    convection-diffusion 1024^2 operator (tol 1e-8)."""
+    import scipy.sparse as sp
+    import bksp_b200 as B
+    from bksp_b200 import problems as P
+    res = {}
+
+    def run(name, fn, reps=2):
+        for _ in range(reps):
+            with B.record() as st:
+                t0 = time.perf_counter()
+                r = fn()
+                dt = time.perf_counter() - t0
+        res[name] = {"ret": r, "e2e_s": dt, "solve_s": st["solve_ms"] / 1e3}
+        log(f"{name}: {res[name]}")
+
+    rp, c, v, n = P.poisson2d(64)
+    lrp, lc, lv, _ = P.lower_triangle(rp, c, v, n)
+    b = P.uniform(n, 0)
+    A1 = B.CsrMatrix(lrp, lc, lv, symmetric=True)
+    run("cfg1_cg_poisson64", lambda: B.bksp_dcg(A1, b, 1e-10, 10000, np.zeros(n)))
+    from oracle import ref as R
+    if R.available():
+        Ar = R.Matrix(lrp, lc, lv, n, symmetric=True)
+        t0 = time.perf_counter()
+        r = R.call("bksp_dcg", Ar, b, 1e-10, 10000, np.zeros(n))[0]
+        res["cfg1_cg_poisson64_reference"] = {"ret": int(r), "s": time.perf_counter() - t0}
+    for nx in (64, 128):
+        rp, c, v, n = P.poisson3d(nx)
+        lrp, lc, lv, _ = P.lower_triangle(rp, c, v, n)
+        Bm = np.random.default_rng(2).standard_normal((n, 16))
+        As = B.CsrMatrix(lrp, lc, lv, symmetric=True)
+        Ag = B.CsrMatrix(rp, c, v)
+        run(f"cfg3_blcg_poisson{nx}", lambda: B.dblcg(As, Bm, 1e-8, 5000, np.zeros((n, 16))), 1)
+        X = np.zeros((n, 16))
+        run(f"cfg3_blbicgstabl2_poisson{nx}", lambda: B.dblbicgstabl(Ag, Bm, 2, 1e-8, 5000, X), 1)
+        Af = sp.csr_matrix((v, c, rp), shape=(n, n))
+        res[f"cfg3_blbicgstabl2_poisson{nx}"]["worst_true_residual"] = float(max(
+            np.linalg.norm(Bm[:, k] - Af @ X[:, k]) / np.linalg.norm(Bm[:, k]) for k in range(16)))
+    rp, c, v, n = P.convdiff2d(1024)
+    b = P.uniform(n, 3)
+    sig = P.log_shifts(32)
+    A4 = B.CsrMatrix(rp, c, v)
+    x = np.zeros(33 * n)
+
+    def shifted():
+        x[:] = 0.0
+        return B.dshbicgstabl(A4, b, 4, sig, 1e-8, 5000, x)
+    run("cfg4_shbicgstabl4_convdiff1024_32shifts", shifted, 1)
+    Af = sp.csr_matrix((v, c, rp), shape=(n, n))
+    res["cfg4_shbicgstabl4_convdiff1024_32shifts"]["worst_true_residual"] = float(max(
+        np.linalg.norm(b - (Af @ x[(k + 1) * n:(k + 2) * n] + s_ * x[(k + 1) * n:(k + 2) * n]))
+        / np.linalg.norm(b) for k, s_ in enumerate(sig)))
+    print(json.dumps({"workload": "configs", "unit": "s", "results": res}), flush=True)
+    return 0
+
+
 def main():
     a = args_()
     if a.reference_solve_worker:
@@ -725,6 +790,8 @@ def main():
         return run_reference(a)
     if a.workload == "kappa_batch":
         return run_batch(a)
+    if a.workload == "configs":
+        return run_configs(a)
     return run_ours(a)
 
 
