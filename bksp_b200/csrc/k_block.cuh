@@ -13,7 +13,8 @@
 namespace bk {
 
 constexpr int kBlkS = 16;           // max block width
-constexpr int kBlkTileRows = 16;    // rows per tile of the block kernel
+constexpr int kBlkTileRows = 32;    // rows per tile of the block kernel
+constexpr int kBlkSub = kBlkTileRows / (kThreads / kBlkS);   // rows per thread
 
 // ------------------------------------------------------------------ SpMM
 // Y = alpha * A X  (mode 0), Y = C + alpha * A X  (mode 1), with the
@@ -106,33 +107,47 @@ k_block(BlkArgs a, Red rd) {
   __syncthreads();
   double gacc[2] = {0.0, 0.0};
   double dacc[2] = {0.0, 0.0};
+  // Tiles of kBlkTileRows rows; thread (r, c) handles rows r + 16 k of the
+  // tile (k < kBlkSub), column c: all of a tile's loads are issued before
+  // its first use.
   const long long ntiles = (a.n + kBlkTileRows - 1) / kBlkTileRows;
   for (long long tl = blockIdx.x; tl < ntiles; tl += gridDim.x) {
-    const long long row = tl * kBlkTileRows + r;
-    const bool valid = c < s && row < a.n;
-    for (int i = 0; i < a.nin; ++i)
-      tile[i][r][c] = valid ? a.in[i][row * s + c] : 0.0;
+    const long long row0 = tl * kBlkTileRows;
+#pragma unroll
+    for (int k = 0; k < kBlkSub; ++k) {
+      const int rr = r + (kThreads / kBlkS) * k;
+      const long long row = row0 + rr;
+      const bool valid = c < s && row < a.n;
+      for (int i = 0; i < a.nin; ++i)
+        tile[i][rr][c] = valid ? a.in[i][row * s + c] : 0.0;
+    }
     __syncthreads();
-    for (int o = 0; o < a.nout; ++o) {
-      double y = 0.0;
-      bool first = true;
-      for (int i = 0; i < a.nin; ++i) {
-        const CfH& cf = a.c[o][i];
-        if (!cf.op) continue;
-        double term;
-        if (a.mslot[o][i] >= 0) {
-          double z = 0.0;
-          for (int b = 0; b < s; ++b) z = fma_rn(tile[i][r][b], mat[o][i][b * s + c], z);
-          term = cs[o][i] * z;
-          y = first ? term : add_rn(y, term);
-        } else {
-          y = first ? mul_rn(cs[o][i], tile[i][r][c])
-                    : fma_rn(cs[o][i], tile[i][r][c], y);
+#pragma unroll
+    for (int k = 0; k < kBlkSub; ++k) {
+      const int rr = r + (kThreads / kBlkS) * k;
+      const long long row = row0 + rr;
+      const bool valid = c < s && row < a.n;
+      for (int o = 0; o < a.nout; ++o) {
+        double y = 0.0;
+        bool first = true;
+        for (int i = 0; i < a.nin; ++i) {
+          const CfH& cf = a.c[o][i];
+          if (!cf.op) continue;
+          double term;
+          if (a.mslot[o][i] >= 0) {
+            double z = 0.0;
+            for (int b = 0; b < s; ++b) z = fma_rn(tile[i][rr][b], mat[o][i][b * s + c], z);
+            term = cs[o][i] * z;
+            y = first ? term : add_rn(y, term);
+          } else {
+            y = first ? mul_rn(cs[o][i], tile[i][rr][c])
+                      : fma_rn(cs[o][i], tile[i][rr][c], y);
+          }
+          first = false;
         }
-        first = false;
+        if (valid) a.out[o][row * s + c] = y;
+        tile[4 + o][rr][c] = valid ? y : 0.0;
       }
-      if (valid) a.out[o][row * s + c] = y;
-      tile[4 + o][r][c] = valid ? y : 0.0;
     }
     __syncthreads();
     for (int g = 0; g < a.ng; ++g) {
@@ -142,7 +157,7 @@ k_block(BlkArgs a, Red rd) {
       const int tv = v < a.nin ? v : 4 + (v - a.nin);
       if (r < s && c < s) {
         double z = gacc[g];
-#pragma unroll 4
+#pragma unroll 8
         for (int q = 0; q < kBlkTileRows; ++q) z = fma_rn(tile[tu][q][r], tile[tv][q][c], z);
         gacc[g] = z;
       }
@@ -151,7 +166,11 @@ k_block(BlkArgs a, Red rd) {
       const int u = a.dot[d][0], v = a.dot[d][1];
       const int tu = u < a.nin ? u : 4 + (u - a.nin);
       const int tv = v < a.nin ? v : 4 + (v - a.nin);
-      dacc[d] = fma_rn(tile[tu][r][c], tile[tv][r][c], dacc[d]);
+#pragma unroll
+      for (int k = 0; k < kBlkSub; ++k) {
+        const int rr = r + (kThreads / kBlkS) * k;
+        dacc[d] = fma_rn(tile[tu][rr][c], tile[tv][rr][c], dacc[d]);
+      }
     }
     __syncthreads();
   }

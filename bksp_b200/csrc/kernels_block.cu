@@ -47,7 +47,8 @@ void launch_block(const BlkH& a, const RedH& rd, cudaStream_t st) {
   static_assert(sizeof(BlkArgs) == sizeof(BlkH), "BlkArgs layout");
   memcpy(&b, &a, sizeof(b));
   const long long tiles = (a.n + kBlkTileRows - 1) / kBlkTileRows;
-  int g = (int)(tiles < kMaxBlocks ? tiles : kMaxBlocks);
+  const int cap = resident_grid(reinterpret_cast<const void*>(k_block));   // one wave
+  int g = (int)(tiles < cap ? tiles : cap);
   if (g < 1) g = 1;
   launch_k(k_block, g, kThreads, 0, st, b, rd);
 }
