@@ -122,31 +122,50 @@ k_block(BlkArgs a, Red rd) {
         tile[i][rr][c] = valid ? a.in[i][row * s + c] : 0.0;
     }
     __syncthreads();
+    // Outputs: for each term the s-by-s matrix column c is read once into
+    // registers and serves all kBlkSub rows of this thread; every element's
+    // terms are accumulated in input order, as before.
+    for (int o = 0; o < a.nout; ++o) {
+      double y[kBlkSub];
+      bool first = true;
+      for (int i = 0; i < a.nin; ++i) {
+        const CfH& cf = a.c[o][i];
+        if (!cf.op) continue;
+        if (a.mslot[o][i] >= 0) {
+          double mc[kBlkS];
 #pragma unroll
-    for (int k = 0; k < kBlkSub; ++k) {
-      const int rr = r + (kThreads / kBlkS) * k;
-      const long long row = row0 + rr;
-      const bool valid = c < s && row < a.n;
-      for (int o = 0; o < a.nout; ++o) {
-        double y = 0.0;
-        bool first = true;
-        for (int i = 0; i < a.nin; ++i) {
-          const CfH& cf = a.c[o][i];
-          if (!cf.op) continue;
-          double term;
-          if (a.mslot[o][i] >= 0) {
+          for (int b = 0; b < kBlkS; ++b) mc[b] = b < s ? mat[o][i][b * s + c] : 0.0;
+#pragma unroll
+          for (int k = 0; k < kBlkSub; ++k) {
+            const int rr = r + (kThreads / kBlkS) * k;
             double z = 0.0;
-            for (int b = 0; b < s; ++b) z = fma_rn(tile[i][rr][b], mat[o][i][b * s + c], z);
-            term = cs[o][i] * z;
-            y = first ? term : add_rn(y, term);
-          } else {
-            y = first ? mul_rn(cs[o][i], tile[i][rr][c])
-                      : fma_rn(cs[o][i], tile[i][rr][c], y);
+#pragma unroll
+            for (int b = 0; b < kBlkS; ++b)
+              if (b < s) z = fma_rn(tile[i][rr][b], mc[b], z);
+            const double term = cs[o][i] * z;
+            y[k] = first ? term : add_rn(y[k], term);
           }
-          first = false;
+        } else {
+#pragma unroll
+          for (int k = 0; k < kBlkSub; ++k) {
+            const int rr = r + (kThreads / kBlkS) * k;
+            y[k] = first ? mul_rn(cs[o][i], tile[i][rr][c])
+                         : fma_rn(cs[o][i], tile[i][rr][c], y[k]);
+          }
         }
-        if (valid) a.out[o][row * s + c] = y;
-        tile[4 + o][rr][c] = valid ? y : 0.0;
+        first = false;
+      }
+      if (first) {
+#pragma unroll
+        for (int k = 0; k < kBlkSub; ++k) y[k] = 0.0;
+      }
+#pragma unroll
+      for (int k = 0; k < kBlkSub; ++k) {
+        const int rr = r + (kThreads / kBlkS) * k;
+        const long long row = row0 + rr;
+        const bool valid = c < s && row < a.n;
+        if (valid) a.out[o][row * s + c] = y[k];
+        tile[4 + o][rr][c] = valid ? y[k] : 0.0;
       }
     }
     __syncthreads();
