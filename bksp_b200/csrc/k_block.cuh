@@ -83,7 +83,7 @@ __device__ __forceinline__ void blk_finish(const double* g, int ng, int s,
                                            const double* dd, int nd,
                                            const BlkArgs& a, const Red& rd);
 
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 4)
 k_block(BlkArgs a, Red rd) {
   if (skip(rd)) return;
   __shared__ double tile[6][kBlkTileRows][kBlkS + 1];
