@@ -693,7 +693,7 @@ def run_batch(a):
         "value": res["mixed_learned"]["s"], "unit": "s", "n_gpus": world,
         "steps": a.steps, "warmup": a.warmup,
         "ms_per_step": res["mixed_learned"]["s"] * 1e3, "higher_is_better": False,
-        "scaling": "strong" if world > 1 else "weak", "vs_baseline": None,
+        "scaling": "strong", "vs_baseline": None,
         "dtype": "f32+f64", "data": "synthetic",
         "config": {"workload": f"kappa_batch_{a.batch_count}", "systems": a.batch_count,
                    "rows": ntot_all, "rows_rank0": ntot, "nnz_rank0": nnz, "l": 2,
