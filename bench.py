@@ -20,8 +20,11 @@ Our arm prints one JSON line:
                measured HBM copy bandwidth;
   cpu_baseline the reference (aldente39/bksp compiled from source with gcc +
                OpenBLAS, oracle/_ref) on this host's cores, one full solve.
-With --gpus N > 1 each rank solves its own replica (the method does not
-shard): value is the max over ranks.
+  modes        every GPU mode with its time, iterations, FP64 true residual
+               and relative error against x_true;
+With --gpus N > 1 each rank solves its own replica (one system does not
+shard without a halo exchange per product and an all-reduce per dot):
+value is the max over ranks.
 
 --impl reference times the reference CPU implementation instead: each step
 runs a bounded number of outer iterations; value = measured time per outer
@@ -71,6 +74,7 @@ def args_():
     p.add_argument("--batch-count", type=int, default=64)
     p.add_argument("--reference-solve-worker", action="store_true",
                    help=argparse.SUPPRESS)
+    p.add_argument("--x-out", default=None, help=argparse.SUPPRESS)
     p.add_argument("--profile", default=None,
                    choices=["plain_fp64", "mixed_none", "mixed_learned", "spmv"],
                    help="profiling driver: set up, run one warm solve, then "
@@ -108,16 +112,19 @@ def usable_cores():
     return max(1, n)
 
 
-def reference_full_solve(nx, timeout):
+def reference_full_solve(nx, timeout, x_out=None):
     """One full reference dbicgstabl solve (oracle/_ref) on usable_cores()
-    threads, in a child process bounded by `timeout` seconds.  Returns
+    threads, in a child process bounded by `timeout` seconds; the child
+    writes its solution to `x_out` (.npy) when given.  Returns
     (seconds, ret, cores) or (None, reason, cores)."""
     cores = usable_cores()
     env = dict(os.environ, OPENBLAS_NUM_THREADS=str(cores), OMP_NUM_THREADS=str(cores))
+    cmd = [sys.executable, os.path.abspath(__file__),
+           "--reference-solve-worker", "--nx", str(nx)]
+    if x_out:
+        cmd += ["--x-out", x_out]
     try:
-        out = subprocess.run([sys.executable, os.path.abspath(__file__),
-                              "--reference-solve-worker", "--nx", str(nx)],
-                             env=env, capture_output=True, text=True,
+        out = subprocess.run(cmd, env=env, capture_output=True, text=True,
                              timeout=timeout)
         d = json.loads(out.stdout.strip().splitlines()[-1])
         return d["s"], d["ret"], cores
@@ -127,22 +134,27 @@ def reference_full_solve(nx, timeout):
         return None, f"failed: {e}", cores
 
 
-def reference_solve_worker(nx):
+def reference_solve_worker(nx, x_out=None):
     from oracle import ref as R
-    rp, c, v, n, b = problem(nx)
+    rp, c, v, n, b, _ = problem(nx)
     A = R.Matrix(rp, c, v, n)
     t0 = time.perf_counter()
-    ret, _, _ = R.call("dbicgstabl", A, b, L_DEG, TOL_TRUE, 10000, np.zeros(n))
-    print(json.dumps({"s": time.perf_counter() - t0, "ret": int(ret)}), flush=True)
+    ret, outs, _ = R.call("dbicgstabl", A, b, L_DEG, TOL_TRUE, 10000, np.zeros(n))
+    dt = time.perf_counter() - t0
+    x = outs[-1]
+    if x_out:
+        np.save(x_out, x)
+    print(json.dumps({"s": dt, "ret": int(ret)}), flush=True)
     return 0
 
 
 def problem(nx):
+    """The operator (CSR), b = A x_true and x_true."""
     from bksp_b200 import problems as P
     rp, c, v, n = P.convdiff3d(nx)
     xt = P.uniform(n, 1)
     b = P.csr_matvec(rp, c, v, xt)
-    return rp, c, v, n, b
+    return rp, c, v, n, b, xt
 
 
 def workload_config(nx, n, nnz):
@@ -172,7 +184,7 @@ def run_reference(a):
         return 0
     iters_full = ret_full + 1 if ret_full >= 0 else 10000
     from oracle import ref as R
-    rp, c, v, n, b = problem(a.nx)
+    rp, c, v, n, b, _ = problem(a.nx)
     A = R.Matrix(rp, c, v, n)
     sample = 8
     for _ in range(max(a.warmup - 1, 0)):
@@ -283,13 +295,14 @@ def run_ours(a):
                                 device_id=torch.device("cuda", local))
     import bksp_b200 as B
 
-    rp, c, v, n, b_h = problem(a.nx)
+    rp, c, v, n, b_h, xt_h = problem(a.nx)
     nnz = int(rp[-1])
     Ah = B.CsrMatrix(rp, c, v)
     G = B.GpuMatrix(Ah, B.FP32)
     log(f"operator uploaded (n={n}, nnz={nnz}, variant {G.variant()})")
     dev = torch.device("cuda", local)
     b = torch.from_numpy(b_h).to(dev)
+    xt = torch.from_numpy(xt_h).to(dev)
     x = torch.zeros(n, dtype=torch.float64, device=dev)
     # A dedicated (non-default) stream: the library orders its work on it and
     # the CUDA events below are recorded on it.
@@ -371,9 +384,10 @@ def run_ours(a):
             ms, (ret_m, st_m) = timed(step, a.steps)
         barrier()
         tr = G.true_residual(b.data_ptr(), x.data_ptr(), sp)
+        xe = float(torch.linalg.vector_norm(x - xt) / torch.linalg.vector_norm(xt))
         log(f"mode {name}: {np.mean(ms):.2f} ms, ret {ret_m}")
         modes[name] = {"s": max_over_ranks(float(np.mean(ms))) / 1e3,
-                       "ret": ret_m, "true_residual": tr,
+                       "ret": ret_m, "true_residual": tr, "x_rel_error": xe,
                        "iters": st_m.get("iters", st_m.get("hist_len")),
                        "launches": int(st_m["launches"])}
     mode = "mixed_learned"
@@ -456,6 +470,7 @@ def run_ours(a):
     log(f"e2e: {e2e_s * 1e3:.1f} ms, rets {e2e_rets}")
     e2e_true = float(np.linalg.norm(b_h - P.csr_matvec(rp, c, v, x_p)) /
                      np.linalg.norm(b_h))
+    e2e_xerr = float(np.linalg.norm(x_p - xt_h) / np.linalg.norm(xt_h))
     # CSR operator (FP64 values), b and x0; everything else (structure scan,
     # diagonal form, the learned preconditioner's slot map) is built on the
     # GPU.
@@ -464,7 +479,7 @@ def run_ours(a):
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
-        cpu = cpu_baseline(a.nx)
+        cpu = cpu_baseline(a.nx, x_ours=x_p, x_true=xt_h)
         log(f"cpu baseline: {cpu}")
 
     if rank == 0:
@@ -486,6 +501,7 @@ def run_ours(a):
             "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "ret": r_e2e, "rets": e2e_rets,
                     "iters": st_e.get("hist_len"), "true_residual": e2e_true,
+                    "x_rel_error": e2e_xerr,
                     "call_ms": st_e.get("total_ms"), "solve_ms": st_e.get("solve_ms")},
             "roofline": {"bound": "hbm", "kernel": kname,
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -539,18 +555,28 @@ def profile_run(a, torch, G, b, x, sp, plain_step, mixed_step, B, n, model):
     return 0
 
 
-def cpu_baseline(nx):
+def cpu_baseline(nx, x_ours=None, x_true=None):
     """One full reference solve on this host (oracle/_ref), on every usable
-    core, bounded to a few minutes."""
+    core, bounded to a few minutes.  With `x_ours` (the end-to-end solution)
+    the reference's solution is compared with it and with x_true."""
+    import tempfile
     from oracle import ref as R
     cores = usable_cores()
     if not R.available():
         return {"value": None, "unit": "s", "cores": cores, "kind": "reference",
                 "sample": "oracle/_ref not built"}
-    dt, ret, cores = reference_full_solve(nx, timeout=300)
-    return {"value": dt, "unit": "s", "cores": cores, "kind": "reference",
-            "sample": f"one full dbicgstabl(l={L_DEG}) solve to tol {TOL_TRUE} "
-                      f"(ret {ret}), {cores} threads"}
+    with tempfile.TemporaryDirectory() as td:
+        xf = os.path.join(td, "x_ref.npy") if x_ours is not None else None
+        dt, ret, cores = reference_full_solve(nx, timeout=300, x_out=xf)
+        out = {"value": dt, "unit": "s", "cores": cores, "kind": "reference",
+               "sample": f"one full dbicgstabl(l={L_DEG}) solve to tol {TOL_TRUE} "
+                         f"(ret {ret}), {cores} threads"}
+        if xf and dt is not None and os.path.exists(xf):
+            xr = np.load(xf)
+            out["x_rel_error"] = float(np.linalg.norm(xr - x_true) / np.linalg.norm(x_true))
+            out["e2e_x_rel_diff_vs_reference"] = float(
+                np.linalg.norm(np.asarray(x_ours) - xr) / np.linalg.norm(xr))
+    return out
 
 
 def run_batch(a):
@@ -785,7 +811,7 @@ def run_configs(a):
 def main():
     a = args_()
     if a.reference_solve_worker:
-        return reference_solve_worker(a.nx)
+        return reference_solve_worker(a.nx, a.x_out)
     if a.impl == "reference":
         return run_reference(a)
     if a.workload == "kappa_batch":
