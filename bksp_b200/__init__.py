@@ -52,7 +52,7 @@ class Stats(C.Structure):
                 ("ret", C.c_int), ("solve_ms", C.c_double),
                 ("total_ms", C.c_double), ("true_res", C.c_double),
                 ("launches", C.c_longlong), ("inner_iters", C.c_int),
-                ("sweeps", C.c_int)]
+                ("sweeps", C.c_int), ("alg_bytes", C.c_longlong)]
 
 
 class MixedOpts(C.Structure):
@@ -291,6 +291,8 @@ def record(hist_cap=0):
         out["solve_ms"] = st.solve_ms
         out["total_ms"] = st.total_ms
         out["true_res"] = st.true_res
+        out["launches"] = st.launches
+        out["alg_bytes"] = st.alg_bytes
 
 
 def version():
@@ -366,6 +368,7 @@ class GpuMatrix:
         return ret, {"ret": st.ret, "hist": buf[:min(st.hist_len, hist_cap)].copy(),
                      "iters": st.hist_len, "solve_ms": st.solve_ms,
                      "true_res": st.true_res, "launches": st.launches,
+                     "alg_bytes": st.alg_bytes,
                      "inner_iters": st.inner_iters,
                      "sweeps": st.sweeps // 1000,
                      "replacements": st.sweeps % 1000}
@@ -381,6 +384,7 @@ class GpuMatrix:
         return ret, {"ret": st.ret, "hist": buf[:min(st.hist_len, hist_cap)].copy(),
                      "hist_len": st.hist_len, "solve_ms": st.solve_ms,
                      "true_res": st.true_res, "launches": st.launches,
+                     "alg_bytes": st.alg_bytes,
                      "inner_iters": st.inner_iters, "sweeps": st.sweeps}
 
     SPMV_VARIANTS = {0: "tile", 1: "tma", 2: "vec4", 3: "vec8", 4: "vec16",
@@ -499,7 +503,8 @@ def _batch_args(mats, bs, xs):
 
 def _batch_stats(st):
     return [{"ret": s.ret, "hist_len": s.hist_len, "true_res": s.true_res,
-             "launches": s.launches, "iters": s.hist_len,
+             "launches": s.launches, "alg_bytes": s.alg_bytes,
+             "iters": s.hist_len,
              "inner_iters": s.inner_iters, "sweeps": s.sweeps,
              "solve_ms": s.solve_ms} for s in st]
 

@@ -145,7 +145,7 @@ int bksp_gpu_solve(bksp_gpu_matrix* m, int method, int l, const double* b,
   try {
     cudaStream_t st = pick(stream);
     Timer tm(st);
-    const long long l0 = launch_count();
+    const long long l0 = launch_count(), y0 = byte_count();
     const int n = m->A.n;
     const long long np = pad64(n);
     double* db = dalloc_n<double>(np, st);
@@ -175,6 +175,7 @@ int bksp_gpu_solve(bksp_gpu_matrix* m, int method, int l, const double* b,
     tm.report(o.ret, &ss, o.iters);
     if (stats) {
       stats->launches = launch_count() - l0;
+      stats->alg_bytes = byte_count() - y0;
       stats->true_res = true_residual_dev(m->A, db, dx, st);
     }
     ss.release(st);

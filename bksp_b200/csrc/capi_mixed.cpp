@@ -88,7 +88,7 @@ int bksp_gpu_solve_mixed(bksp_gpu_matrix* m, const double* b, double* x,
   try {
     cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : Ctx::get().st;
     Timer tm(st);
-    const long long l0 = launch_count();
+    const long long l0 = launch_count(), y0 = byte_count();
     const int n = m->A.n;
     const long long np = pad64(n);
     double* db = dalloc_n<double>(np, st);
@@ -122,6 +122,7 @@ int bksp_gpu_solve_mixed(bksp_gpu_matrix* m, const double* b, double* x,
     tm.report(r.ret, &ss, r.iters);
     if (stats) {
       stats->launches = launch_count() - l0;
+      stats->alg_bytes = byte_count() - y0;
       stats->true_res = r.true_res;
       stats->inner_iters = inner;
       stats->sweeps = sweeps * 1000 + reps;   // sweeps*1000 + replacements

@@ -80,6 +80,7 @@ struct CsrH {
   int nrb;
   int variant;   // SpMV kernel variant (kernels.cu: spmv_dispatch)
   DiaH dia;
+  int nnz;       // stored entries (host-side byte accounting only)
 };
 
 // One linear-combination launch: out[o] = sum_i c[o][i] * in[i], terms
@@ -134,6 +135,12 @@ inline thread_local int g_plain_launches = 0;     // the next n launches plain
 // Kernel launches issued by this thread (graph replays are added by the
 // loop runner: captured body kernels x trips).
 long long& launch_count();
+// Algorithmic DRAM bytes of this thread's launches of the single-vector
+// kernels (SpMV, linear combinations, Gram, precision conversions, the
+// preconditioner build): every operand counted once per launch, matrix
+// bytes as its storage format holds them.  Graph replays are added like
+// launch_count; block and shifted-method kernels are not counted.
+long long& byte_count();
 // SpMV: VT = matrix value type, T = vector/accumulation type.
 void launch_spmv_d(const CsrH& A, const SpmvH<double>& io, const RedH& rd,
                    cudaStream_t st);

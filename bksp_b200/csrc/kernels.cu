@@ -23,6 +23,11 @@ long long& launch_count() {
   return n;
 }
 
+long long& byte_count() {
+  thread_local long long n = 0;
+  return n;
+}
+
 // Blocks of `kernel` (kThreads threads, no dynamic shared memory) that are
 // resident on the whole GPU at once, cached per kernel.
 int resident_grid(const void* kernel) {
@@ -62,10 +67,12 @@ __global__ void k_convert_f2d(const float* __restrict__ a, double* __restrict__ 
 }
 void launch_convert_d2f(const double* a, float* b, long long n, cudaStream_t st) {
   ++launch_count();
+  byte_count() += n * 12;
   k_convert_d2f<<<grid_for(n), kThreads, 0, st>>>(a, b, n);
 }
 void launch_convert_f2d(const float* a, double* b, long long n, cudaStream_t st) {
   ++launch_count();
+  byte_count() += n * 12;
   k_convert_f2d<<<grid_for(n), kThreads, 0, st>>>(a, b, n);
 }
 
@@ -178,6 +185,7 @@ void launch_mx_d2f(const double* in, float* o0, float* o1, float* o2,
                    const float* w, int nd, long long n, const RedH& rd,
                    cudaStream_t st) {
   ++launch_count();
+  byte_count() += n * (8 + 4 * ((o1 != nullptr) + (o2 != nullptr) + 1 + (w != nullptr)));
   if (nd)
     launch_k(k_mx_d2f<1>, grid_wave(k_mx_d2f<1>, n), kThreads, 0, st, in, o0, o1, o2, w, n, rd);
   else
@@ -199,6 +207,7 @@ k_mx_accum(double* __restrict__ x, const float* __restrict__ t,
 void launch_mx_accum(double* x, const float* t, float* y, long long n,
                      const RedH& rd, cudaStream_t st) {
   ++launch_count();
+  byte_count() += n * 24;   // x read and written, t read, y written
   launch_k(k_mx_accum, grid_wave(k_mx_accum, n), kThreads, 0, st, x, t, y, n, rd);
 }
 

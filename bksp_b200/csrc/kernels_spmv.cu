@@ -113,6 +113,19 @@ static void spmv_dia_launch(const CsrH& A, const SpmvH<XT>& io, const RedH& rd,
   }
 }
 
+// Algorithmic bytes of one product: the matrix as the chosen format stores
+// it (diagonal form: nd values and a mask byte per row; CSR: values, column
+// indices and row pointers) and each vector operand once.
+template <typename VT, typename XT>
+static long long spmv_bytes(const CsrH& A, const SpmvH<XT>& io, bool dia) {
+  const long long n = A.n;
+  const long long mat = dia ? n * ((long long)A.dia.nd * (long long)sizeof(VT) + 1)
+                            : (long long)A.nnz * (long long)(sizeof(VT) + 4) + 4 * (n + 1);
+  const int vecs = 2 + (io.y2 != nullptr) + (io.mode == 1 && io.b != nullptr) +
+                   (io.w0 != nullptr) + (io.w1 != nullptr);
+  return mat + vecs * n * (long long)sizeof(XT);
+}
+
 template <typename VT, typename XT>
 static void spmv_dispatch(const CsrH& A, const SpmvH<XT>& io, const RedH& rd,
                           cudaStream_t st) {
@@ -120,11 +133,13 @@ static void spmv_dispatch(const CsrH& A, const SpmvH<XT>& io, const RedH& rd,
   if (var < 0) var = A.variant;
   if (var == 7) {
     if (dia_usable(A, io)) {
+      byte_count() += spmv_bytes<VT, XT>(A, io, true);
       spmv_dia_launch<VT, XT>(A, io, rd, st);
       return;
     }
     var = 0;
   }
+  byte_count() += spmv_bytes<VT, XT>(A, io, false);
   switch (var) {
     case 1:
       switch (io.nd) {
@@ -168,14 +183,24 @@ void launch_spmv_f(const CsrH& A, const SpmvH<float>& io, const RedH& rd,
   spmv_dispatch<float, float>(A, io, rd, st);
 }
 
+// CSR values, columns and row pointers read; nd diagonals (and masks) written.
+template <typename T>
+static long long csr2dia_bytes(const CsrH& A, bool mask) {
+  const long long n = A.n;
+  return (long long)A.nnz * (long long)(sizeof(T) + 4) + 4 * (n + 1) +
+         n * (long long)A.dia.nd * (long long)sizeof(T) + (mask ? n : 0);
+}
+
 void launch_csr2dia_d(const CsrH& A, const double* val, double* dval,
                       unsigned char* mask, cudaStream_t st) {
   ++launch_count();
+  byte_count() += csr2dia_bytes<double>(A, mask != nullptr);
   launch_k(k_csr2dia<double>, (A.n + 255) / 256, 256, 0, st, A, val, dval, mask);
 }
 void launch_csr2dia_f(const CsrH& A, const float* val, float* dval,
                       unsigned char* mask, cudaStream_t st) {
   ++launch_count();
+  byte_count() += csr2dia_bytes<float>(A, mask != nullptr);
   launch_k(k_csr2dia<float>, (A.n + 255) / 256, 256, 0, st, A, val, dval, mask);
 }
 

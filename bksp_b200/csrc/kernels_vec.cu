@@ -36,12 +36,23 @@ static void lc_dispatch(const LcH<T>& d, const RedH& rd, cudaStream_t st) {
   else lc_nd<T, 24, 6>(d, rd, st);
 }
 
+// Every input and output once per repetition it is advanced in, else once.
+template <typename T>
+static long long lc_bytes(const LcH<T>& d) {
+  long long vecs = 0;
+  for (int i = 0; i < d.nin; ++i) vecs += (d.in_rep_mask >> i) & 1u ? d.reps : 1;
+  for (int o = 0; o < d.nout; ++o) vecs += (d.out_rep_mask >> o) & 1u ? d.reps : 1;
+  return vecs * d.n * (long long)sizeof(T);
+}
+
 void launch_lincomb_d(const LcH<double>& d, const RedH& rd, cudaStream_t st) {
   ++launch_count();
+  byte_count() += lc_bytes(d);
   lc_dispatch<double>(d, rd, st);
 }
 void launch_lincomb_f(const LcH<float>& d, const RedH& rd, cudaStream_t st) {
   ++launch_count();
+  byte_count() += lc_bytes(d);
   lc_dispatch<float>(d, rd, st);
 }
 
@@ -50,6 +61,7 @@ void launch_lincomb_f(const LcH<float>& d, const RedH& rd, cudaStream_t st) {
 template <typename T>
 static void gram_dispatch(const GramH<T>& g, const RedH& rd, cudaStream_t st) {
   ++launch_count();
+  byte_count() += (long long)g.m * g.n * (long long)sizeof(T);
   const long long q = (g.n / Pack<T>::N + 1) / 2;   // two packets per thread
   switch (g.m) {
 #define BK_GRAM(M)                                                        \

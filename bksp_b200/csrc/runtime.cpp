@@ -404,7 +404,7 @@ void cond_block(SolveState& ss, cudaStream_t st,
   if (!ss.side) BK_CHECK(cudaStreamCreateWithFlags(&ss.side, cudaStreamNonBlocking));
   BK_CHECK(cudaStreamBeginCaptureToGraph(ss.side, cp.conditional.phGraph_out[0], nullptr,
                                          nullptr, 0, cudaStreamCaptureModeThreadLocal));
-  const long long c0 = launch_count();
+  const long long c0 = launch_count(), y0 = byte_count();
   g_plain_scope = true;
   try {
     inner(ss.side);
@@ -418,6 +418,7 @@ void cond_block(SolveState& ss, cudaStream_t st,
   g_plain_scope = false;
   g_plain_launches = 1;   // the kernel after the node follows it plainly
   ss.cond_kernels = launch_count() - c0;
+  ss.cond_bytes = byte_count() - y0;
   cudaGraph_t captured = nullptr;
   BK_CHECK(cudaStreamEndCapture(ss.side, &captured));
   BK_CHECK(cudaStreamUpdateCaptureDependencies(st, &node, 1,
@@ -508,7 +509,8 @@ void spmv(const DevCsr& A, const SpmvH<float>& io, const RedH& rd,
 
 static bool run_graph_while(SolveState& ss,
                             const std::function<void(cudaStream_t)>& body,
-                            cudaStream_t st, long long& body_kernels) {
+                            cudaStream_t st, long long& body_kernels,
+                            long long& body_bytes) {
   cudaGraph_t g = nullptr;
   cudaGraphExec_t ex = nullptr;
   if (cudaGraphCreate(&g, 0) != cudaSuccess) return false;
@@ -532,9 +534,10 @@ static bool run_graph_while(SolveState& ss,
                                       cudaStreamCaptureModeThreadLocal) !=
         cudaSuccess)
       break;
-    const long long c0 = launch_count();
+    const long long c0 = launch_count(), y0 = byte_count();
     ss.has_cond = false;
     ss.cond_kernels = 0;
+    ss.cond_bytes = 0;
     bool body_ok = true;
     try {
       body(st);
@@ -546,6 +549,8 @@ static bool run_graph_while(SolveState& ss,
     g_plain_launches = 0;
     body_kernels = launch_count() - c0;
     launch_count() = c0;   // captured, not launched
+    body_bytes = byte_count() - y0;
+    byte_count() = y0;
     cudaGraph_t captured = nullptr;
     const cudaError_t ce = cudaStreamEndCapture(st, &captured);
     if (ce != cudaSuccess || !body_ok) {
@@ -578,10 +583,11 @@ CtlH run_loop(SolveState& ss, const std::function<void(cudaStream_t)>& body,
               cudaStream_t st) {
   Ctx& cx = Ctx::get();
   if (cx.use_cond_graph) {
-    long long bk_n = 0;
-    if (run_graph_while(ss, body, st, bk_n)) {
+    long long bk_n = 0, bk_bytes = 0;
+    if (run_graph_while(ss, body, st, bk_n, bk_bytes)) {
       CtlH c = ss.read(st);
       launch_count() += bk_n * c.trips;
+      byte_count() += bk_bytes * c.trips;
       return c;
     }
     cx.use_cond_graph = false;   // not supported here: poll from now on

@@ -70,7 +70,7 @@ struct DevCsr {
   CsrH h64() const { return hview(v64, d64); }
   CsrH h32() const { return hview(v32, d32); }
   CsrH hview(const void* v, const void* dv) const {
-    CsrH h{rowptr, col, v, rb, n, nrb, variant, DiaH{}};
+    CsrH h{rowptr, col, v, rb, n, nrb, variant, DiaH{}, nnz};
     if (ndia > 0 && dv) {
       h.dia.val = dv;
       h.dia.mask = dmask;
@@ -129,6 +129,7 @@ struct SolveState {
   bool has_cond = false;
   unsigned long long cond_handle = 0;
   long long cond_kernels = 0;
+  long long cond_bytes = 0;   // their algorithmic bytes (byte_count)
   cudaStream_t side = nullptr;   // capture stream of the conditional body
   void create(int hist_cap, cudaStream_t st);
   void release(cudaStream_t st);

@@ -229,8 +229,11 @@ MixedOut bicgstabl_mixed(const DevCsr& A, const DevCsr* M, const double* b,
   out.replacements = (int)ss.get_scalar(kMxReps, st);
   // The conditional node's kernels ran only in the iterations with a
   // replacement (run_loop counted them in every trip).
-  if (ss.has_cond)
-    launch_count() -= ss.cond_kernels * (long long)std::max(0, c.trips - out.replacements);
+  if (ss.has_cond) {
+    const long long idle = std::max(0, c.trips - out.replacements);
+    launch_count() -= ss.cond_kernels * idle;
+    byte_count() -= ss.cond_bytes * idle;
+  }
   ss.has_cond = false;
   out.true_res = ss.get_scalar(kMxTrue, st);
   dfree(w, st);

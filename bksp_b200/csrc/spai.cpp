@@ -78,6 +78,8 @@ DevCsr spai_apply(bksp_gpu_spai_model* model, bksp_gpu_matrix* m, float* mvals,
   BK_CHECK(cudaMemsetAsync(mvals, 0, sizeof(float) * ((size_t)m->A.nnz + 8), st));
   launch_spai_infer(n, model->w, m->spai.feat, m->spai.dinv, m->spai.slot_entry,
                     mvals, st);
+  // features, slot map and 1/a_ii read per row; M's values written
+  byte_count() += (long long)n * (8LL * kSlots + 4) + 4LL * m->A.nnz;
   BK_CHECK(cudaGetLastError());
   DevCsr v;
   v.n = n;

@@ -31,6 +31,11 @@ typedef struct {
     long long launches;  /* out: GPU kernel launches the call issued        */
     int inner_iters;     /* out: mixed solves: inner iterations, all sweeps */
     int sweeps;          /* out: mixed solves: refinement sweeps            */
+    long long alg_bytes; /* out (bksp_gpu_solve, mixed solves): algorithmic
+                          * DRAM bytes of the solve's kernels (SpMV in the
+                          * stored format, linear combinations, Gram,
+                          * precision conversions, preconditioner build),
+                          * each operand once per launch                   */
 } bksp_gpu_stats;
 
 /* Route statistics of this thread's subsequent bksp calls into *s (NULL

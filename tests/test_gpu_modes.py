@@ -35,7 +35,8 @@ for name, fn in (
     torch.cuda.synchronize()
     ret, st = fn(x)
     torch.cuda.synchronize()
-    out[name] = {"ret": ret, "x": x.cpu().numpy().tolist()}
+    out[name] = {"ret": ret, "x": x.cpu().numpy().tolist(),
+                 "launches": st["launches"], "alg_bytes": st["alg_bytes"]}
 print(json.dumps(out))
 """
 
@@ -55,3 +56,12 @@ def test_loop_modes_agree_bitwise():
         for name in base:
             assert base[name]["ret"] == other[name]["ret"] >= 0, (extra, name)
             assert np.array_equal(np.array(base[name]["x"]), np.array(other[name]["x"])), (extra, name)
+            # Launch and byte accounting: the same graph with and without
+            # programmatic launches counts the same; the host-polled loop
+            # also counts its guarded launches that skip.
+            b0, b1 = base[name]["alg_bytes"], other[name]["alg_bytes"]
+            assert b0 > 0 and base[name]["launches"] > 0, name
+            if "BKSP_GPU_PDL" in extra:
+                assert (b0, base[name]["launches"]) == (b1, other[name]["launches"]), name
+            else:
+                assert b1 >= b0, (name, b0, b1)
