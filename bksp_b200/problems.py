@@ -109,7 +109,7 @@ def gaussian_random_field(L, seed, corr=0.1, var=1.0):
     kz = 2.0 * np.pi * np.fft.rfftfreq(L, d=1.0 / L)
     k2 = k[:, None, None] ** 2 + k[None, :, None] ** 2 + kz[None, None, :] ** 2
     filt = np.exp(-0.25 * corr * corr * k2)   # sqrt of exp(-corr^2 k^2 / 2)
-    g = np.fft.irfftn(np.fft.rfftn(noise) * filt, s=(L, L, L))
+    g = np.fft.irfftn(np.fft.rfftn(noise) * filt, s=(L, L, L), axes=(0, 1, 2))
     g -= g.mean()
     s = g.std()
     return g * (np.sqrt(var) / s if s > 0 else 0.0)
