@@ -148,9 +148,26 @@ def reference_solve_worker(nx, x_out=None):
     return 0
 
 
+def problems_module():
+    """bksp_b200/problems.py loaded by file path: the synthetic-problem
+    generators are plain NumPy, and importing them through the package would
+    load the CUDA library (the package's __init__ does), which the
+    reference arm's process must not map."""
+    import importlib.util
+    name = "_bksp_problems"
+    if name in sys.modules:
+        return sys.modules[name]
+    spec = importlib.util.spec_from_file_location(
+        name, os.path.join(ROOT, "bksp_b200", "problems.py"))
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
 def problem(nx):
     """The operator (CSR), b = A x_true and x_true."""
-    from bksp_b200 import problems as P
+    P = problems_module()
     rp, c, v, n = P.convdiff3d(nx)
     xt = P.uniform(n, 1)
     b = P.csr_matvec(rp, c, v, xt)
@@ -204,8 +221,9 @@ def run_reference(a):
         "data": "synthetic", "config": workload_config(a.nx, n, int(rp[-1])),
         "cpu_baseline": {"value": value, "unit": "s", "cores": cores,
                          "kind": "reference",
-                         "sample": f"{sample} outer iterations per step; "
-                                   f"x {iters_full} iterations of one full "
+                         "sample": f"{sample} outer iterations per step, "
+                                   f"extrapolated: per-iteration time x the "
+                                   f"{iters_full} iterations of one full "
                                    f"solve ({full_s:.1f} s wall, ret {ret_full})"},
         "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
@@ -499,7 +517,8 @@ def run_ours(a):
             "scaling": "weak", "vs_baseline": None,
             "dtype": "f64" if mode == "plain_fp64" else "f32+f64",
             "data": "synthetic",
-            "config": dict(workload_config(a.nx, n, nnz), mode=mode),
+            "config": workload_config(a.nx, n, nnz),
+            "mode": mode,
             "ret": ret, "true_residual": true_res,
             "plain_fp64_s": plain_ms / 1e3,
             "speedup_vs_plain_fp64": plain_ms / step_ms,
@@ -515,7 +534,10 @@ def run_ours(a):
             "roofline": {"bound": "hbm", "kernel": kname,
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
-                         "traffic": traffic, "alg_bytes": alg_bytes,
+                         "traffic": traffic,
+                         "traffic_source": "profiles/traffic.json (ncu DRAM "
+                                           "bytes of one launch, committed)",
+                         "alg_bytes": alg_bytes,
                          "csr_alg_bytes": csr_bytes,
                          "launch_ms": launch_ms,
                          "variant": vname, "diagonals": ndia,

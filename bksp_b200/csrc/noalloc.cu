@@ -16,11 +16,15 @@
 // and it keeps the last call's contents, so the arrival ticket and the
 // control block are cleared at the start of each call; two calls whose
 // work overlaps on the GPU (different streams, or different host threads)
-// race on it and must be serialised by the caller.
+// race on it and must be serialised by the caller.  The device address of
+// the array is looked up once per device and cached; a cudaDeviceReset
+// invalidates it, so a process that resets a device must not call this
+// entry point on that device again.
 #include <cuda_runtime.h>
 
 #include <cmath>
 #include <cstdio>
+#include <exception>
 #include <mutex>
 
 #include "capi_internal.h"
@@ -85,7 +89,30 @@ extern "C" int bksp_gpu_true_residual_noalloc(bksp_gpu_matrix* m,
                  "(use bksp_gpu_true_residual)\n", n, kNoAllocMaxRows);
     return INVALID_PARAMETERS;
   }
-  cudaStream_t st = stream ? static_cast<cudaStream_t>(stream) : Ctx::get().st;
+  // The scratch is picked by the current device, so the operator must live
+  // on that device: a kernel on one GPU reading another GPU's operator
+  // through this GPU's scratch would fault or silently cross the link.
+  int cur = -1;
+  if (cudaGetDevice(&cur) != cudaSuccess || cur != m->device) {
+    cudaGetLastError();
+    std::fprintf(stderr,
+                 "bksp_gpu_true_residual_noalloc: the operator lives on device "
+                 "%d but device %d is current\n", m->device, cur);
+    return INVALID_PARAMETERS;
+  }
+  cudaStream_t st = nullptr;
+  if (stream) {
+    st = static_cast<cudaStream_t>(stream);
+  } else {
+    // The calling thread's library stream; its first use on a thread
+    // creates it, which can fail (and throws inside the library).
+    try {
+      st = Ctx::get().st;
+    } catch (const std::exception&) {
+      cudaGetLastError();
+      return INVALID_PARAMETERS;
+    }
+  }
   double* base = scratch_for_current_device();
   if (!base) return INVALID_PARAMETERS;
   double* r = base;

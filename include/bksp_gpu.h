@@ -233,9 +233,10 @@ int bksp_gpu_solve_batch(bksp_gpu_matrix *const *A, int method, int l,
  * stderr.  The first call on each device looks up that array's device
  * address (make it before any stream capture).  All calls on a device share
  * the array: calls whose GPU work overlaps race and must be serialised by
- * the caller.  b, x: device pointers to n doubles; *res receives the
- * residual; returns 0 or INVALID_PARAMETERS; synchronous on `stream` (NULL:
- * library stream).
+ * the caller.  The operator's device must be the current device (else
+ * INVALID_PARAMETERS).  b, x: device pointers to n doubles; *res receives
+ * the residual; returns 0 or INVALID_PARAMETERS; synchronous on `stream`
+ * (NULL: library stream).
  */
 int bksp_gpu_true_residual_noalloc(bksp_gpu_matrix *A, const double *b,
                                    const double *x, void *stream,

@@ -30,7 +30,19 @@ from oracle import ref as R          # noqa: E402
 from oracle import solvers as S      # noqa: E402
 from bksp_b200 import problems as P  # noqa: E402
 
-REF_TESTMAT = "/root/reference/testmat"
+def reference_dir():
+    """The reference's source tree: BKSP_REFERENCE, else the location
+    oracle/Makefile builds from."""
+    d = os.environ.get("BKSP_REFERENCE")
+    if not d:
+        import subprocess
+        d = subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"),
+                            "print-ref"], capture_output=True, text=True,
+                           check=True).stdout.strip()
+    return d
+
+
+REF_TESTMAT = os.path.join(reference_dir(), "testmat")
 
 
 def dlarnv_block(n, s):

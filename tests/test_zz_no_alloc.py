@@ -56,6 +56,44 @@ def test_noalloc_residual_matches_allocating_entry_point(gpu):
     A2.close()
 
 
+def test_noalloc_on_caller_stream_and_second_thread(gpu):
+    """A caller-supplied stream, and a call from a thread whose library
+    stream is created by that call, give the allocating entry point's
+    value."""
+    import threading
+
+    import torch
+    B = gpu
+    rp, c, v, n = P.convdiff3d(24)
+    A = B.GpuMatrix(B.CsrMatrix(rp, c, v))
+    rng = np.random.default_rng(12)
+    b = torch.from_numpy(rng.uniform(-1, 1, n)).cuda()
+    x = torch.from_numpy(rng.uniform(-1, 1, n)).cuda()
+    torch.cuda.synchronize()
+    ref = A.true_residual(b.data_ptr(), x.data_ptr())
+    f = _noalloc(B)
+    s = torch.cuda.Stream()
+    for _ in range(2):
+        out = C.c_double(-1.0)
+        assert f(A.h, b.data_ptr(), x.data_ptr(), C.c_void_p(s.cuda_stream),
+                 C.byref(out)) == 0
+        assert abs(out.value - ref) <= 1e-12 * ref, (out.value, ref)
+    got = {}
+
+    def worker():
+        torch.cuda.set_device(0)
+        o = C.c_double(-1.0)
+        got["rc"] = f(A.h, b.data_ptr(), x.data_ptr(), None, C.byref(o))
+        got["res"] = o.value
+
+    t = threading.Thread(target=worker)
+    t.start()
+    t.join()
+    assert got["rc"] == 0
+    assert abs(got["res"] - ref) <= 1e-12 * ref, (got, ref)
+    A.close()
+
+
 def test_noalloc_rejects_operators_beyond_its_limit(gpu):
     import torch
     B = gpu
