@@ -617,10 +617,11 @@ def run_batch(a):
     f ~ N(0,1); time to an FP64 true relative residual of 1e-8 on every
     system.  value: mixed-precision BiCGSTAB(2) with the learned SPAI
     preconditioner (trained beforehand on 64 smaller systems of the same
-    family, seeds 1000+i), all systems in one batched call; plain_fp64_s:
+    family, seeds 1000+i), all systems in one persistent launch; plain_fp64_s:
     FP64 BiCGSTAB(2) on the Jacobi right-scaled systems A D^-1 y = b, x = D^-1 y,
-    batched the same way; sequential_s: the learned solve one system at a
-    time."""
+    batched the same way; the modes also time both with one CUDA-graph loop
+    per system on eight host threads (*_graphs) and the learned solve one
+    system at a time (mixed_learned_sequential)."""
     import torch
     import torch.distributed as dist
     import bksp_b200 as B
@@ -697,9 +698,10 @@ def run_batch(a):
                                            target=TOL_TRUE, precond=B.PRECOND_LEARNED,
                                            model=model, workers=workers)
 
-    def plain():
-        return B.solve_batch(scaled, B.BICGSTABL_FAST, [b.data_ptr() for b in bs],
-                             [x.data_ptr() for x in xs], TOL_TRUE, 20000, l=2)
+    def plain(workers=0):
+        return lambda: B.solve_batch(scaled, B.BICGSTABL_FAST, [b.data_ptr() for b in bs],
+                                     [x.data_ptr() for x in xs], TOL_TRUE, 20000, l=2,
+                                     workers=workers)
 
     def worst_true_res(scale):
         w = 0.0
@@ -710,8 +712,13 @@ def run_batch(a):
         return w
 
     res = {}
-    for name, fn, k, scale in (("plain_fp64", plain, a.steps, True),
+    # workers=0: every system in one persistent launch (the default);
+    # workers=8: eight host threads, one CUDA-graph loop per system;
+    # workers=1: one system after the other.
+    for name, fn, k, scale in (("plain_fp64", plain(), a.steps, True),
+                               ("plain_fp64_graphs", plain(8), a.steps, True),
                                ("mixed_learned_sequential", learned(1), 1, False),
+                               ("mixed_learned_graphs", learned(8), a.steps, False),
                                ("mixed_learned", learned(), a.steps, False)):
         for _ in range(a.warmup if k > 1 else 0):
             for x in xs:

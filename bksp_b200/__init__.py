@@ -116,6 +116,12 @@ def _load():
     L.bksp_gpu_solve_batch.argtypes = [C.POINTER(vp), i, i, C.POINTER(vp),
                                        C.POINTER(vp), i, d, i, i,
                                        C.POINTER(Stats)]
+    L.bksp_gpu_persist_status.argtypes = [C.POINTER(C.c_int)]
+    L.bksp_gpu_persist_status.restype = i
+    L.bksp_gpu_persist_debug.argtypes = [C.c_longlong, i]
+    L.bksp_gpu_persist_debug.restype = None
+    L.bksp_gpu_loop_mode.argtypes = [i]
+    L.bksp_gpu_loop_mode.restype = i
     L.bksp_gpu_spai_create.argtypes = [C.c_uint, C.POINTER(vp)]
     L.bksp_gpu_spai_destroy.argtypes = [vp]
     L.bksp_gpu_spai_params.argtypes = [vp, C.POINTER(C.c_float), i]
@@ -514,7 +520,9 @@ def solve_mixed_batch(mats, bs, xs, l=4, target=1e-8, max_iter=10000,
                       workers=0):
     """bksp_gpu_solve_mixed_batch: mixed-precision BiCGSTAB(l) on every
     (GpuMatrix, b, x) of the lists (device pointers, ready before the call,
-    x in/out), several systems at once; returns (ret, per-system stats)."""
+    x in/out); workers=0: all systems in one persistent launch, workers>0:
+    that many host threads, one graph loop per system.  Returns (ret,
+    per-system stats)."""
     n, A, B, X, st = _batch_args(mats, bs, xs)
     o = MixedOpts(l, target, max_iter, precond,
                   model.h if model is not None else None, delta, period,
@@ -530,3 +538,27 @@ def solve_batch(mats, method, bs, xs, tol, max_iter, l=4, workers=0):
     ret = lib.bksp_gpu_solve_batch(A, int(method), int(l), B, X, n, float(tol),
                                    int(max_iter), int(workers), st)
     return ret, _batch_stats(st)
+
+
+def persist_status():
+    """(status, grid) of this thread's last persistent batch: status 0 ok,
+    1 a grid-barrier wait ran out, 2 launch failure."""
+    g = C.c_int(0)
+    st = lib.bksp_gpu_persist_status(C.byref(g))
+    return st, g.value
+
+
+def persist_debug(spin_limit=0, absent_cta=-1):
+    """Test hook of the persistent batch's bounded barrier waits."""
+    lib.bksp_gpu_persist_debug(int(spin_limit), int(absent_cta))
+
+
+@contextlib.contextmanager
+def loop_mode(mode):
+    """Run this thread's single-system solves with iteration loop `mode`
+    (0 CUDA-graph loop, 1 persistent launch) inside the block."""
+    prev = lib.bksp_gpu_loop_mode(int(mode))
+    try:
+        yield
+    finally:
+        lib.bksp_gpu_loop_mode(prev)

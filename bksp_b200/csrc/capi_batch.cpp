@@ -1,15 +1,20 @@
 // Batched solves (bksp_gpu.h): many independent systems in one call.
 //
-// Host worker threads take systems from a shared counter and run the
-// ordinary device solve on each, on the worker's own CUDA stream (the
-// library's per-thread stream).  Every system is therefore one CUDA graph
-// with its own device-side while loop and convergence flag -- a converged
-// system stops, the others keep iterating -- and the GPU runs the graphs
-// of different workers concurrently, so small systems share the SMs
-// instead of queueing behind each other.  Graph capture and instantiation,
-// the host part of a solve, also proceed in parallel.  Results are
-// deterministic: each system's arithmetic does not depend on what runs
-// beside it.
+// Default (workers = 0): one persistent launch.  Every system's solve runs
+// on a host thread of its own up to its iteration loop (operator-dependent
+// set-up such as the learned preconditioner's values, the initial
+// residual), records one iteration of its method and joins a
+// PersistGroup; the group's last member launches one cooperative kernel
+// that iterates all systems in lockstep with per-system convergence masks
+// (kernels_persist.cu).  A system whose iteration has no persistent form,
+// and a learned solve's Jacobi retry, run as a graph loop instead.
+//
+// workers > 0: that many host worker threads take systems from a shared
+// counter and run the ordinary device solve on each, on the worker's own
+// CUDA stream -- one CUDA graph with its own device-side while loop per
+// system, graphs of different workers running concurrently.
+//
+// Either way each system's result does not depend on what runs beside it.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -33,7 +38,6 @@ template <typename F>
 void run_workers(int count, int workers, const F& solve_one, std::vector<int>& rets) {
   int dev = 0;
   cudaGetDevice(&dev);
-  if (workers <= 0) workers = 8;
   workers = std::max(1, std::min(workers, count));
   std::atomic<int> next{0};
   auto work = [&]() {
@@ -54,6 +58,52 @@ void run_workers(int count, int workers, const F& solve_one, std::vector<int>& r
   }
   work();
   for (auto& t : pool) t.join();
+}
+
+// Test hooks and status of this thread's persistent batches.
+thread_local long long g_spin_limit = 0;
+thread_local int g_absent_cta = -1;
+thread_local int g_last_status = 0;
+thread_local int g_last_grid = 0;
+
+// One host thread per system, each joined to one persistent group; a
+// system whose thread cannot be created withdraws from the group and is
+// solved by the calling thread afterwards, outside the group.
+template <typename F>
+void run_persistent(int count, const F& solve_one, std::vector<int>& rets) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  PersistGroup grp(count);
+  grp.spin_limit = g_spin_limit;
+  grp.absent_cta = g_absent_cta;
+  auto member = [&](int i) {
+    cudaSetDevice(dev);
+    persist_group() = &grp;
+    rets[i] = solve_one(i);
+    if (persist_group() == &grp) {   // ended before its iteration loop
+      persist_group() = nullptr;
+      try {
+        grp.withdraw(Ctx::get().st);
+      } catch (const std::exception&) {
+        grp.withdraw(nullptr);
+      }
+    }
+  };
+  std::vector<std::thread> pool;
+  std::vector<int> later;
+  for (int i = 1; i < count; ++i) {
+    try {
+      pool.emplace_back(member, i);
+    } catch (const std::system_error&) {
+      later.push_back(i);
+      grp.withdraw(Ctx::get().st);
+    }
+  }
+  member(0);
+  for (auto& t : pool) t.join();
+  for (int i : later) rets[i] = solve_one(i);
+  g_last_status = grp.status;
+  g_last_grid = grp.grid;
 }
 
 int summarise(const std::vector<int>& rets) {
@@ -78,10 +128,14 @@ int bksp_gpu_solve_mixed_batch(bksp_gpu_matrix* const* A, const double* const* b
     if (!A[i] || !b[i] || !x[i]) return INVALID_PARAMETERS;
   if (count == 0) return 0;
   std::vector<int> rets(count, INVALID_PARAMETERS);
-  run_workers(count, workers, [&](int i) {
+  auto one = [&](int i) {
     return bksp_gpu_solve_mixed(A[i], b[i], x[i], opts, nullptr,
                                 stats ? &stats[i] : nullptr);
-  }, rets);
+  };
+  if (workers > 0)
+    run_workers(count, workers, one, rets);
+  else
+    run_persistent(count, one, rets);
   return summarise(rets);
 }
 
@@ -94,11 +148,37 @@ int bksp_gpu_solve_batch(bksp_gpu_matrix* const* A, int method, int l,
     if (!A[i] || !b[i] || !x[i]) return INVALID_PARAMETERS;
   if (count == 0) return 0;
   std::vector<int> rets(count, INVALID_PARAMETERS);
-  run_workers(count, workers, [&](int i) {
+  auto one = [&](int i) {
     return bksp_gpu_solve(A[i], method, l, b[i], x[i], tol, max_iter, nullptr,
                           stats ? &stats[i] : nullptr);
-  }, rets);
+  };
+  if (workers > 0)
+    run_workers(count, workers, one, rets);
+  else
+    run_persistent(count, one, rets);
   return summarise(rets);
+}
+
+void bksp_gpu_persist_debug(long long spin_limit, int absent_cta) {
+  g_spin_limit = spin_limit > 0 ? spin_limit : 0;
+  g_absent_cta = absent_cta;
+}
+
+int bksp_gpu_loop_mode(int mode) {
+  try {
+    Ctx& cx = Ctx::get();
+    const int prev = cx.persistent ? 1 : 0;
+    if (mode == 0 || mode == 1) cx.persistent = mode == 1;
+    return prev;
+  } catch (const std::exception&) {
+    cudaGetLastError();
+    return INVALID_PARAMETERS;
+  }
+}
+
+int bksp_gpu_persist_status(int* grid) {
+  if (grid) *grid = g_last_grid;
+  return g_last_status;
 }
 
 }  // extern "C"

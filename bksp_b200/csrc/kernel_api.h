@@ -238,6 +238,90 @@ void launch_spmm(const CsrH& A, const SpmmH& a, const RedH& rd, cudaStream_t st)
 void launch_block(const BlkH& a, const RedH& rd, cudaStream_t st);
 void launch_cm2rm(const double* cm, double* rm, int n, int s, cudaStream_t st);
 void launch_rm2cm(const double* rm, double* cm, int n, int s, cudaStream_t st);
+// ---- persistent loop (kernels_persist.cu) ----
+// One iteration's launches recorded as operations (run_loop in persistent
+// mode) and executed for a whole batch of systems by one cooperative
+// kernel: phase k runs operation k of every system that is still
+// iterating, its work split into units of kPersistUnit rows/elements over
+// the whole grid; a grid barrier separates phases.  Reductions are per
+// system: each CTA that worked on a system publishes one partial per dot,
+// the last of them sums the partials in CTA-slot order and runs the
+// system's scalar epilogue.
+constexpr int kPersistUnit = 1024;
+constexpr int kPersistMaxSys = 512;
+enum : int {
+  kOpNone = 0,
+  kOpSpmvDiaD, kOpSpmvDiaF,   // diagonal-form SpMV (k_spmv_dia's row order)
+  kOpSpmvCsrD, kOpSpmvCsrF,   // CSR SpMV, one thread per row (same order)
+  kOpLcD, kOpLcF,             // linear combination (k_lincomb)
+  kOpGramD, kOpGramF,         // pairwise Gram products, m <= kPersistGramMax
+  kOpMxD2f, kOpMxAccum,       // mixed-precision steps
+  kOpEpi,                     // scalar epilogue only
+};
+constexpr int kPersistGramMax = 5;
+struct MxD2fH {
+  const double* in;
+  float* o0;
+  float* o1;
+  float* o2;
+  const float* w;
+  long long n;
+  int nd;
+};
+struct MxAccH {
+  double* x;
+  const float* t;
+  float* y;
+  long long n;
+};
+struct alignas(16) ProgOpH {
+  int kind;
+  int units;   // work units of kPersistUnit
+  RedH rd;
+  union U {
+    struct { CsrH A; SpmvH<double> io; } sd;
+    struct { CsrH A; SpmvH<float> io; } sf;
+    LcH<double> ld;
+    LcH<float> lf;
+    GramH<double> gd;
+    GramH<float> gf;
+    MxD2fH d2f;
+    MxAccH acc;
+  } u;
+};
+// Grid-barrier state of one persistent launch (zeroed before the launch).
+struct PBarH {
+  unsigned count;
+  unsigned gen;
+  int err;        // 1: a barrier wait ran out of polls
+  int err_phase;  // the phase at which it did
+};
+struct PersistH {
+  const ProgOpH* ops;   // [nsys][max_ops]
+  const int* nops;      // operations per system
+  CtlH* const* ctl;     // each system's control block
+  int nsys, max_ops;
+  PBarH* bar;
+  long long spin_limit;   // polls per barrier wait before giving up
+  int absent_cta;         // test hook: this CTA never arrives (-1: none)
+};
+// Recording target of this thread's launch wrappers (null: launch).  The
+// wrappers append an operation instead of launching; a wrapper without a
+// persistent form throws CudaError.
+inline thread_local void* g_prog_rec = nullptr;
+void prog_push(const ProgOpH& op);           // runtime.cpp
+[[noreturn]] void prog_unsupported(const char* what);
+// Units of kPersistUnit covering n rows / elements (at least one).
+inline int prog_units(long long n) {
+  const long long u = (n + kPersistUnit - 1) / kPersistUnit;
+  return u < 1 ? 1 : (int)u;
+}
+// Largest grid the persistent kernel may be launched with on the current
+// device (all CTAs resident at once).
+int persist_max_grid();
+// Cooperative launch of the persistent kernel (grid CTAs of kThreads).
+cudaError_t launch_persist(const PersistH& p, int grid, cudaStream_t st);
+
 // Solve start: reset control + ticket, optionally preset S[slot] (slot < 0:
 // none).  Scalar preset without host synchronisation.
 void launch_ctl_init(CtlH* c, unsigned* ticket, double* S, int iter0,

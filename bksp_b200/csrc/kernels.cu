@@ -66,11 +66,13 @@ __global__ void k_convert_f2d(const float* __restrict__ a, double* __restrict__ 
     b[i] = (double)a[i];
 }
 void launch_convert_d2f(const double* a, float* b, long long n, cudaStream_t st) {
+  if (g_prog_rec) prog_unsupported("precision conversion");
   ++launch_count();
   byte_count() += n * 12;
   k_convert_d2f<<<grid_for(n), kThreads, 0, st>>>(a, b, n);
 }
 void launch_convert_f2d(const float* a, double* b, long long n, cudaStream_t st) {
+  if (g_prog_rec) prog_unsupported("precision conversion");
   ++launch_count();
   byte_count() += n * 12;
   k_convert_f2d<<<grid_for(n), kThreads, 0, st>>>(a, b, n);
@@ -184,8 +186,18 @@ k_mx_d2f(const double* __restrict__ in, float* o0, float* o1, float* o2,
 void launch_mx_d2f(const double* in, float* o0, float* o1, float* o2,
                    const float* w, int nd, long long n, const RedH& rd,
                    cudaStream_t st) {
-  ++launch_count();
   byte_count() += n * (8 + 4 * ((o1 != nullptr) + (o2 != nullptr) + 1 + (w != nullptr)));
+  if (g_prog_rec) {
+    ProgOpH op;
+    std::memset(&op, 0, sizeof(op));
+    op.kind = kOpMxD2f;
+    op.u.d2f = MxD2fH{in, o0, o1, o2, w, n, nd ? 1 : 0};
+    op.units = prog_units(n);
+    op.rd = rd;
+    prog_push(op);
+    return;
+  }
+  ++launch_count();
   if (nd)
     launch_k(k_mx_d2f<1>, grid_wave(k_mx_d2f<1>, n), kThreads, 0, st, in, o0, o1, o2, w, n, rd);
   else
@@ -206,8 +218,18 @@ k_mx_accum(double* __restrict__ x, const float* __restrict__ t,
 
 void launch_mx_accum(double* x, const float* t, float* y, long long n,
                      const RedH& rd, cudaStream_t st) {
-  ++launch_count();
   byte_count() += n * 24;   // x read and written, t read, y written
+  if (g_prog_rec) {
+    ProgOpH op;
+    std::memset(&op, 0, sizeof(op));
+    op.kind = kOpMxAccum;
+    op.u.acc = MxAccH{x, t, y, n};
+    op.units = prog_units(n);
+    op.rd = rd;
+    prog_push(op);
+    return;
+  }
+  ++launch_count();
   launch_k(k_mx_accum, grid_wave(k_mx_accum, n), kThreads, 0, st, x, t, y, n, rd);
 }
 
@@ -248,6 +270,7 @@ __global__ void k_set_scalar(double* S, short slot, double v) {
 }
 
 void launch_set_scalar(double* S, short slot, double v, cudaStream_t st) {
+  if (g_prog_rec) prog_unsupported("scalar preset");
   ++launch_count();
   launch_k(k_set_scalar, 1, 1, 0, st, S, slot, v);
 }
@@ -258,6 +281,15 @@ __global__ void k_epilogue(Red rd) {
 }
 
 void launch_epilogue(const RedH& rd, cudaStream_t st) {
+  if (g_prog_rec) {
+    ProgOpH op;
+    std::memset(&op, 0, sizeof(op));
+    op.kind = kOpEpi;
+    op.units = 1;
+    op.rd = rd;
+    prog_push(op);
+    return;
+  }
   ++launch_count();
   launch_k(k_epilogue, 1, 1, 0, st, rd);
 }
@@ -281,6 +313,7 @@ __global__ void k_loop_control(Ctl* c, cudaGraphConditionalHandle h,
 
 void launch_loop_control(CtlH* ctl, unsigned long long handle, int use_handle,
                          cudaStream_t st) {
+  if (g_prog_rec) prog_unsupported("loop control");
   ++launch_count();
   launch_k(k_loop_control, 1, 1, 0, st, ctl, (cudaGraphConditionalHandle)handle,
                                   use_handle);

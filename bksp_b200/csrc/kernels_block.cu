@@ -18,6 +18,7 @@ namespace bk {
 // ------------------------------------------------------- shifted methods
 
 void launch_shift(const ShiftArgsH& a, const RedH& rd, cudaStream_t st) {
+  if (g_prog_rec) prog_unsupported("block / shifted kernel");
   ++launch_count();
   ShiftArgs s{a.r, a.p, a.x, a.xs, a.ps, a.np, a.ns, a.l, a.j, a.mode};
   switch (a.mode) {
@@ -31,6 +32,7 @@ void launch_shift(const ShiftArgsH& a, const RedH& rd, cudaStream_t st) {
 // --------------------------------------------------------- block methods
 
 void launch_spmm(const CsrH& A, const SpmmH& a, const RedH& rd, cudaStream_t st) {
+  if (g_prog_rec) prog_unsupported("block / shifted kernel");
   ++launch_count();
   SpmmArgs s{a.X, a.Y, a.C, a.W, a.alpha, a.mode, a.s, a.nd};
   const int g = grid_for((long long)A.n * kBlkS);
@@ -42,6 +44,7 @@ void launch_spmm(const CsrH& A, const SpmmH& a, const RedH& rd, cudaStream_t st)
 }
 
 void launch_block(const BlkH& a, const RedH& rd, cudaStream_t st) {
+  if (g_prog_rec) prog_unsupported("block / shifted kernel");
   ++launch_count();
   BlkArgs b;
   static_assert(sizeof(BlkArgs) == sizeof(BlkH), "BlkArgs layout");

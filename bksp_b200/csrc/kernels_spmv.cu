@@ -126,11 +126,39 @@ static long long spmv_bytes(const CsrH& A, const SpmvH<XT>& io, bool dia) {
   return mat + vecs * n * (long long)sizeof(XT);
 }
 
+// Persistent-loop form of one product: the diagonal form where the
+// stand-alone launch would use it, else the one-thread-per-row CSR unit.
+template <typename VT, typename XT>
+static void spmv_record(const CsrH& A, const SpmvH<XT>& io, const RedH& rd,
+                        int var) {
+  if (io.nd > 3) prog_unsupported("spmv with more than three dots");
+  ProgOpH op;
+  std::memset(&op, 0, sizeof(op));
+  const bool dia = var == 7 && dia_usable(A, io);
+  byte_count() += spmv_bytes<VT, XT>(A, io, dia);
+  if constexpr (sizeof(XT) == 8) {
+    op.kind = dia ? kOpSpmvDiaD : kOpSpmvCsrD;
+    op.u.sd.A = A;
+    op.u.sd.io = io;
+  } else {
+    op.kind = dia ? kOpSpmvDiaF : kOpSpmvCsrF;
+    op.u.sf.A = A;
+    op.u.sf.io = io;
+  }
+  op.units = prog_units(A.n);
+  op.rd = rd;
+  prog_push(op);
+}
+
 template <typename VT, typename XT>
 static void spmv_dispatch(const CsrH& A, const SpmvH<XT>& io, const RedH& rd,
                           cudaStream_t st) {
   int var = spmv_override();
   if (var < 0) var = A.variant;
+  if (g_prog_rec) {
+    spmv_record<VT, XT>(A, io, rd, var);
+    return;
+  }
   if (var == 7) {
     if (dia_usable(A, io)) {
       byte_count() += spmv_bytes<VT, XT>(A, io, true);
@@ -174,12 +202,12 @@ static void spmv_dispatch(const CsrH& A, const SpmvH<XT>& io, const RedH& rd,
 
 void launch_spmv_d(const CsrH& A, const SpmvH<double>& io, const RedH& rd,
                    cudaStream_t st) {
-  ++launch_count();
+  if (!g_prog_rec) ++launch_count();
   spmv_dispatch<double, double>(A, io, rd, st);
 }
 void launch_spmv_f(const CsrH& A, const SpmvH<float>& io, const RedH& rd,
                    cudaStream_t st) {
-  ++launch_count();
+  if (!g_prog_rec) ++launch_count();
   spmv_dispatch<float, float>(A, io, rd, st);
 }
 
@@ -193,12 +221,14 @@ static long long csr2dia_bytes(const CsrH& A, bool mask) {
 
 void launch_csr2dia_d(const CsrH& A, const double* val, double* dval,
                       unsigned char* mask, cudaStream_t st) {
+  if (g_prog_rec) prog_unsupported("csr2dia");
   ++launch_count();
   byte_count() += csr2dia_bytes<double>(A, mask != nullptr);
   launch_k(k_csr2dia<double>, (A.n + 255) / 256, 256, 0, st, A, val, dval, mask);
 }
 void launch_csr2dia_f(const CsrH& A, const float* val, float* dval,
                       unsigned char* mask, cudaStream_t st) {
+  if (g_prog_rec) prog_unsupported("csr2dia");
   ++launch_count();
   byte_count() += csr2dia_bytes<float>(A, mask != nullptr);
   launch_k(k_csr2dia<float>, (A.n + 255) / 256, 256, 0, st, A, val, dval, mask);

@@ -45,14 +45,34 @@ static long long lc_bytes(const LcH<T>& d) {
   return vecs * d.n * (long long)sizeof(T);
 }
 
+// Persistent-loop form: units run over (repetition, chunk).
+template <typename T>
+static void lc_record(const LcH<T>& d, const RedH& rd) {
+  if (d.nd > 3) prog_unsupported("linear combination with more than three dots");
+  ProgOpH op;
+  std::memset(&op, 0, sizeof(op));
+  if constexpr (sizeof(T) == 8) {
+    op.kind = kOpLcD;
+    op.u.ld = d;
+  } else {
+    op.kind = kOpLcF;
+    op.u.lf = d;
+  }
+  op.units = prog_units(d.n) * (d.reps > 0 ? d.reps : 1);
+  op.rd = rd;
+  prog_push(op);
+}
+
 void launch_lincomb_d(const LcH<double>& d, const RedH& rd, cudaStream_t st) {
-  ++launch_count();
   byte_count() += lc_bytes(d);
+  if (g_prog_rec) return lc_record<double>(d, rd);
+  ++launch_count();
   lc_dispatch<double>(d, rd, st);
 }
 void launch_lincomb_f(const LcH<float>& d, const RedH& rd, cudaStream_t st) {
-  ++launch_count();
   byte_count() += lc_bytes(d);
+  if (g_prog_rec) return lc_record<float>(d, rd);
+  ++launch_count();
   lc_dispatch<float>(d, rd, st);
 }
 
@@ -60,8 +80,24 @@ void launch_lincomb_f(const LcH<float>& d, const RedH& rd, cudaStream_t st) {
 
 template <typename T>
 static void gram_dispatch(const GramH<T>& g, const RedH& rd, cudaStream_t st) {
-  ++launch_count();
   byte_count() += (long long)g.m * g.n * (long long)sizeof(T);
+  if (g_prog_rec) {
+    if (g.m > kPersistGramMax) prog_unsupported("Gram of more than five vectors");
+    ProgOpH op;
+    std::memset(&op, 0, sizeof(op));
+    if constexpr (sizeof(T) == 8) {
+      op.kind = kOpGramD;
+      op.u.gd = g;
+    } else {
+      op.kind = kOpGramF;
+      op.u.gf = g;
+    }
+    op.units = prog_units(g.n);
+    op.rd = rd;
+    prog_push(op);
+    return;
+  }
+  ++launch_count();
   const long long q = (g.n / Pack<T>::N + 1) / 2;   // two packets per thread
   switch (g.m) {
 #define BK_GRAM(M)                                                        \

@@ -24,6 +24,7 @@ Ctx& Ctx::get() {
     BK_CHECK(cudaStreamCreateWithFlags(&cx.st, cudaStreamNonBlocking));
     const char* loop = std::getenv("BKSP_GPU_LOOP");
     cx.use_cond_graph = !(loop && std::string(loop) == "poll");
+    cx.persistent = loop && std::string(loop) == "persist";
     // Keep freed solve buffers cached in the device pool between calls.
     cudaMemPool_t pool;
     if (cudaDeviceGetDefaultMemPool(&pool, cx.device) == cudaSuccess) {
@@ -579,8 +580,47 @@ static bool run_graph_while(SolveState& ss,
   return ok;
 }
 
+// Records `body` and runs it in the group's persistent launch; false when
+// the body has an operation without a persistent form (the caller then
+// runs the graph loop).
+static bool run_persist_member(PersistGroup& grp, SolveState& ss,
+                               const std::function<void(cudaStream_t)>& body,
+                               cudaStream_t st, CtlH& out) {
+  std::vector<ProgOpH> ops;
+  const long long c0 = launch_count(), y0 = byte_count();
+  bool ok = true;
+  g_prog_rec = &ops;
+  ss.has_cond = false;
+  try {
+    body(st);
+  } catch (const CudaError&) {
+    ok = false;
+  }
+  g_prog_rec = nullptr;
+  const long long body_bytes = byte_count() - y0;
+  launch_count() = c0;
+  byte_count() = y0;
+  if (!ok || ops.empty()) {
+    grp.withdraw(st);
+    return false;
+  }
+  out = grp.join(ss, ops, st);
+  launch_count() += 1;
+  byte_count() += body_bytes * out.trips;
+  return true;
+}
+
 CtlH run_loop(SolveState& ss, const std::function<void(cudaStream_t)>& body,
               cudaStream_t st) {
+  if (PersistGroup* grp = persist_group()) {
+    persist_group() = nullptr;
+    CtlH c;
+    if (run_persist_member(*grp, ss, body, st, c)) return c;
+  } else if (Ctx::get().persistent) {
+    PersistGroup one(1);   // this solve alone in a persistent launch
+    CtlH c;
+    if (run_persist_member(one, ss, body, st, c)) return c;
+  }
   Ctx& cx = Ctx::get();
   if (cx.use_cond_graph) {
     long long bk_n = 0, bk_bytes = 0;

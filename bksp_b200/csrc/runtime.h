@@ -33,6 +33,7 @@ struct Ctx {
   int device = 0;
   cudaStream_t st = nullptr;
   bool use_cond_graph = true;   // CUDA-graph while loop (else host polling)
+  bool persistent = false;      // iteration loops as persistent launches
   static Ctx& get();
 };
 
@@ -208,9 +209,47 @@ struct Lc {
 
 // Runs `body` (one iteration's launches) until the solve is done, as a
 // CUDA-graph while loop (one graph launch per solve) or, as fallback, by
-// host polling.  Returns the final control block.
+// host polling.  Returns the final control block.  When the calling thread
+// has joined a persistent group (persist_group()), the body is recorded
+// instead and runs, with the group's other systems, inside one persistent
+// launch; a body that cannot be recorded runs as a graph loop.
 CtlH run_loop(SolveState& ss, const std::function<void(cudaStream_t)>& body,
               cudaStream_t st);
+
+// A set of solves whose iteration loops run together in one persistent
+// cooperative launch (kernels_persist.cu).  Each member thread runs its
+// solve as usual up to run_loop, which records the iteration, hands it to
+// the group and waits; the last of `expected` members to arrive (or to
+// withdraw) launches the kernel for all of them, after every member's
+// set-up work on its own stream.  Every member then continues on its own
+// stream with its converged state.
+struct PersistGroup {
+  explicit PersistGroup(int expected);
+  ~PersistGroup();
+  PersistGroup(const PersistGroup&) = delete;
+  PersistGroup& operator=(const PersistGroup&) = delete;
+  // Hand in this member's recorded iteration; returns its control block
+  // after the launch (throws CudaError when the launch failed).
+  CtlH join(SolveState& ss, std::vector<ProgOpH>& ops, cudaStream_t st);
+  // This member will not join (its solve ended before the loop, or its
+  // body has no persistent form).
+  void withdraw(cudaStream_t st);
+  // Launch parameters (set before any member arrives).
+  long long spin_limit = 0;   // 0: default
+  int absent_cta = -1;        // test hook (PersistH::absent_cta)
+  int max_grid = 0;           // 0: every CTA that fits
+  // Results.
+  int status = 0;             // 0 ok, 1 a barrier wait ran out, 2 launch error
+  int grid = 0;               // CTAs launched
+  int err_phase = -1;
+ private:
+  struct Impl;
+  Impl* p_;
+  void launch_locked(cudaStream_t st);
+};
+// The group the calling thread's next run_loop joins (null: none); run_loop
+// clears it, so one solve joins at most once.
+PersistGroup*& persist_group();
 
 // Convenience for SpMV launches.
 template <typename T>

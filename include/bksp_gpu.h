@@ -203,16 +203,27 @@ int bksp_dbicgstabl_mixed(dspmat *A, double *b, const bksp_gpu_mixed_opts *opts,
 
 /* ------------------------------------------------------------ batches */
 
-/* Many independent systems in one call: `workers` host threads (0: 8; at
- * most count), each with its own CUDA stream, take the systems in turn and
- * solve each exactly as bksp_gpu_solve_mixed / bksp_gpu_solve would, so the
- * GPU runs several systems' solves at once and every result equals the
- * single-system call's.  A[i], b[i], x[i]: system i's operator and device
- * vectors (x in/out); they must be ready when the call is made, and every
- * x[i] holds its result when it returns.  stats: NULL or count entries
- * (stats[i].ret = system i's return code).  Returns 0 when every system
- * converged, NOT_CONVERGED when at least one did not (or diverged),
- * INVALID_PARAMETERS on bad arguments or a failed system. */
+/* Many independent systems in one call, each solved as bksp_gpu_solve_mixed
+ * / bksp_gpu_solve would solve it.
+ *   workers = 0: one persistent launch.  Each system's set-up (initial
+ *     residual, preconditioner values) runs on a host thread of its own;
+ *     then a single cooperative kernel iterates every system in lockstep,
+ *     operation by operation, with a per-system convergence mask: a
+ *     converged system drops out, the others continue, and each phase's
+ *     work is spread over the whole GPU.  Grid barriers are bounded: a
+ *     wait that runs out ends the launch and the call returns
+ *     INVALID_PARAMETERS (bksp_gpu_persist_status reports it).  Up to
+ *     512 systems; a system whose method has no persistent form (block
+ *     and shifted methods, Gram steps of more than five vectors) runs as
+ *     its own CUDA-graph loop.
+ *   workers > 0: that many host threads (at most count), each with its own
+ *     stream, solve the systems in turn, one CUDA-graph loop per system.
+ * A[i], b[i], x[i]: system i's operator and device vectors (x in/out); they
+ * must be ready when the call is made, and every x[i] holds its result when
+ * it returns.  stats: NULL or count entries (stats[i].ret = system i's
+ * return code).  Returns 0 when every system converged, NOT_CONVERGED when
+ * at least one did not (or diverged), INVALID_PARAMETERS on bad arguments
+ * or a failed system. */
 int bksp_gpu_solve_mixed_batch(bksp_gpu_matrix *const *A, const double *const *b,
                                double *const *x, int count,
                                const bksp_gpu_mixed_opts *opts, int workers,
@@ -221,6 +232,25 @@ int bksp_gpu_solve_batch(bksp_gpu_matrix *const *A, int method, int l,
                          const double *const *b, double *const *x, int count,
                          double tol, int max_iter, int workers,
                          bksp_gpu_stats *stats);
+
+/* Iteration loop of the calling thread's subsequent single-system solves:
+ * 0 a CUDA-graph while loop (default), 1 a persistent launch (the batch
+ * path's kernel with one system: one launch per solve, a grid barrier per
+ * operation; pays off for small systems, where a graph's per-kernel cost
+ * dominates).  Other values only query.  Returns the previous mode.  The
+ * BKSP_GPU_LOOP=persist environment variable sets 1 as the default. */
+int bksp_gpu_loop_mode(int mode);
+
+/* Status of the calling thread's last persistent batch: 0 ok, 1 a grid
+ * barrier wait ran out of polls, 2 the launch failed; *grid (may be NULL)
+ * receives the CTAs it launched. */
+int bksp_gpu_persist_status(int *grid);
+
+/* Test hook for the persistent batch's bounded waits (calling thread's
+ * subsequent batches): polls per barrier wait before giving up (0: the
+ * default, or BKSP_GPU_SPIN_LIMIT), and a CTA that never arrives at a
+ * barrier (-1: none), which makes the others' waits run out. */
+void bksp_gpu_persist_debug(long long spin_limit, int absent_cta);
 
 /* The FP64 relative true residual of bksp_gpu_true_residual, computed
  * without allocating any memory, for callers that cannot allocate device

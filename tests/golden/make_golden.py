@@ -2,6 +2,7 @@
 that has the reference sources; the outputs are committed).
 
     make -C oracle && OPENBLAS_NUM_THREADS=1 python tests/golden/make_golden.py
+    OPENBLAS_NUM_THREADS=8 OMP_NUM_THREADS=8 python tests/golden/make_golden.py --full
 
 * ``testmats.npz`` -- the reference's two test matrices (testmat/bfwb398.mtx,
   symmetric, one triangle; testmat/pde2961.mtx, general) as read by the
@@ -13,6 +14,9 @@ that has the reference sources; the outputs are committed).
   residual and the per-iteration convergence-test history, for the calls of
   tests/test.c and for small seeded configurations of the benchmark problems
   (bksp_b200.problems).
+* ``reference_full.json`` (``--full``) -- the same records at the full sizes
+  of the block and shifted benchmark configurations (3D Poisson 64^3 with 16
+  right-hand sides; 2D convection-diffusion 1024^2 with 32 shifts).
 """
 import ctypes as C
 import json
@@ -163,5 +167,33 @@ def main():
         json.dump(out, f, indent=1)
 
 
+def main_full():
+    """Full-size configurations (minutes of CPU each), written to
+    reference_full.json: shifted BiCGSTAB(4) with 32 shifts on the 2D
+    convection-diffusion 1024^2 operator, and Block CG / Block BiCGSTAB(2)
+    with 16 right-hand sides on the 3D Poisson 64^3 operator."""
+    out = {"threads": os.environ.get("OPENBLAS_NUM_THREADS", "default")}
+    rp, c, v, n = P.poisson3d(64)
+    lrp, lc, lv, _ = P.lower_triangle(rp, c, v, n)
+    Af = csr(rp, c, v, n)
+    Bm = np.random.default_rng(2).standard_normal((n, 16))
+    record(out, "cfg3/blcg_p64", R.Matrix(lrp, lc, lv, n, symmetric=True), Af, None,
+           "dblcg", (Bm, 1e-8, 5000, np.zeros((n, 16))), kind="block")
+    record(out, "cfg3/blbicgstabl2_p64", R.Matrix(rp, c, v, n), Af, None,
+           "dblbicgstabl", (Bm, 2, 1e-8, 5000, np.zeros((n, 16))), kind="block")
+    rp, c, v, n = P.convdiff2d(1024)
+    Af = csr(rp, c, v, n)
+    b = P.uniform(n, 3)
+    sig = P.log_shifts(32)
+    record(out, "cfg4/shbicgstabl4_cd1024", R.Matrix(rp, c, v, n), Af, b,
+           "dshbicgstabl", (b, 4, sig, 32, 1e-8, 5000, np.zeros(33 * n)),
+           kind="shift", sigma=sig)
+    with open(os.path.join(HERE, "reference_full.json"), "w") as f:
+        json.dump(out, f, indent=1)
+
+
 if __name__ == "__main__":
-    main()
+    if "--full" in sys.argv[1:]:
+        main_full()
+    else:
+        main()

@@ -1,0 +1,167 @@
+"""GPU tests of the persistent loop (kernels_persist.cu): a batch of
+systems iterated in one cooperative launch with per-system convergence
+masks, and single solves run as a persistent launch.
+
+The persistent kernel does each element's arithmetic exactly as the
+stand-alone kernels do; only the order in which per-CTA partial dot
+products are added differs, so results agree with the graph loop to
+rounding, not bit for bit: iteration counts within one, histories to
+1e-9 relative while well above the rounding floor, every system at its
+FP64 target."""
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+from bksp_b200 import problems as P
+from oracle import solvers as S
+from conftest import hist_close
+
+pytestmark = pytest.mark.gpu
+
+
+def _dev(torch, a):
+    return torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).cuda()
+
+
+@pytest.fixture(scope="module")
+def kbatch(gpu):
+    B = gpu
+    out = []
+    for i, L in enumerate((10, 13, 16, 12, 19, 14, 22, 9)):
+        rp, c, v, n = P.kappa_diffusion3d(L, 150 + i)
+        b = np.random.default_rng(180 + i).standard_normal(n)
+        A = sp.csr_matrix((v, c, rp), shape=(n, n))
+        out.append((B.GpuMatrix(B.CsrMatrix(rp, c, v), B.FP32), A, b))
+    yield out
+    for s in out:
+        s[0].close()
+
+
+@pytest.fixture(scope="module")
+def kmodel(gpu):
+    B = gpu
+    mats = [B.GpuMatrix(B.CsrMatrix(*P.kappa_diffusion3d(L, 900 + L)[:3]), B.FP32)
+            for L in (10, 12, 14)]
+    model = B.SpaiModel(seed=2)
+    model.train(mats, epochs=60, probes=8, lr=3e-3, seed=3)
+    yield model
+    for m in mats:
+        m.close()
+    model.close()
+
+
+@pytest.mark.parametrize("precond,l", [(0, 2), (1, 2), (2, 2), (2, 4)])
+def test_persistent_mixed_batch_matches_graph_loops(gpu, kbatch, kmodel, precond, l):
+    import torch
+    B = gpu
+    mats = [s[0] for s in kbatch]
+    bs = [_dev(torch, s[2]) for s in kbatch]
+    xp = [torch.zeros_like(b) for b in bs]
+    xg = [torch.zeros_like(b) for b in bs]
+    torch.cuda.synchronize()
+    rp_, sp_ = B.solve_mixed_batch(mats, [b.data_ptr() for b in bs],
+                                   [x.data_ptr() for x in xp], l=l, target=1e-8,
+                                   precond=precond, model=kmodel, workers=0)
+    status, grid = B.persist_status()
+    assert status == 0 and grid >= 1
+    rg_, sg_ = B.solve_mixed_batch(mats, [b.data_ptr() for b in bs],
+                                   [x.data_ptr() for x in xg], l=l, target=1e-8,
+                                   precond=precond, model=kmodel, workers=4)
+    assert rp_ == 0 and rg_ == 0, ([s["ret"] for s in sp_], [s["ret"] for s in sg_])
+    for (G, A, b), x1, x2, s1, s2 in zip(kbatch, xp, xg, sp_, sg_):
+        assert abs(s1["ret"] - s2["ret"]) <= 1, (s1["ret"], s2["ret"])
+        xh = x1.cpu().numpy()
+        assert S.true_residual(A, b, xh) <= 1e-8
+        ref = x2.cpu().numpy()
+        assert np.linalg.norm(xh - ref) <= 1e-6 * np.linalg.norm(ref)
+
+
+def test_persistent_fp64_batch_matches_graph_loops(gpu, kbatch):
+    """FP64 BiCGSTAB(2) (one-pass MR step) and CG: the persistent batch and
+    per-system graph loops agree to rounding."""
+    import torch
+    B = gpu
+    mats = [s[0] for s in kbatch]
+    bs = [_dev(torch, s[2]) for s in kbatch]
+    for method in (B.BICGSTABL_FAST, B.CG, B.BICGSTAB):
+        xp = [torch.zeros_like(b) for b in bs]
+        xg = [torch.zeros_like(b) for b in bs]
+        torch.cuda.synchronize()
+        r1, s1 = B.solve_batch(mats, method, [b.data_ptr() for b in bs],
+                               [x.data_ptr() for x in xp], 1e-9, 5000, l=2, workers=0)
+        assert B.persist_status()[0] == 0
+        r2, s2 = B.solve_batch(mats, method, [b.data_ptr() for b in bs],
+                               [x.data_ptr() for x in xg], 1e-9, 5000, l=2, workers=3)
+        assert r1 == 0 and r2 == 0
+        for (G, A, b), a1, a2, x1 in zip(kbatch, s1, s2, xp):
+            assert abs(a1["ret"] - a2["ret"]) <= 1, (method, a1["ret"], a2["ret"])
+            assert S.true_residual(A, b, x1.cpu().numpy()) <= 2e-9
+
+
+@pytest.mark.parametrize("method,l", [("cg", 0), ("bicgstab", 0), ("bicgstabl", 4),
+                                      ("bicgstabl_fast", 2), ("cr", 0)])
+def test_single_solve_persistent_matches_graph_loop(gpu, method, l):
+    """One system, loop mode 1 (persistent launch) against the default
+    graph loop: the same return index and residual history."""
+    import torch
+    B = gpu
+    if method in ("cg", "cr"):
+        rp, c, v, n = P.poisson2d(64)
+        b = P.uniform(n, 0)
+    else:
+        rp, c, v, n = P.convdiff3d(20)
+        A0 = sp.csr_matrix((v, c, rp), shape=(n, n))
+        b = A0 @ P.uniform(n, 1)
+    G = B.GpuMatrix(B.CsrMatrix(rp, c, v))
+    code = {"cg": B.CG, "cr": B.CR, "bicgstab": B.BICGSTAB, "bicgstabl": B.BICGSTABL,
+            "bicgstabl_fast": B.BICGSTABL_FAST}[method]
+    bd = _dev(torch, b)
+    out = {}
+    for mode in (0, 1):
+        x = torch.zeros_like(bd)
+        torch.cuda.synchronize()
+        with B.loop_mode(mode):
+            ret, st = G.solve(code, bd.data_ptr(), x.data_ptr(), 1e-10, 3000, l=l,
+                              hist_cap=4000)
+        out[mode] = (ret, st, x.cpu().numpy())
+    (r0, s0, x0), (r1, s1, x1) = out[0], out[1]
+    assert r0 >= 0 and abs(r0 - r1) <= 1, (r0, r1)
+    hist_close(s1["hist"], s0["hist"], k=40, rtol=1e-9, floor=1e-8)
+    A = sp.csr_matrix((v, c, rp), shape=(n, n))
+    assert S.true_residual(A, b, x1) < 1e-9
+    # The persistent launch is one launch (plus set-up) instead of one per
+    # kernel per iteration.
+    assert s1["launches"] < s0["launches"] / 4
+    G.close()
+
+
+def test_persistent_barrier_wait_runs_out(gpu, kbatch):
+    """Failure detection of the persistent loop's grid barriers: one CTA
+    never arrives (the test hook), so the others' bounded waits run out; the
+    call reports the failure instead of hanging, and the device stays
+    usable for the next batch."""
+    import torch
+    B = gpu
+    mats = [s[0] for s in kbatch[:4]]
+    bs = [_dev(torch, s[2]) for s in kbatch[:4]]
+    xs = [torch.zeros_like(b) for b in bs]
+    torch.cuda.synchronize()
+    B.persist_debug(spin_limit=20000, absent_cta=0)
+    try:
+        ret, _ = B.solve_batch(mats, B.BICGSTABL_FAST, [b.data_ptr() for b in bs],
+                               [x.data_ptr() for x in xs], 1e-9, 500, l=2, workers=0)
+        status, grid = B.persist_status()
+    finally:
+        B.persist_debug(0, -1)
+    assert grid >= 2
+    assert status == 1
+    assert ret == B.INVALID_PARAMETERS
+    # The context is intact: the same batch now converges.
+    for x in xs:
+        x.zero_()
+    torch.cuda.synchronize()
+    ret, st = B.solve_batch(mats, B.BICGSTABL_FAST, [b.data_ptr() for b in bs],
+                            [x.data_ptr() for x in xs], 1e-9, 5000, l=2, workers=0)
+    assert ret == 0 and B.persist_status()[0] == 0
+    for (G, A, b), x in zip(kbatch[:4], xs):
+        assert S.true_residual(A, b, x.cpu().numpy()) <= 2e-9
