@@ -617,11 +617,11 @@ def run_batch(a):
     f ~ N(0,1); time to an FP64 true relative residual of 1e-8 on every
     system.  value: mixed-precision BiCGSTAB(2) with the learned SPAI
     preconditioner (trained beforehand on 64 smaller systems of the same
-    family, seeds 1000+i), all systems in one persistent launch; plain_fp64_s:
-    FP64 BiCGSTAB(2) on the Jacobi right-scaled systems A D^-1 y = b, x = D^-1 y,
-    batched the same way; the modes also time both with one CUDA-graph loop
-    per system on eight host threads (*_graphs) and the learned solve one
-    system at a time (mixed_learned_sequential)."""
+    family, seeds 1000+i), one CUDA-graph loop per system on eight host
+    threads; plain_fp64_s: FP64 BiCGSTAB(2) on the Jacobi right-scaled
+    systems A D^-1 y = b, x = D^-1 y, batched the same way; the modes also
+    time both as one persistent launch for the whole batch (*_persistent)
+    and the learned solve one system at a time (mixed_learned_sequential)."""
     import torch
     import torch.distributed as dist
     import bksp_b200 as B
@@ -712,14 +712,14 @@ def run_batch(a):
         return w
 
     res = {}
-    # workers=0: every system in one persistent launch (the default);
-    # workers=8: eight host threads, one CUDA-graph loop per system;
+    # workers=8: eight host threads, one CUDA-graph loop per system (the
+    # default); workers=-1: every system in one persistent launch;
     # workers=1: one system after the other.
-    for name, fn, k, scale in (("plain_fp64", plain(), a.steps, True),
-                               ("plain_fp64_graphs", plain(8), a.steps, True),
+    for name, fn, k, scale in (("plain_fp64", plain(8), a.steps, True),
+                               ("plain_fp64_persistent", plain(-1), a.steps, True),
                                ("mixed_learned_sequential", learned(1), 1, False),
-                               ("mixed_learned_graphs", learned(8), a.steps, False),
-                               ("mixed_learned", learned(), a.steps, False)):
+                               ("mixed_learned_persistent", learned(-1), a.steps, False),
+                               ("mixed_learned", learned(8), a.steps, False)):
         for _ in range(a.warmup if k > 1 else 0):
             for x in xs:
                 x.zero_()

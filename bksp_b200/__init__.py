@@ -520,9 +520,9 @@ def solve_mixed_batch(mats, bs, xs, l=4, target=1e-8, max_iter=10000,
                       workers=0):
     """bksp_gpu_solve_mixed_batch: mixed-precision BiCGSTAB(l) on every
     (GpuMatrix, b, x) of the lists (device pointers, ready before the call,
-    x in/out); workers=0: all systems in one persistent launch, workers>0:
-    that many host threads, one graph loop per system.  Returns (ret,
-    per-system stats)."""
+    x in/out); workers>=0: that many host threads (0: 8), one graph loop
+    per system; workers<0: all systems in one persistent launch.  Returns
+    (ret, per-system stats)."""
     n, A, B, X, st = _batch_args(mats, bs, xs)
     o = MixedOpts(l, target, max_iter, precond,
                   model.h if model is not None else None, delta, period,

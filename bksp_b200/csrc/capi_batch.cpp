@@ -1,18 +1,18 @@
 // Batched solves (bksp_gpu.h): many independent systems in one call.
 //
-// Default (workers = 0): one persistent launch.  Every system's solve runs
-// on a host thread of its own up to its iteration loop (operator-dependent
-// set-up such as the learned preconditioner's values, the initial
-// residual), records one iteration of its method and joins a
-// PersistGroup; the group's last member launches one cooperative kernel
-// that iterates all systems in lockstep with per-system convergence masks
+// workers >= 0 (default 0 = 8): that many host worker threads take systems
+// from a shared counter and run the ordinary device solve on each, on the
+// worker's own CUDA stream -- one CUDA graph with its own device-side while
+// loop per system, graphs of different workers running concurrently.
+//
+// workers < 0: one persistent launch.  Every system's solve runs on a host
+// thread of its own up to its iteration loop (operator-dependent set-up
+// such as the learned preconditioner's values, the initial residual),
+// records one iteration of its method and joins a PersistGroup; the
+// group's last member launches one cooperative kernel that iterates all
+// systems in lockstep with per-system convergence masks
 // (kernels_persist.cu).  A system whose iteration has no persistent form,
 // and a learned solve's Jacobi retry, run as a graph loop instead.
-//
-// workers > 0: that many host worker threads take systems from a shared
-// counter and run the ordinary device solve on each, on the worker's own
-// CUDA stream -- one CUDA graph with its own device-side while loop per
-// system, graphs of different workers running concurrently.
 //
 // Either way each system's result does not depend on what runs beside it.
 #include <cuda_runtime.h>
@@ -132,10 +132,10 @@ int bksp_gpu_solve_mixed_batch(bksp_gpu_matrix* const* A, const double* const* b
     return bksp_gpu_solve_mixed(A[i], b[i], x[i], opts, nullptr,
                                 stats ? &stats[i] : nullptr);
   };
-  if (workers > 0)
-    run_workers(count, workers, one, rets);
-  else
+  if (workers < 0)
     run_persistent(count, one, rets);
+  else
+    run_workers(count, workers > 0 ? workers : 8, one, rets);
   return summarise(rets);
 }
 
@@ -152,10 +152,10 @@ int bksp_gpu_solve_batch(bksp_gpu_matrix* const* A, int method, int l,
     return bksp_gpu_solve(A[i], method, l, b[i], x[i], tol, max_iter, nullptr,
                           stats ? &stats[i] : nullptr);
   };
-  if (workers > 0)
-    run_workers(count, workers, one, rets);
-  else
+  if (workers < 0)
     run_persistent(count, one, rets);
+  else
+    run_workers(count, workers > 0 ? workers : 8, one, rets);
   return summarise(rets);
 }
 

@@ -247,7 +247,8 @@ void launch_rm2cm(const double* rm, double* cm, int n, int s, cudaStream_t st);
 // system: each CTA that worked on a system publishes one partial per dot,
 // the last of them sums the partials in CTA-slot order and runs the
 // system's scalar epilogue.
-constexpr int kPersistUnit = 1024;
+constexpr int kPersistThreads = 256;   // threads per CTA
+constexpr int kPersistUnit = 1024;     // four rows / elements per thread
 constexpr int kPersistMaxSys = 512;
 enum : int {
   kOpNone = 0,
@@ -296,8 +297,16 @@ struct PBarH {
   int err;        // 1: a barrier wait ran out of polls
   int err_phase;  // the phase at which it did
 };
+// What a phase needs to know of an operation before loading it: its units
+// and guard slot.
+struct OpHdrH {
+  int units;
+  int guard;
+  const double* S;
+};
 struct PersistH {
   const ProgOpH* ops;   // [nsys][max_ops]
+  const OpHdrH* hdr;    // [nsys][max_ops] (units 0: no operation)
   const int* nops;      // operations per system
   CtlH* const* ctl;     // each system's control block
   int nsys, max_ops;
@@ -311,6 +320,9 @@ struct PersistH {
 inline thread_local void* g_prog_rec = nullptr;
 void prog_push(const ProgOpH& op);           // runtime.cpp
 [[noreturn]] void prog_unsupported(const char* what);
+// Vector operands of a recorded operation: 16-byte aligned (else the
+// operation has no persistent form).
+void prog_require_aligned(const void* p);
 // Units of kPersistUnit covering n rows / elements (at least one).
 inline int prog_units(long long n) {
   const long long u = (n + kPersistUnit - 1) / kPersistUnit;

@@ -188,6 +188,10 @@ void launch_mx_d2f(const double* in, float* o0, float* o1, float* o2,
                    cudaStream_t st) {
   byte_count() += n * (8 + 4 * ((o1 != nullptr) + (o2 != nullptr) + 1 + (w != nullptr)));
   if (g_prog_rec) {
+    if (n % 4) prog_unsupported("unpadded vector");
+    for (const void* p : {(const void*)in, (const void*)o0, (const void*)o1,
+                          (const void*)o2, (const void*)w})
+      if (p) prog_require_aligned(p);
     ProgOpH op;
     std::memset(&op, 0, sizeof(op));
     op.kind = kOpMxD2f;
@@ -220,6 +224,10 @@ void launch_mx_accum(double* x, const float* t, float* y, long long n,
                      const RedH& rd, cudaStream_t st) {
   byte_count() += n * 24;   // x read and written, t read, y written
   if (g_prog_rec) {
+    if (n % 4) prog_unsupported("unpadded vector");
+    prog_require_aligned(x);
+    prog_require_aligned(t);
+    prog_require_aligned(y);
     ProgOpH op;
     std::memset(&op, 0, sizeof(op));
     op.kind = kOpMxAccum;

@@ -49,6 +49,9 @@ static long long lc_bytes(const LcH<T>& d) {
 template <typename T>
 static void lc_record(const LcH<T>& d, const RedH& rd) {
   if (d.nd > 3) prog_unsupported("linear combination with more than three dots");
+  if (d.n % 4 || (d.reps > 1 && d.stride % 4)) prog_unsupported("unpadded vector");
+  for (int i = 0; i < d.nin; ++i) prog_require_aligned(d.in[i]);
+  for (int o = 0; o < d.nout; ++o) prog_require_aligned(d.out[o]);
   ProgOpH op;
   std::memset(&op, 0, sizeof(op));
   if constexpr (sizeof(T) == 8) {
@@ -83,6 +86,8 @@ static void gram_dispatch(const GramH<T>& g, const RedH& rd, cudaStream_t st) {
   byte_count() += (long long)g.m * g.n * (long long)sizeof(T);
   if (g_prog_rec) {
     if (g.m > kPersistGramMax) prog_unsupported("Gram of more than five vectors");
+    if (g.n % 4) prog_unsupported("unpadded vector");
+    for (int i = 0; i < g.m; ++i) prog_require_aligned(g.v[i]);
     ProgOpH op;
     std::memset(&op, 0, sizeof(op));
     if constexpr (sizeof(T) == 8) {

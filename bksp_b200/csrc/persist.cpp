@@ -8,6 +8,7 @@
 #include <condition_variable>
 #include <cstdio>
 #include <cstdlib>
+#include <cstdint>
 #include <cstring>
 #include <mutex>
 #include <vector>
@@ -22,6 +23,10 @@ void prog_push(const ProgOpH& op) {
 
 void prog_unsupported(const char* what) {
   throw CudaError(std::string("no persistent form: ") + what);
+}
+
+void prog_require_aligned(const void* p) {
+  if (reinterpret_cast<uintptr_t>(p) & 15u) prog_unsupported("unaligned vector");
 }
 
 PersistGroup*& persist_group() {
@@ -112,7 +117,10 @@ void PersistGroup::launch_locked(cudaStream_t st) {
     if (nsys > kPersistMaxSys) throw CudaError("persistent group too large");
     int max_ops = 0;
     for (auto& m : g.members) max_ops = std::max(max_ops, (int)m.ops.size());
-    // Widest phase: the grid needs no more CTAs than its units.
+    // Grid: at least kUnitsPerCta units of the widest phase per CTA (a
+    // CTA streams its units back to back; below that the barrier costs more
+    // than the extra parallelism gains), at most every CTA that fits.
+    constexpr long long kUnitsPerCta = 4;
     long long widest = 1;
     for (int k = 0; k < max_ops; ++k) {
       long long u = 0;
@@ -122,20 +130,29 @@ void PersistGroup::launch_locked(cudaStream_t st) {
     }
     int cap = persist_max_grid();
     if (max_grid > 0) cap = std::min(cap, max_grid);
-    grid = (int)std::min<long long>(widest, cap);
-    // Device layout: operations, control-block pointers, counts, barrier.
-    const size_t ops_b = sizeof(ProgOpH) * (size_t)nsys * max_ops;
+    grid = (int)std::max<long long>(1, std::min<long long>((widest + kUnitsPerCta - 1) / kUnitsPerCta, cap));
+    if (absent_cta >= 0) grid = std::max(grid, std::min(cap, absent_cta + 2));
+    // Device layout: operations, their headers, control-block pointers,
+    // counts, barrier.
+    const size_t nop = (size_t)nsys * max_ops;
+    const size_t ops_b = sizeof(ProgOpH) * nop;
+    const size_t hdr_b = sizeof(OpHdrH) * nop;
     const size_t ctl_b = sizeof(CtlH*) * nsys;
     const size_t cnt_b = sizeof(int) * nsys;
     auto up16 = [](size_t x) { return (x + 15) / 16 * 16; };
-    const size_t off_ctl = up16(ops_b), off_cnt = off_ctl + up16(ctl_b),
-                 off_bar = off_cnt + up16(cnt_b);
+    const size_t off_hdr = up16(ops_b), off_ctl = off_hdr + up16(hdr_b),
+                 off_cnt = off_ctl + up16(ctl_b), off_bar = off_cnt + up16(cnt_b);
     const size_t total = off_bar + up16(sizeof(PBarH));
     std::vector<unsigned char> host(total, 0);
     for (int s = 0; s < nsys; ++s) {
       auto& m = g.members[s];
       std::memcpy(host.data() + sizeof(ProgOpH) * (size_t)s * max_ops,
                   m.ops.data(), sizeof(ProgOpH) * m.ops.size());
+      for (size_t k = 0; k < m.ops.size(); ++k) {
+        const OpHdrH h{m.ops[k].units, m.ops[k].rd.guard, m.ops[k].rd.S};
+        std::memcpy(host.data() + off_hdr + sizeof(OpHdrH) * ((size_t)s * max_ops + k),
+                    &h, sizeof(h));
+      }
       CtlH* c = m.ss->ctl;
       std::memcpy(host.data() + off_ctl + sizeof(CtlH*) * s, &c, sizeof(c));
       const int n = (int)m.ops.size();
@@ -147,6 +164,7 @@ void PersistGroup::launch_locked(cudaStream_t st) {
     BK_CHECK(cudaMemcpyAsync(dev, host.data(), total, cudaMemcpyHostToDevice, st));
     PersistH p;
     p.ops = reinterpret_cast<const ProgOpH*>(dev);
+    p.hdr = reinterpret_cast<const OpHdrH*>(dev + off_hdr);
     p.ctl = reinterpret_cast<CtlH* const*>(dev + off_ctl);
     p.nops = reinterpret_cast<const int*>(dev + off_cnt);
     p.nsys = nsys;

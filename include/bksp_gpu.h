@@ -205,7 +205,10 @@ int bksp_dbicgstabl_mixed(dspmat *A, double *b, const bksp_gpu_mixed_opts *opts,
 
 /* Many independent systems in one call, each solved as bksp_gpu_solve_mixed
  * / bksp_gpu_solve would solve it.
- *   workers = 0: one persistent launch.  Each system's set-up (initial
+ *   workers >= 0: that many host threads (0: 8; at most count), each with
+ *     its own stream, solve the systems in turn, one CUDA-graph loop per
+ *     system.
+ *   workers < 0: one persistent launch.  Each system's set-up (initial
  *     residual, preconditioner values) runs on a host thread of its own;
  *     then a single cooperative kernel iterates every system in lockstep,
  *     operation by operation, with a per-system convergence mask: a
@@ -215,9 +218,10 @@ int bksp_dbicgstabl_mixed(dspmat *A, double *b, const bksp_gpu_mixed_opts *opts,
  *     INVALID_PARAMETERS (bksp_gpu_persist_status reports it).  Up to
  *     512 systems; a system whose method has no persistent form (block
  *     and shifted methods, Gram steps of more than five vectors) runs as
- *     its own CUDA-graph loop.
- *   workers > 0: that many host threads (at most count), each with its own
- *     stream, solve the systems in turn, one CUDA-graph loop per system.
+ *     its own CUDA-graph loop.  On the benchmark batch (64 systems of
+ *     32^3..96^3 rows) this mode is about four times slower than the
+ *     graph loops: one CTA of eight warps per SM keeps too few loads in
+ *     flight for the streaming phases.
  * A[i], b[i], x[i]: system i's operator and device vectors (x in/out); they
  * must be ready when the call is made, and every x[i] holds its result when
  * it returns.  stats: NULL or count entries (stats[i].ret = system i's
