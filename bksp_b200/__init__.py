@@ -109,6 +109,9 @@ def _load():
     L.bksp_gpu_solve_mixed.argtypes = [vp, vp, vp, C.POINTER(MixedOpts), vp,
                                        C.POINTER(Stats)]
     L.bksp_dbicgstabl_mixed.argtypes = [sp, _dp, C.POINTER(MixedOpts), _dp]
+    L.bksp_gpu_cg_mixed.argtypes = [vp, vp, vp, C.POINTER(MixedOpts), vp,
+                                    C.POINTER(Stats)]
+    L.bksp_dcg_mixed.argtypes = [sp, _dp, C.POINTER(MixedOpts), _dp]
     L.bksp_gpu_solve_mixed_batch.argtypes = [C.POINTER(vp), C.POINTER(vp),
                                              C.POINTER(vp), i,
                                              C.POINTER(MixedOpts), i,
@@ -361,16 +364,17 @@ class GpuMatrix:
 
     def solve_mixed(self, b_ptr, x_ptr, l=4, target=1e-8, max_iter=10000,
                     precond=0, model=None, delta=0.0, period=0, fallback=1,
-                    stream=None, hist_cap=0):
-        """Mixed-precision BiCGSTAB(l) on device vectors; (ret, stats)."""
+                    stream=None, hist_cap=0, method="bicgstabl"):
+        """Mixed-precision BiCGSTAB(l) (method="cg": preconditioned CG,
+        bksp_gpu_cg_mixed) on device vectors; (ret, stats)."""
         o = MixedOpts(l, target, max_iter, precond,
                       model.h if model is not None else None, delta, period,
                       fallback)
         buf = np.zeros(max(int(hist_cap), 1))
         st = Stats(buf.ctypes.data_as(_dp), int(hist_cap), 0, 0, 0.0, 0.0,
                    0.0, 0, 0, 0)
-        ret = lib.bksp_gpu_solve_mixed(self.h, b_ptr, x_ptr, C.byref(o),
-                                       stream, C.byref(st))
+        fn = lib.bksp_gpu_cg_mixed if method == "cg" else lib.bksp_gpu_solve_mixed
+        ret = fn(self.h, b_ptr, x_ptr, C.byref(o), stream, C.byref(st))
         return ret, {"ret": st.ret, "hist": buf[:min(st.hist_len, hist_cap)].copy(),
                      "iters": st.hist_len, "solve_ms": st.solve_ms,
                      "true_res": st.true_res, "launches": st.launches,
@@ -494,6 +498,17 @@ def dbicgstabl_mixed(A, b, x, l=4, target=1e-8, max_iter=10000, precond=0,
                   model.h if model is not None else None, 0.0, 0, fallback)
     return lib.bksp_dbicgstabl_mixed(A.ptr, b.ctypes.data_as(_dp), C.byref(o),
                                      _inplace(x))
+
+
+def dcg_mixed(A, b, x, target=1e-8, max_iter=10000, precond=0, model=None,
+              fallback=1):
+    """Host-array mixed-precision preconditioned CG (bksp_dcg_mixed); A is
+    a "symmetric" CsrMatrix holding one triangle, as for bksp_dcg."""
+    b = _vec(b)
+    o = MixedOpts(0, target, max_iter, precond,
+                  model.h if model is not None else None, 0.0, 0, fallback)
+    return lib.bksp_dcg_mixed(A.ptr, b.ctypes.data_as(_dp), C.byref(o),
+                              _inplace(x))
 
 
 def _batch_args(mats, bs, xs):

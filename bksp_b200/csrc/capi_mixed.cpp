@@ -44,7 +44,9 @@ int fail(const std::exception& e) {
   return INVALID_PARAMETERS;
 }
 
-MixedOut run_mixed(bksp_gpu_matrix* m, const double* db, double* dx,
+enum MixedMethod { kMixedBicgstabl = 0, kMixedCg = 1 };
+
+MixedOut run_mixed(bksp_gpu_matrix* m, int method, const double* db, double* dx,
                    const bksp_gpu_mixed_opts* o, int precond, SolveState& ss,
                    cudaStream_t st, float* mvals_scratch) {
   MixedOpts mo;
@@ -59,16 +61,22 @@ MixedOut run_mixed(bksp_gpu_matrix* m, const double* db, double* dx,
     M = &m->jacobi;
   } else if (precond == BKSP_GPU_PRECOND_LEARNED) {
     if (m->spai.ok) {
-      view = spai_apply(o->model, m, mvals_scratch, st);
+      // CG needs a symmetric preconditioner: (M + M^T) / 2.
+      view = spai_apply(o->model, m, mvals_scratch, st, method == kMixedCg);
       M = &view;
     } else if (m->diag_ok) {   // not stencil-like: Jacobi instead
       build_jacobi(m, st);
       M = &m->jacobi;
     }
   }
-  return bicgstabl_mixed(m->A, M, db, o->l, dx, o->max_iter > 0 ? o->max_iter : 10000,
-                         mo, ss, st);
+  const int max_iter = o->max_iter > 0 ? o->max_iter : 10000;
+  if (method == kMixedCg) return cg_mixed(m->A, M, db, dx, max_iter, mo, ss, st);
+  return bicgstabl_mixed(m->A, M, db, o->l, dx, max_iter, mo, ss, st);
 }
+
+int solve_mixed_impl(bksp_gpu_matrix* m, int method, const double* b, double* x,
+                     const bksp_gpu_mixed_opts* o, void* stream,
+                     bksp_gpu_stats* stats);
 
 }  // namespace
 
@@ -77,9 +85,25 @@ extern "C" {
 int bksp_gpu_solve_mixed(bksp_gpu_matrix* m, const double* b, double* x,
                          const bksp_gpu_mixed_opts* o, void* stream,
                          bksp_gpu_stats* stats) {
+  return solve_mixed_impl(m, kMixedBicgstabl, b, x, o, stream, stats);
+}
+
+int bksp_gpu_cg_mixed(bksp_gpu_matrix* m, const double* b, double* x,
+                      const bksp_gpu_mixed_opts* o, void* stream,
+                      bksp_gpu_stats* stats) {
+  return solve_mixed_impl(m, kMixedCg, b, x, o, stream, stats);
+}
+
+}  // extern "C"
+
+namespace {
+
+int solve_mixed_impl(bksp_gpu_matrix* m, int method, const double* b, double* x,
+                     const bksp_gpu_mixed_opts* o, void* stream,
+                     bksp_gpu_stats* stats) {
   if (!m || !b || !x || !o) return INVALID_PARAMETERS;
   if (!m->A.v32) return INVALID_PARAMETERS;
-  if (o->l < 1 || o->l > kBlMaxL) return INVALID_PARAMETERS;
+  if (method == kMixedBicgstabl && (o->l < 1 || o->l > kBlMaxL)) return INVALID_PARAMETERS;
   if (o->precond < 0 || o->precond > 2) return INVALID_PARAMETERS;
   if (o->precond == BKSP_GPU_PRECOND_LEARNED && !o->model) return INVALID_PARAMETERS;
   bksp_gpu_stats* saved = g_stats;
@@ -95,7 +119,8 @@ int bksp_gpu_solve_mixed(bksp_gpu_matrix* m, const double* b, double* x,
     double* dx = dalloc_n<double>(np, st);
     double* x0 = dalloc_n<double>(np, st);
     float* mv = o->precond == BKSP_GPU_PRECOND_LEARNED
-                    ? dalloc_n<float>(spai_scratch_floats(m), st) : nullptr;
+                    ? dalloc_n<float>(spai_scratch_floats(m, method == kMixedCg), st)
+                    : nullptr;
     BK_CHECK(cudaMemsetAsync(db, 0, sizeof(double) * np, st));
     BK_CHECK(cudaMemsetAsync(dx, 0, sizeof(double) * np, st));
     tm.begin_solve();
@@ -104,14 +129,15 @@ int bksp_gpu_solve_mixed(bksp_gpu_matrix* m, const double* b, double* x,
     BK_CHECK(cudaMemcpyAsync(x0, dx, sizeof(double) * np, cudaMemcpyDeviceToDevice, st));
     SolveState ss;
     ss.create(hist_cap_for(o->max_iter > 0 ? o->max_iter : 10000), st);
-    MixedOut r = run_mixed(m, db, dx, o, o->precond, ss, st, mv);
+    MixedOut r = run_mixed(m, method, db, dx, o, o->precond, ss, st, mv);
     int sweeps = 1, inner = r.iters, reps = r.replacements;
     if (r.ret < 0 && o->fallback && o->precond == BKSP_GPU_PRECOND_LEARNED) {
       // Stagnation / breakdown of the learned preconditioner: plain Jacobi
       // from the original initial guess.
       BK_CHECK(cudaMemcpyAsync(dx, x0, sizeof(double) * np, cudaMemcpyDeviceToDevice, st));
-      r = run_mixed(m, db, dx, o, m->diag_ok ? BKSP_GPU_PRECOND_JACOBI
-                                             : BKSP_GPU_PRECOND_NONE, ss, st, mv);
+      r = run_mixed(m, method, db, dx, o, m->diag_ok ? BKSP_GPU_PRECOND_JACOBI
+                                                     : BKSP_GPU_PRECOND_NONE,
+                    ss, st, mv);
       sweeps = 2;
       inner += r.iters;
       reps += r.replacements;
@@ -141,11 +167,11 @@ int bksp_gpu_solve_mixed(bksp_gpu_matrix* m, const double* b, double* x,
   return ret;
 }
 
-int bksp_dbicgstabl_mixed(dspmat* A, double* b, const bksp_gpu_mixed_opts* o,
-                          double* x) {
-  if (check_matrix(A) != 0 || !b || !x || !o) return INVALID_PARAMETERS;
+// Host arrays in the bksp.h style: upload A (flags), b, x; solve; download.
+int host_mixed(dspmat* A, int flags, int method, double* b,
+               const bksp_gpu_mixed_opts* o, double* x) {
   bksp_gpu_matrix* m = nullptr;
-  int rc = bksp_gpu_matrix_create(A, BKSP_GPU_FP32, &m);
+  int rc = bksp_gpu_matrix_create(A, flags, &m);
   if (rc != 0) return rc;
   int ret = INVALID_PARAMETERS;
   try {
@@ -155,7 +181,7 @@ int bksp_dbicgstabl_mixed(dspmat* A, double* b, const bksp_gpu_mixed_opts* o,
     double* dx = dalloc_n<double>(n, st);
     BK_CHECK(cudaMemcpyAsync(db, b, sizeof(double) * n, cudaMemcpyHostToDevice, st));
     BK_CHECK(cudaMemcpyAsync(dx, x, sizeof(double) * n, cudaMemcpyHostToDevice, st));
-    ret = bksp_gpu_solve_mixed(m, db, dx, o, st, g_stats);
+    ret = solve_mixed_impl(m, method, db, dx, o, st, g_stats);
     BK_CHECK(cudaMemcpyAsync(x, dx, sizeof(double) * n, cudaMemcpyDeviceToHost, st));
     BK_CHECK(cudaStreamSynchronize(st));
     dfree(db, st);
@@ -165,6 +191,23 @@ int bksp_dbicgstabl_mixed(dspmat* A, double* b, const bksp_gpu_mixed_opts* o,
   }
   bksp_gpu_matrix_destroy(m);
   return ret;
+}
+
+}  // namespace
+
+extern "C" {
+
+int bksp_dbicgstabl_mixed(dspmat* A, double* b, const bksp_gpu_mixed_opts* o,
+                          double* x) {
+  if (check_matrix(A) != 0 || !b || !x || !o) return INVALID_PARAMETERS;
+  return host_mixed(A, BKSP_GPU_FP32, kMixedBicgstabl, b, o, x);
+}
+
+int bksp_dcg_mixed(dspmat* A, double* b, const bksp_gpu_mixed_opts* o, double* x) {
+  if (check_matrix(A) != 0 || !b || !x || !o) return INVALID_PARAMETERS;
+  // As bksp_dcg: a "symmetric" matrix holding one triangle (src/cg.c:9-11).
+  if (!is_symmetric(A)) return INVALID_MATRIX_TYPE;
+  return host_mixed(A, BKSP_GPU_FP32 | BKSP_GPU_MIRROR, kMixedCg, b, o, x);
 }
 
 }  // extern "C"

@@ -503,6 +503,54 @@ static __device__ __noinline__ void run_epilogue(const Red& rd) {
       S[kMxDoRep] = 0.0;
       bl_beta0(S, l, D[0]);
       break;
+    // ---------------- mixed-precision preconditioned CG (no reference
+    // counterpart; the recurrence is src/cg.c:35-54 with z = M r).
+    // E_MCG_RES's a0: 0 = (r, z) comes later (E_MCG_BETA), else it is
+    // D[a0 - 1] of this reduction.
+    case E_MCG_RHO0:         // after r = fl(r64), z = M r: D0 = (r, z)
+      S[kRho] = D[0];
+      break;
+    case E_MCG_ALPHA:        // q = A p: D0 = (p, q)
+      S[kAlpha] = S[kRho] / D[0];
+      break;
+    case E_MCG_RES: {        // after y += alpha p, r -= alpha q: D0 = (r, r)
+      Ctl* c = rd.ctl;
+      const double rec = sqrt(D[0]) / S[kFnb];
+      S[kErr] = rec;
+      if (c->hist && c->hist_len < c->hist_cap) c->hist[c->hist_len] = rec;
+      c->hist_len++;
+      if (!isfinite(rec)) {
+        c->done = 1;
+        c->ret = kDivergence;
+        break;
+      }
+      S[kMxSinceRep] += 1.0;
+      const bool rep = rec <= S[kMxTarget] ||
+                       rec < S[kMxDelta] * S[kMxLastRep] ||
+                       S[kMxSinceRep] >= S[kMxPeriod];
+      if (c->use_cond)   // a1: which of the body's conditional nodes
+        cudaGraphSetConditional(
+            (cudaGraphConditionalHandle)(rd.a1 ? c->cond_alt : c->cond), rep ? 1u : 0u);
+      S[kMxDoRep] = rep ? 1.0 : 0.0;
+      if (!rep) {
+        if (rd.a0) {   // (r, z) in D[a0 - 1] (z = r: D0; fused M r: D1)
+          const double rz = D[rd.a0 - 1];
+          S[kBeta] = rz / S[kRho];
+          S[kRho] = rz;
+        }
+        c->iter++;
+        if (c->iter >= c->max_iter) {
+          c->done = 1;
+          c->ret = kNotConverged;
+        }
+      }
+      break;
+    }
+    case E_MCG_BETA:         // z = M r (or the replaced r): D0 = (r, z)
+      S[kMxDoRep] = 0.0;
+      S[kBeta] = D[0] / S[kRho];
+      S[kRho] = D[0];
+      break;
     // ---------------- shifted BiCG, src/shbicg.c
     case E_SHB_INIT: {       // :27-46; then rho / beta of iteration 0 (:52-53)
       const int ns = (int)S[kNs];

@@ -170,6 +170,97 @@ k_spmv_dia(CsrH A, SpmvH<XT> io, Red rd) {
   if (ND > 0 || rd.epi) finish_reduction<ND>(acc, rd);
 }
 
+// Diagonal-form product with fused neighbouring updates (kernel_api.h:
+// SpmvFuseH).  Same row order and rounding as k_spmv_dia for the product;
+// the gathered input x_j = ca xa_j + cb xb_j is formed per element, exactly
+// as the row that owns j forms (and stores) it.
+template <typename T, int ND>
+__global__ void __launch_bounds__(kThreads, 4)
+k_spmv_dia_fused(CsrH A, SpmvFuseH<T> f, Red rd) {
+  constexpr int R = 4;
+  if (skip(rd)) return;
+  const T* __restrict__ V = static_cast<const T*>(A.dia.val);
+  const long long stride = A.dia.stride;
+  const int nd = A.dia.nd, n = A.n;
+  const T ca = (T)eval_cf(f.ca, rd.S), cb = f.xb ? (T)eval_cf(f.cb, rd.S) : T(0);
+  const T c0 = f.fo ? (T)eval_cf(f.c0, rd.S) : T(0);
+  const T c1 = (f.fo && f.f1) ? (T)eval_cf(f.c1, rd.S) : T(0);
+  const bool hb = f.xb != nullptr;
+  double acc[ND > 0 ? ND : 1];
+#pragma unroll
+  for (int d = 0; d < ND; ++d) acc[d] = 0.0;
+  const int ngroups = (n + R - 1) / R;
+  for (int g = blockIdx.x * kThreads + threadIdx.x; g < ngroups;
+       g += gridDim.x * kThreads) {
+    const int i0 = g * R;
+    const unsigned m = load_mask<R>(A.dia.mask, i0);
+    T sum[R];
+#pragma unroll
+    for (int e = 0; e < R; ++e) sum[e] = T(0);
+#pragma unroll
+    for (int d = 0; d < kDiaMax; ++d) {
+      if (d < nd) {
+        T v[R];
+        load_rows<T>(V + d * stride, i0, v);
+        const int o = A.dia.off[d];
+        T xa[R], xb[R];
+        load_x<T>(f.xa, i0 + o, o, n, xa);
+        if (hb) load_x<T>(f.xb, i0 + o, o, n, xb);
+#pragma unroll
+        for (int e = 0; e < R; ++e) {
+          const T xv = hb ? fma_rn(cb, xb[e], mul_rn(ca, xa[e])) : mul_rn(ca, xa[e]);
+          if ((m >> (8 * e + d)) & 1u) sum[e] = add_rn(sum[e], mul_rn(v[e], xv));
+        }
+      }
+    }
+    // The row's own x, product and second update.
+    T xo[R], xa[R], xb[R], fv[R];
+    load_opnd<T>(f.xa, i0, n, xa);
+    if (hb) load_opnd<T>(f.xb, i0, n, xb);
+#pragma unroll
+    for (int e = 0; e < R; ++e)
+      xo[e] = hb ? fma_rn(cb, xb[e], mul_rn(ca, xa[e])) : mul_rn(ca, xa[e]);
+    if (f.fo) {
+      T a0[R], a1[R];
+      load_opnd<T>(f.f0, i0, n, a0);
+      if (f.f1) load_opnd<T>(f.f1, i0, n, a1);
+#pragma unroll
+      for (int e = 0; e < R; ++e)
+        fv[e] = f.f1 ? fma_rn(c1, a1[e], mul_rn(c0, a0[e])) : mul_rn(c0, a0[e]);
+    } else {
+#pragma unroll
+      for (int e = 0; e < R; ++e) fv[e] = T(0);
+    }
+    if (i0 + R <= n) {
+      store_rows<T>(f.y, i0, sum);
+      if (f.xe) store_rows<T>(f.xe, i0, xo);
+      if (f.fo) store_rows<T>(f.fo, i0, fv);
+    } else {
+#pragma unroll
+      for (int e = 0; e < R; ++e)
+        if (i0 + e < n) {
+          f.y[i0 + e] = sum[e];
+          if (f.xe) f.xe[i0 + e] = xo[e];
+          if (f.fo) f.fo[i0 + e] = fv[e];
+        }
+    }
+    if (ND > 0) {
+#pragma unroll
+      for (int e = 0; e < R; ++e)
+        if (i0 + e < n) {
+#pragma unroll
+          for (int d = 0; d < ND; ++d) {
+            const int a = f.dot[d][0], b = f.dot[d][1];
+            const T u = a == 0 ? sum[e] : a == 1 ? xo[e] : fv[e];
+            const T w = b == 0 ? sum[e] : b == 1 ? xo[e] : fv[e];
+            acc[d] += (double)u * (double)w;
+          }
+        }
+    }
+  }
+  if (ND > 0 || rd.epi) finish_reduction<ND>(acc, rd);
+}
+
 // Fill the diagonal form from CSR values (and, when mask is given, the row
 // masks): one thread per row; a row's columns ascend, so its diagonal index
 // only moves forward.

@@ -47,6 +47,9 @@ struct CtlH {
   unsigned long long cond;
   int use_cond;
   int cond_pad;
+  // A second conditional node in the same body (a body that holds two
+  // iterations); the deciding epilogue picks one by its a1.
+  unsigned long long cond_alt;
 };
 
 struct RedH {
@@ -123,6 +126,38 @@ struct SpmvH {
   int nd;
   unsigned char dot[kMaxDotsApi][2];   // 0 = y, 1 = b, 2 = w0, 3 = w1
 };
+
+// Diagonal-form product with its neighbouring vector updates fused in
+// (k_spmv_dia_fused): the input is formed on the fly,
+//   x = ca xa + cb xb          (xb null: x = ca xa)
+// for every element the rows read, so the update of x needs no pass of its
+// own; each row's own x is stored to xe, the product to y, and a second
+// own-row update fo = c0 f0 + c1 f1 rides along.  Both combinations round as
+// a linear-combination launch would (first term a product, then an FMA), so
+// a row's stored x equals the value its neighbours used.  Up to three dots
+// of the row values: operand 0 = y, 1 = x, 2 = fo.
+template <typename T>
+struct SpmvFuseH {
+  const T* xa;
+  const T* xb;
+  CfH ca, cb;
+  T* xe;
+  T* y;
+  const T* f0;
+  const T* f1;
+  T* fo;
+  CfH c0, c1;
+  int nd;
+  unsigned char dot[3][2];
+};
+// A must have a diagonal form and every vector must be 16-byte aligned
+// (else CudaError through the caller's check: spmv_fused_usable).
+bool spmv_fused_usable_d(const CsrH& A, const SpmvFuseH<double>& f);
+bool spmv_fused_usable_f(const CsrH& A, const SpmvFuseH<float>& f);
+void launch_spmv_fused_d(const CsrH& A, const SpmvFuseH<double>& f,
+                         const RedH& rd, cudaStream_t st);
+void launch_spmv_fused_f(const CsrH& A, const SpmvFuseH<float>& f,
+                         const RedH& rd, cudaStream_t st);
 
 // Programmatic dependent launch is kept off for the kernels of a
 // conditional node's body and for the first launch after such a node (a

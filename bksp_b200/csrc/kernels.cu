@@ -259,6 +259,7 @@ __global__ void k_ctl_init(Ctl* c, unsigned* ticket, double* S, int iter0,
   c->tol = tol;
   c->hist = hist;
   c->cond = 0ull;
+  c->cond_alt = 0ull;
   c->use_cond = 0;
   ticket[0] = 0u;
   if (slot >= 0) S[slot] = value;

@@ -211,6 +211,51 @@ void launch_spmv_f(const CsrH& A, const SpmvH<float>& io, const RedH& rd,
   spmv_dispatch<float, float>(A, io, rd, st);
 }
 
+// ------------------------------------------------- fused diagonal product
+
+template <typename T>
+static bool fused_usable(const CsrH& A, const SpmvFuseH<T>& f) {
+  return A.dia.nd > 0 && f.nd <= 3 && aligned16(f.xa) && aligned16(f.xb) &&
+         aligned16(f.xe) && aligned16(f.y) && aligned16(f.f0) &&
+         aligned16(f.f1) && aligned16(f.fo) && f.xa && f.y;
+}
+bool spmv_fused_usable_d(const CsrH& A, const SpmvFuseH<double>& f) {
+  return fused_usable(A, f);
+}
+bool spmv_fused_usable_f(const CsrH& A, const SpmvFuseH<float>& f) {
+  return fused_usable(A, f);
+}
+
+template <typename T>
+static void spmv_fused_launch(const CsrH& A, const SpmvFuseH<T>& f, const RedH& rd,
+                              cudaStream_t st) {
+  if (g_prog_rec) prog_unsupported("fused product");
+  ++launch_count();
+  const long long n = A.n;
+  // Diagonal values and masks, the input vectors, the product, the stored
+  // own x and the second update's operands, each once.
+  const int vecs = 2 + (f.xb != nullptr) + (f.xe != nullptr) +
+                   (f.fo != nullptr) * (1 + (f.f0 != nullptr) + (f.f1 != nullptr));
+  byte_count() += n * ((long long)A.dia.nd * (long long)sizeof(T) + 1) +
+                  vecs * n * (long long)sizeof(T);
+  const long long groups = (n + 3) / 4;
+  switch (f.nd) {
+    case 0: launch_k(k_spmv_dia_fused<T, 0>, grid_wave(k_spmv_dia_fused<T, 0>, groups), kThreads, 0, st, A, f, rd); break;
+    case 1: launch_k(k_spmv_dia_fused<T, 1>, grid_wave(k_spmv_dia_fused<T, 1>, groups), kThreads, 0, st, A, f, rd); break;
+    case 2: launch_k(k_spmv_dia_fused<T, 2>, grid_wave(k_spmv_dia_fused<T, 2>, groups), kThreads, 0, st, A, f, rd); break;
+    default: launch_k(k_spmv_dia_fused<T, 3>, grid_wave(k_spmv_dia_fused<T, 3>, groups), kThreads, 0, st, A, f, rd); break;
+  }
+}
+
+void launch_spmv_fused_d(const CsrH& A, const SpmvFuseH<double>& f,
+                         const RedH& rd, cudaStream_t st) {
+  spmv_fused_launch<double>(A, f, rd, st);
+}
+void launch_spmv_fused_f(const CsrH& A, const SpmvFuseH<float>& f,
+                         const RedH& rd, cudaStream_t st) {
+  spmv_fused_launch<float>(A, f, rd, st);
+}
+
 // CSR values, columns and row pointers read; nd diagonals (and masks) written.
 template <typename T>
 static long long csr2dia_bytes(const CsrH& A, bool mask) {

@@ -1,6 +1,7 @@
 #include "runtime.h"
 
 #include <algorithm>
+#include <cstddef>
 #include <climits>
 #include <cstdio>
 #include <cstdlib>
@@ -418,13 +419,14 @@ void cond_block(SolveState& ss, cudaStream_t st,
   }
   g_plain_scope = false;
   g_plain_launches = 1;   // the kernel after the node follows it plainly
-  ss.cond_kernels = launch_count() - c0;
-  ss.cond_bytes = byte_count() - y0;
+  ss.cond_kernels += launch_count() - c0;
+  ss.cond_bytes += byte_count() - y0;
   cudaGraph_t captured = nullptr;
   BK_CHECK(cudaStreamEndCapture(ss.side, &captured));
   BK_CHECK(cudaStreamUpdateCaptureDependencies(st, &node, 1,
                                                cudaStreamSetCaptureDependencies));
-  ss.cond_handle = (unsigned long long)h;
+  if (ss.n_cond >= 2) throw CudaError("more than two conditional nodes in a body");
+  ss.cond_handle[ss.n_cond++] = (unsigned long long)h;
   ss.has_cond = true;
 }
 
@@ -537,6 +539,7 @@ static bool run_graph_while(SolveState& ss,
       break;
     const long long c0 = launch_count(), y0 = byte_count();
     ss.has_cond = false;
+    ss.n_cond = 0;
     ss.cond_kernels = 0;
     ss.cond_bytes = 0;
     bool body_ok = true;
@@ -569,7 +572,9 @@ static bool run_graph_while(SolveState& ss,
   if (ok) {
     if (ss.has_cond) {
       // Hand the conditional node's handle to the device epilogues.
-      struct { unsigned long long cond; int use; int pad; } cc{ss.cond_handle, 1, 0};
+      struct { unsigned long long cond; int use; int pad; unsigned long long alt; } cc{
+          ss.cond_handle[0], 1, 0, ss.cond_handle[1]};
+      static_assert(sizeof(cc) == sizeof(CtlH) - offsetof(CtlH, cond), "control block tail");
       BK_CHECK(cudaMemcpyAsync(&ss.ctl->cond, &cc, sizeof(cc), cudaMemcpyHostToDevice, st));
     }
     BK_CHECK(cudaGraphLaunch(ex, st));

@@ -128,8 +128,9 @@ struct SolveState {
   // Conditional block of the captured iteration (cond_block): its handle
   // and the kernels it holds, valid for the solve being captured.
   bool has_cond = false;
-  unsigned long long cond_handle = 0;
-  long long cond_kernels = 0;
+  int n_cond = 0;                       // conditional nodes in the body
+  unsigned long long cond_handle[2] = {0, 0};
+  long long cond_kernels = 0;           // kernels of all of them
   long long cond_bytes = 0;   // their algorithmic bytes (byte_count)
   cudaStream_t side = nullptr;   // capture stream of the conditional body
   void create(int hist_cap, cudaStream_t st);
@@ -156,9 +157,10 @@ struct SolveState {
 
 // Inside the body that run_loop captures: launch `inner`'s kernels in a
 // conditional IF node, so they run only in the iterations in which an
-// epilogue upstream sets the node's condition (through ctl->cond); in the
-// others no kernel is launched at all.  Outside a capture (host-polled
-// loop) inner runs directly and its kernels' own guards decide.
+// epilogue upstream sets the node's condition (through ctl->cond for the
+// body's first node, ctl->cond_alt for a second); in the others no kernel
+// is launched at all.  Outside a capture (host-polled loop) inner runs
+// directly and its kernels' own guards decide.
 void cond_block(SolveState& ss, cudaStream_t st,
                 const std::function<void(cudaStream_t)>& inner);
 

@@ -120,6 +120,8 @@ enum : short {
   E_BLF_MR,         // one-pass minimal-residual step from the Gram matrix
   // mixed-precision BiCGSTAB(l)
   E_MX_INIT, E_MX_INIT2, E_MX_CHECK, E_MX_TRUE, E_MX_REBETA,
+  // mixed-precision preconditioned CG
+  E_MCG_RHO0, E_MCG_ALPHA, E_MCG_RES, E_MCG_BETA,
   // shifted BiCG (src/shbicg.c)
   E_SHB_INIT, E_SHB_ALPHA, E_SHB_CHECK,
   // shifted BiCGSTAB(l) (src/shbicgstabl.c)

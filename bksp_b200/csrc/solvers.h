@@ -54,5 +54,11 @@ struct MixedOut : SolveOut {
 MixedOut bicgstabl_mixed(const DevCsr& A, const DevCsr* M, const double* b,
                          int l, double* x, int max_iter, const MixedOpts& o,
                          SolveState& ss, cudaStream_t st);
+// Mixed-precision preconditioned CG (A symmetric positive definite, M
+// symmetric; nullptr: none) with the same precision split and reliable
+// replacement; stops on the FP64 true relative residual.
+MixedOut cg_mixed(const DevCsr& A, const DevCsr* M, const double* b, double* x,
+                  int max_iter, const MixedOpts& o, SolveState& ss,
+                  cudaStream_t st);
 
 }  // namespace bk

@@ -12,6 +12,7 @@
 //     captured iteration, behind a device-side guard;
 //   * convergence is decided on that FP64 true residual only.
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 
 #include "solvers.h"
@@ -229,6 +230,251 @@ MixedOut bicgstabl_mixed(const DevCsr& A, const DevCsr* M, const double* b,
   out.replacements = (int)ss.get_scalar(kMxReps, st);
   // The conditional node's kernels ran only in the iterations with a
   // replacement (run_loop counted them in every trip).
+  if (ss.has_cond) {
+    const long long idle = std::max(0, c.trips - out.replacements);
+    launch_count() -= ss.cond_kernels * idle;
+    byte_count() -= ss.cond_bytes * idle;
+  }
+  ss.has_cond = false;
+  out.true_res = ss.get_scalar(kMxTrue, st);
+  dfree(w, st);
+  dfree(r64, st);
+  return out;
+}
+
+MixedOut cg_mixed_fused(const DevCsr& A, const DevCsr* M, const double* b,
+                        double* x, int max_iter, const MixedOpts& o,
+                        SolveState& ss, cudaStream_t st) {
+  MixedOut out;
+  const long long np = pad64(A.n);
+  float* w = zeros<float>(7 * np, st);
+  float* R[2] = {w, w + np};
+  float* P[2] = {w + 2 * np, w + 3 * np};
+  float *z = w + 4 * np, *q = w + 5 * np, *y = w + 6 * np;
+  double* r64 = zeros<double>(np, st);
+
+  ss.start(0, max_iter, 0.0, st);
+  ss.set_scalar(kMxTarget, o.target, st);
+  ss.set_scalar(kMxDelta, o.delta, st);
+  ss.set_scalar(kMxPeriod, (double)std::max(1, o.period), st);
+  ss.set_scalar(kBeta, 0.0, st);   // first p = z + 0 * 0
+  {
+    SpmvH<double> io = spmv_io<double>(x, r64);
+    io.b = b;
+    io.mode = 1;
+    set_dot(io, 0, Y, Y);
+    set_dot(io, 1, B, B);
+    spmv(A, io, ss.red(kD, E_MX_INIT), st);
+  }
+  // r = fl32(r64); z = M r and rho = (r, z) (z = r without M).
+  auto restart = [&](float* r, const RedH& conv, const RedH& beta, cudaStream_t s) {
+    if (M) {
+      launch_mx_d2f(r64, r, nullptr, nullptr, nullptr, 0, np, conv, s);
+      SpmvH<float> io = spmv_io<float>(r, z);
+      io.w0 = r;
+      set_dot(io, 0, W0, Y);
+      spmv(*M, io, beta, s);
+    } else {
+      launch_mx_d2f(r64, r, nullptr, nullptr, nullptr, 1, np, beta, s);
+    }
+  };
+  restart(R[0], ss.red(kD, E_NONE), ss.red(kD, E_MCG_RHO0), st);
+
+  auto half = [&](int h, cudaStream_t s) {
+    float *pa = P[h], *pb = P[1 - h], *ra = R[h], *rb = R[1 - h];
+    {  // p = z + beta p_old (stored to pb), q = A p, alpha = rho / (p, q)
+      SpmvFuseH<float> f;
+      std::memset(&f, 0, sizeof(f));
+      f.xa = M ? z : ra;
+      f.ca = cf_const(1);
+      f.xb = pa;
+      f.cb = cf_slot(kBeta);
+      f.xe = pb;
+      f.y = q;
+      f.nd = 1;
+      f.dot[0][0] = 1;
+      f.dot[0][1] = 0;
+      launch_spmv_fused_f(A.h32(), f, ss.red(kD, E_MCG_ALPHA), s);
+    }
+    if (M) {  // r = r_old - alpha q (stored to rb), z = M r, y += alpha p
+      SpmvFuseH<float> f;
+      std::memset(&f, 0, sizeof(f));
+      f.xa = ra;
+      f.ca = cf_const(1);
+      f.xb = q;
+      f.cb = cf_slot(kAlpha, -1);
+      f.xe = rb;
+      f.y = z;
+      f.f0 = y;
+      f.c0 = cf_const(1);
+      f.f1 = pb;
+      f.c1 = cf_slot(kAlpha);
+      f.fo = y;
+      f.nd = 2;
+      f.dot[0][0] = 1; f.dot[0][1] = 1;   // (r, r)
+      f.dot[1][0] = 1; f.dot[1][1] = 0;   // (r, z)
+      launch_spmv_fused_f(M->h32(), f, ss.red(kD, E_MCG_RES, 2, (short)h), s);
+    } else {
+      Lc<float> u(np);
+      const int iy = u.in(y), ip = u.in(pb), ir = u.in(ra), iq = u.in(q);
+      const int oy = u.out(y), orr = u.out(rb);
+      u.term(oy, iy, cf_const(1)).term(oy, ip, cf_slot(kAlpha));
+      u.term(orr, ir, cf_const(1)).term(orr, iq, cf_slot(kAlpha, -1));
+      u.dot(OUT + orr, OUT + orr);
+      u.launch(ss.red(kD, E_MCG_RES, 1, (short)h), s);
+    }
+    cond_block(ss, s, [&](cudaStream_t s2) {   // the h-th node of the body
+      launch_mx_accum(x, y, y, np, ss.red_if(kMxDoRep, kD, E_NONE), s2);
+      SpmvH<double> io = spmv_io<double>(x, r64);
+      io.b = b;
+      io.mode = 1;
+      set_dot(io, 0, Y, Y);
+      spmv(A, io, ss.red_if(kMxDoRep, kD, E_MX_TRUE), s2);
+      restart(rb, ss.red_if(kMxDoRep, kD, E_NONE),
+              ss.red_if(kMxDoRep, kD, E_MCG_BETA), s2);
+    });
+  };
+  auto body = [&](cudaStream_t s) {
+    half(0, s);
+    half(1, s);
+  };
+  const CtlH c = run_loop(ss, body, st);
+  launch_mx_accum(x, y, y, np, ss.red_after(kD, E_NONE), st);
+  BK_CHECK(cudaGetLastError());
+  out.ret = c.ret;
+  out.iters = c.hist_len;
+  out.replacements = (int)ss.get_scalar(kMxReps, st);
+  if (ss.has_cond) {
+    // two conditional nodes per body: the idle ones launched nothing
+    const long long idle = std::max(0, 2 * c.trips - out.replacements);
+    launch_count() -= ss.cond_kernels / 2 * idle;
+    byte_count() -= ss.cond_bytes / 2 * idle;
+  }
+  ss.has_cond = false;
+  out.true_res = ss.get_scalar(kMxTrue, st);
+  dfree(w, st);
+  dfree(r64, st);
+  return out;
+}
+
+// Mixed-precision preconditioned CG with reliable updates (no reference
+// counterpart; the recurrence is src/cg.c:35-54 with a symmetric
+// preconditioner z = M r): FP32 values of A and M and FP32 vectors r, z, p,
+// q = A p and the correction y (solution space), FP64 dots, scalars and
+// solution.  Every replacement folds y into the FP64 x, recomputes the
+// FP64 true residual b - A x with the FP64 operator and restarts r from it
+// (p kept); convergence is decided on that true residual.
+namespace {
+
+// The same method with each iteration in two launches, for operators (and
+// preconditioners) in diagonal form: the product q = A p forms p = z + beta
+// p_old on the fly (and stores it), the preconditioner product z = M r
+// forms r = r_old - alpha q on the fly (storing it) and carries y += alpha
+// p along; p and r alternate between two buffers, two iterations per loop
+// body.
+bool cg_fusable(const DevCsr& A, const DevCsr* M) {
+  static const bool off = [] {
+    const char* e = std::getenv("BKSP_GPU_FUSE");
+    return e && std::strcmp(e, "0") == 0;
+  }();
+  return !off && A.ndia > 0 && A.d32 &&
+         (!M || (M->ndia > 0 && M->d32));
+}
+
+}  // namespace
+
+MixedOut cg_mixed(const DevCsr& A, const DevCsr* M, const double* b, double* x,
+                  int max_iter, const MixedOpts& o, SolveState& ss,
+                  cudaStream_t st) {
+  if (!A.v32 || (M && !M->v32)) throw CudaError("mixed solve: FP32 values missing");
+  if (cg_fusable(A, M)) return cg_mixed_fused(A, M, b, x, max_iter, o, ss, st);
+  MixedOut out;
+  const long long np = pad64(A.n);
+  float* w = zeros<float>(5 * np, st);
+  float *r = w, *z = w + np, *p = w + 2 * np, *q = w + 3 * np, *y = w + 4 * np;
+  double* r64 = zeros<double>(np, st);
+  const short unprec = M ? 0 : 1;
+
+  ss.start(0, max_iter, 0.0, st);
+  ss.set_scalar(kMxTarget, o.target, st);
+  ss.set_scalar(kMxDelta, o.delta, st);
+  ss.set_scalar(kMxPeriod, (double)std::max(1, o.period), st);
+
+  // r64 = b - A x0 (FP64), ||b||, true residual; r = fl32(r64); z = M r,
+  // p = z, rho = (r, z).
+  {
+    SpmvH<double> io = spmv_io<double>(x, r64);
+    io.b = b;
+    io.mode = 1;
+    set_dot(io, 0, Y, Y);
+    set_dot(io, 1, B, B);
+    spmv(A, io, ss.red(kD, E_MX_INIT), st);
+  }
+  auto precondition = [&](const RedH& rd, cudaStream_t s) {
+    // z = M r, p-independent; (r, z) into the epilogue of rd
+    SpmvH<float> io = spmv_io<float>(r, z);
+    io.w0 = r;
+    set_dot(io, 0, W0, Y);
+    spmv(*M, io, rd, s);
+  };
+  if (M) {
+    launch_mx_d2f(r64, r, nullptr, nullptr, nullptr, 0, np, ss.red(kD, E_NONE), st);
+    SpmvH<float> io = spmv_io<float>(r, z);
+    io.y2 = p;
+    io.w0 = r;
+    set_dot(io, 0, W0, Y);
+    spmv(*M, io, ss.red(kD, E_MCG_RHO0), st);
+  } else {
+    launch_mx_d2f(r64, r, p, nullptr, nullptr, 1, np, ss.red(kD, E_MCG_RHO0), st);
+  }
+
+  auto body = [&](cudaStream_t s) {
+    {  // q = A p, alpha = rho / (p, q)
+      SpmvH<float> io = spmv_io<float>(p, q);
+      io.w0 = p;
+      set_dot(io, 0, W0, Y);
+      spmv(A, io, ss.red(kD, E_MCG_ALPHA), s);
+    }
+    {  // y += alpha p, r -= alpha q, (r, r): replacement decision
+      Lc<float> u(np);
+      const int iy = u.in(y), ip = u.in(p), ir = u.in(r), iq = u.in(q);
+      const int oy = u.out(y), orr = u.out(r);
+      u.term(oy, iy, cf_const(1)).term(oy, ip, cf_slot(kAlpha));
+      u.term(orr, ir, cf_const(1)).term(orr, iq, cf_slot(kAlpha, -1));
+      u.dot(OUT + orr, OUT + orr);
+      u.launch(ss.red(kD, E_MCG_RES, unprec), s);
+    }
+    cond_block(ss, s, [&](cudaStream_t s2) {
+      // x += y (FP64), y = 0; r64 = b - A x; r = fl32(r64)
+      launch_mx_accum(x, y, y, np, ss.red_if(kMxDoRep, kD, E_NONE), s2);
+      SpmvH<double> io = spmv_io<double>(x, r64);
+      io.b = b;
+      io.mode = 1;
+      set_dot(io, 0, Y, Y);
+      spmv(A, io, ss.red_if(kMxDoRep, kD, E_MX_TRUE), s2);
+      if (M)
+        launch_mx_d2f(r64, r, nullptr, nullptr, nullptr, 0, np,
+                      ss.red_if(kMxDoRep, kD, E_NONE), s2);
+      else
+        launch_mx_d2f(r64, r, nullptr, nullptr, nullptr, 1, np,
+                      ss.red_if(kMxDoRep, kD, E_MCG_BETA), s2);
+    });
+    if (M) precondition(ss.red(kD, E_MCG_BETA), s);
+    {  // p = z + beta p
+      Lc<float> u(np);
+      const int iz = u.in(M ? z : r), ip = u.in(p);
+      const int op_ = u.out(p);
+      u.term(op_, iz, cf_const(1)).term(op_, ip, cf_slot(kBeta));
+      u.launch(ss.red(kD, E_NONE), s);
+    }
+  };
+  const CtlH c = run_loop(ss, body, st);
+  // Fold the correction not yet accumulated.
+  launch_mx_accum(x, y, y, np, ss.red_after(kD, E_NONE), st);
+  BK_CHECK(cudaGetLastError());
+  out.ret = c.ret;
+  out.iters = c.hist_len;
+  out.replacements = (int)ss.get_scalar(kMxReps, st);
   if (ss.has_cond) {
     const long long idle = std::max(0, c.trips - out.replacements);
     launch_count() -= ss.cond_kernels * idle;

@@ -67,19 +67,29 @@ static void ensure_features(bksp_gpu_matrix* m, cudaStream_t st) {
   BK_CHECK(cudaGetLastError());
 }
 
-long long spai_scratch_floats(const bksp_gpu_matrix* m) {
-  return pad64((long long)m->A.nnz + 8) + (long long)m->A.ndia * pad64(m->A.n);
+long long spai_scratch_floats(const bksp_gpu_matrix* m, bool symmetric) {
+  const long long csr = pad64((long long)m->A.nnz + 8);
+  return csr + (long long)m->A.ndia * pad64(m->A.n) + (symmetric ? csr : 0);
 }
 
 DevCsr spai_apply(bksp_gpu_spai_model* model, bksp_gpu_matrix* m, float* mvals,
-                  cudaStream_t st) {
+                  cudaStream_t st, bool symmetric) {
   ensure_features(m, st);
   const int n = m->A.n;
-  BK_CHECK(cudaMemsetAsync(mvals, 0, sizeof(float) * ((size_t)m->A.nnz + 8), st));
+  const long long csr = pad64((long long)m->A.nnz + 8);
+  float* pred = symmetric
+                    ? mvals + csr + (long long)m->A.ndia * pad64(n)
+                    : mvals;
+  BK_CHECK(cudaMemsetAsync(pred, 0, sizeof(float) * ((size_t)m->A.nnz + 8), st));
   launch_spai_infer(n, model->w, m->spai.feat, m->spai.dinv, m->spai.slot_entry,
-                    mvals, st);
+                    pred, st);
   // features, slot map and 1/a_ii read per row; M's values written
   byte_count() += (long long)n * (8LL * kSlots + 4) + 4LL * m->A.nnz;
+  if (symmetric) {
+    BK_CHECK(cudaMemsetAsync(mvals, 0, sizeof(float) * ((size_t)m->A.nnz + 8), st));
+    launch_spai_symmetrize(n, m->A.rowptr, m->A.col, pred, mvals, st);
+    byte_count() += 4LL * (n + 1) + 12LL * m->A.nnz;
+  }
   BK_CHECK(cudaGetLastError());
   DevCsr v;
   v.n = n;

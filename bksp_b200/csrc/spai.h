@@ -36,12 +36,14 @@ struct SpaiSlots {
 // s.ok false when the operator is not stencil-like.
 void spai_build_slots(const DevCsr& A, SpaiSlots& s, cudaStream_t st);
 // Scratch floats spai_apply needs: M's CSR values (nnz + 8, padded to 64)
-// then, when A has a diagonal form, M's diagonal form.
-long long spai_scratch_floats(const bksp_gpu_matrix* m);
+// then, when A has a diagonal form, M's diagonal form, then (symmetric)
+// the predicted values before symmetrisation.
+long long spai_scratch_floats(const bksp_gpu_matrix* m, bool symmetric = false);
 // M (FP32 values in mvals, spai_scratch_floats floats) on A's pattern from
 // the model; returns a view sharing A's index arrays and row masks (never
-// released).
+// released).  symmetric: M = (M_pred + M_pred^T) / 2, for CG, whose
+// preconditioner must be symmetric.
 DevCsr spai_apply(bksp_gpu_spai_model* model, bksp_gpu_matrix* m,
-                  float* mvals, cudaStream_t st);
+                  float* mvals, cudaStream_t st, bool symmetric = false);
 
 }  // namespace bk

@@ -23,6 +23,9 @@ void launch_spai_slot_map(int n, const int* rowptr, const int* col,
 void launch_spai_features(int n, const int* rowptr, const double* val,
                           const int* slot_entry, float* feat, float* dinv,
                           cudaStream_t st);
+// out = (M + M^T) / 2 on M's (symmetric) pattern, CSR values in and out.
+void launch_spai_symmetrize(int n, const int* rowptr, const int* col,
+                            const float* in, float* out, cudaStream_t st);
 void launch_spai_infer(int n, const float* w, const float* feat,
                        const float* dinv, const int* slot_entry, float* mval,
                        cudaStream_t st);

@@ -377,6 +377,36 @@ k_spai_slot_map(int n, const int* __restrict__ rowptr, const int* __restrict__ c
   for (int s = 0; s < kSlots; ++s) slot_entry[(long long)i * kSlots + s] = e[s];
 }
 
+// out = (M + M^T) / 2 on M's pattern, which is A's pattern and symmetric
+// for the symmetric operators this serves (CG): entry (i, j) averages with
+// the first stored (j, i); an entry without a transposed partner keeps its
+// own value.  One thread per row.
+__global__ void __launch_bounds__(256)
+k_spai_symmetrize(int n, const int* __restrict__ rowptr, const int* __restrict__ col,
+                  const float* __restrict__ in, float* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (int k = rowptr[i]; k < rowptr[i + 1]; ++k) {
+    const int j = col[k];
+    float v = in[k];
+    if (j != i && j >= 0 && j < n) {
+      for (int kk = rowptr[j]; kk < rowptr[j + 1]; ++kk) {
+        if (col[kk] == i) {
+          v = (float)(0.5 * ((double)in[k] + (double)in[kk]));
+          break;
+        }
+      }
+    }
+    out[k] = v;
+  }
+}
+
+void launch_spai_symmetrize(int n, const int* rowptr, const int* col,
+                            const float* in, float* out, cudaStream_t st) {
+  ++launch_count();
+  k_spai_symmetrize<<<(n + 255) / 256, 256, 0, st>>>(n, rowptr, col, in, out);
+}
+
 void launch_spai_slot_map(int n, const int* rowptr, const int* col,
                           const int* so, const int* sl, int ns, int* slot_entry,
                           cudaStream_t st) {

@@ -201,6 +201,24 @@ int bksp_gpu_solve_mixed(bksp_gpu_matrix *A, const double *b, double *x,
 int bksp_dbicgstabl_mixed(dspmat *A, double *b, const bksp_gpu_mixed_opts *opts,
                           double *x);
 
+/* Preconditioned CG in mixed precision, the same split as
+ * bksp_gpu_solve_mixed: FP32 values of A and M and FP32 vectors (r, z = M r,
+ * p, A p, the correction), FP64 dot products, scalars and solution, FP64
+ * reliable replacement of r by b - A x, stopping on the FP64 true relative
+ * residual.  A symmetric positive definite, full storage (BKSP_GPU_MIRROR
+ * for one triangle) with BKSP_GPU_FP32.  The preconditioner is symmetric:
+ * Jacobi, or the learned one symmetrised, (M + M^T) / 2.  opts->l is not
+ * used.  Returns the index of the converging iteration, NOT_CONVERGED,
+ * DIVERGENCE or INVALID_PARAMETERS. */
+int bksp_gpu_cg_mixed(bksp_gpu_matrix *A, const double *b, double *x,
+                      const bksp_gpu_mixed_opts *opts, void *stream,
+                      bksp_gpu_stats *stats);
+
+/* The same with host arrays, taking bksp_dcg's matrix: type "symmetric",
+ * one triangle stored (INVALID_MATRIX_TYPE otherwise). */
+int bksp_dcg_mixed(dspmat *A, double *b, const bksp_gpu_mixed_opts *opts,
+                   double *x);
+
 /* ------------------------------------------------------------ batches */
 
 /* Many independent systems in one call, each solved as bksp_gpu_solve_mixed

