@@ -112,6 +112,8 @@ def _load():
     L.bksp_gpu_cg_mixed.argtypes = [vp, vp, vp, C.POINTER(MixedOpts), vp,
                                     C.POINTER(Stats)]
     L.bksp_dcg_mixed.argtypes = [sp, _dp, C.POINTER(MixedOpts), _dp]
+    L.bksp_dblcg_mixed.argtypes = [sp, mp, C.POINTER(MixedOpts), mp]
+    L.bksp_dblbicgstabl_mixed.argtypes = [sp, mp, C.POINTER(MixedOpts), mp]
     L.bksp_gpu_solve_mixed_batch.argtypes = [C.POINTER(vp), C.POINTER(vp),
                                              C.POINTER(vp), i,
                                              C.POINTER(MixedOpts), i,
@@ -509,6 +511,20 @@ def dcg_mixed(A, b, x, target=1e-8, max_iter=10000, precond=0, model=None,
                   model.h if model is not None else None, 0.0, 0, fallback)
     return lib.bksp_dcg_mixed(A.ptr, b.ctypes.data_as(_dp), C.byref(o),
                               _inplace(x))
+
+
+def dblcg_mixed(A, B, X, target=1e-8, max_iter=10000, inner_tol=0.0):
+    """bksp_dblcg_mixed: Block CG, FP64 refinement around FP32 inner solves
+    (inner relative residual inner_tol, 0: 1e-4); X (n-by-s) updated in
+    place."""
+    o = MixedOpts(0, target, max_iter, 0, None, inner_tol, 0, 0)
+    return _block(lib.bksp_dblcg_mixed, A, B, (C.byref(o),), X)
+
+
+def dblbicgstabl_mixed(A, B, l, X, target=1e-8, max_iter=10000, inner_tol=0.0):
+    """bksp_dblbicgstabl_mixed: Block BiCGSTAB(l), as dblcg_mixed."""
+    o = MixedOpts(l, target, max_iter, 0, None, inner_tol, 0, 0)
+    return _block(lib.bksp_dblbicgstabl_mixed, A, B, (C.byref(o),), X)
 
 
 def _batch_args(mats, bs, xs):

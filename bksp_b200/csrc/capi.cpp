@@ -237,10 +237,12 @@ int solve_block(BMethod m, dspmat* A, dmat* B, int l, double tol, int max_iter,
       BlockCtx bc(n, s, ss, st);
       tm.begin_solve();
       switch (m) {
-        case BMethod::CG: o = bk::blcg(bc, dA, dB, dX, tol, max_iter); break;
-        case BMethod::BICGSTAB: o = bk::blbicgstab(bc, dA, dB, dX, tol, max_iter); break;
+        case BMethod::CG: o = bk::blcg<double>(bc, dA, dB, dX, tol, max_iter); break;
+        case BMethod::BICGSTAB:
+          o = bk::blbicgstab<double>(bc, dA, dB, dX, tol, max_iter);
+          break;
         case BMethod::BICGSTABL:
-          o = bk::blbicgstabl(bc, dA, dB, dX, l, tol, max_iter, &true_res);
+          o = bk::blbicgstabl<double>(bc, dA, dB, dX, l, tol, max_iter, &true_res);
           break;
       }
       tm.end_solve();
@@ -278,9 +280,80 @@ int solve_block(BMethod m, dspmat* A, dmat* B, int l, double tol, int max_iter,
   }
 }
 
+// Host arrays in, the mixed-precision block solve, host arrays out.
+int solve_block_mixed(BMethod m, dspmat* A, dmat* B, const bksp_gpu_mixed_opts* o,
+                      dmat* X) {
+  if (check_matrix(A) != 0 || !B || !X || !B->value || !X->value || !o)
+    return INVALID_PARAMETERS;
+  if (m == BMethod::CG && !is_symmetric(A)) return INVALID_MATRIX_TYPE;
+  const int n = *A->row_size, s = B->col_size;
+  if (B->row_size != n || X->row_size != n || X->col_size != s || s < 1 ||
+      s > kBlockMaxS)
+    return INVALID_PARAMETERS;
+  const int l = o->l;
+  if (m == BMethod::BICGSTABL && (l < 1 || l > kBlMaxL)) return INVALID_PARAMETERS;
+  try {
+    Ctx& cx = Ctx::get();
+    cudaStream_t st = cx.st;
+    Timer tm(st);
+    DevCsr dA;
+    upload_operator(A, m == BMethod::CG, true, dA, st);
+    const long long np = pad64(n);
+    double* tmp = dalloc_n<double>((long long)n * s, st);
+    double* dB = dalloc_n<double>(np * s, st);
+    double* dX = dalloc_n<double>(np * s, st);
+    BK_CHECK(cudaMemsetAsync(dB, 0, sizeof(double) * np * s, st));
+    BK_CHECK(cudaMemsetAsync(dX, 0, sizeof(double) * np * s, st));
+    BK_CHECK(cudaMemcpyAsync(tmp, B->value, sizeof(double) * n * s,
+                             cudaMemcpyHostToDevice, st));
+    launch_cm2rm(tmp, dB, n, s, st);
+    BK_CHECK(cudaMemcpyAsync(tmp, X->value, sizeof(double) * n * s,
+                             cudaMemcpyHostToDevice, st));
+    launch_cm2rm(tmp, dX, n, s, st);
+    const int max_iter = o->max_iter > 0 ? o->max_iter : 10000;
+    SolveState ss;
+    ss.create(hist_cap_for(max_iter), st);
+    tm.begin_solve();
+    const BlockMixedOut r = block_mixed(m == BMethod::CG ? 0 : 2, dA, dB, dX, n, s, l,
+                                        o->target > 0 ? o->target : 1e-8, max_iter,
+                                        o->delta > 0 ? o->delta : 1e-4, ss, st);
+    tm.end_solve();
+    launch_rm2cm(dX, tmp, n, s, st);
+    BK_CHECK(cudaMemcpyAsync(X->value, tmp, sizeof(double) * n * s,
+                             cudaMemcpyDeviceToHost, st));
+    BK_CHECK(cudaStreamSynchronize(st));
+    tm.report(r.ret, nullptr, r.inner_iters);
+    if (g_stats) {
+      g_stats->true_res = r.true_res;
+      g_stats->inner_iters = r.inner_iters;
+      g_stats->sweeps = r.sweeps;
+    }
+    ss.release(st);
+    dfree(tmp, st);
+    dfree(dB, st);
+    dfree(dX, st);
+    dA.release(st);
+    BK_CHECK(cudaStreamSynchronize(st));
+    return r.ret;
+  } catch (const std::exception& e) {
+    if (std::getenv("BKSP_GPU_VERBOSE")) std::fprintf(stderr, "bksp: %s\n", e.what());
+    cudaGetLastError();
+    return INVALID_PARAMETERS;
+  }
+}
+
 }  // namespace
 
 extern "C" {
+
+int bksp_dblcg_mixed(dspmat* A, dmat* B, const bksp_gpu_mixed_opts* opts, dmat* X) {
+  return solve_block_mixed(BMethod::CG, A, B, opts, X);
+}
+
+int bksp_dblbicgstabl_mixed(dspmat* A, dmat* B, const bksp_gpu_mixed_opts* opts,
+                            dmat* X) {
+  return solve_block_mixed(BMethod::BICGSTABL, A, B, opts, X);
+}
 
 int dblcg(dspmat* A, dmat* B, double tol, int max_iter, dmat* X) {
   return solve_block(BMethod::CG, A, B, 0, tol, max_iter, X);

@@ -20,40 +20,45 @@ constexpr int kBlkSub = kBlkTileRows / (kThreads / kBlkS);   // rows per thread
 // Y = alpha * A X  (mode 0), Y = C + alpha * A X  (mode 1), with the
 // reference's per-entry rounding (y += (alpha a_k) x_k, no FMA).  Optional
 // Frobenius dots (Y, W) and (Y, Y) into S[out], S[out + 1].
+// T = value and block element type (double: the reference-parity path;
+// float: the inner solves of the mixed-precision block methods, dots still
+// accumulated in FP64).
+template <typename T>
 struct SpmmArgs {
-  const double* X;
-  double* Y;
-  const double* C;
-  const double* W;
+  const T* X;
+  T* Y;
+  const T* C;
+  const T* W;
   double alpha;
-  int mode, s, nd;
+  int mode, s, nd, prec;
 };
 
-template <int ND>
+template <typename T, int ND>
 __global__ void __launch_bounds__(kThreads, 8)
-k_spmm(CsrH A, SpmmArgs a, Red rd) {
+k_spmm(CsrH A, SpmmArgs<T> a, Red rd) {
   if (skip(rd)) return;
-  const double* __restrict__ val = static_cast<const double*>(A.val);
+  const T* __restrict__ val = static_cast<const T*>(A.val);
   const int lane = threadIdx.x & (kBlkS - 1);
   const int grp = (blockIdx.x * kThreads + threadIdx.x) / kBlkS;
   const int ngrp = gridDim.x * kThreads / kBlkS;
   const int s = a.s;
+  const T alpha = (T)a.alpha;
   double acc[ND > 0 ? ND : 1];
 #pragma unroll
   for (int d = 0; d < ND; ++d) acc[d] = 0.0;
   for (int row = grp; row < A.n; row += ngrp) {
     if (lane < s) {
-      double y = 0.0;
+      T y = T(0);
       const int k0 = __ldg(A.rowptr + row), k1 = __ldg(A.rowptr + row + 1);
       for (int k = k0; k < k1; ++k) {
-        const double av = mul_rn(a.alpha, __ldg(val + k));
+        const T av = mul_rn(alpha, __ldg(val + k));
         y = add_rn(y, mul_rn(av, __ldg(a.X + (long long)__ldg(A.col + k) * s + lane)));
       }
       const long long o = (long long)row * s + lane;
       if (a.mode == 1) y = add_rn(a.C[o], y);
       a.Y[o] = y;
-      if (ND > 0) acc[0] += y * a.W[o];
-      if (ND > 1) acc[1] += y * y;
+      if (ND > 0) acc[0] += (double)y * (double)a.W[o];
+      if (ND > 1) acc[1] += (double)y * (double)y;
     }
   }
   if (ND > 0 || rd.epi) finish_reduction<ND>(acc, rd);
@@ -64,9 +69,10 @@ k_spmm(CsrH A, SpmmArgs a, Red rd) {
 // c * in[i] * M (M s-by-s from slots, optionally transposed); then up to
 // two Gram products G_g = U_g^T V_g (U, V among [in..., out...]) written to
 // S[gslot_g + a * s + b], and up to two Frobenius dots.
+template <typename T>
 struct BlkArgs {
-  const double* in[4];
-  double* out[2];
+  const T* in[4];
+  T* out[2];
   CfH c[2][4];
   short mslot[2][4];     // >= 0: matrix term
   unsigned char trans[2][4];
@@ -77,24 +83,28 @@ struct BlkArgs {
   short gslot[2];
   int nd;
   unsigned char dot[2][2];
+  int prec;
 };
 
 __device__ __forceinline__ void blk_finish(const double* g, int ng, int s,
                                            const double* dd, int nd,
-                                           const BlkArgs& a, const Red& rd);
+                                           const short* gslot, const Red& rd);
 
+// Terms are formed in T (the block's element type); Gram products and dots
+// accumulate in FP64 either way.
+template <typename T>
 __global__ void __launch_bounds__(kThreads, 4)
-k_block(BlkArgs a, Red rd) {
+k_block(BlkArgs<T> a, Red rd) {
   if (skip(rd)) return;
-  __shared__ double tile[6][kBlkTileRows][kBlkS + 1];
-  __shared__ double mat[2][4][kBlkS * kBlkS];
-  __shared__ double cs[2][4];
+  __shared__ T tile[6][kBlkTileRows][kBlkS + 1];
+  __shared__ T mat[2][4][kBlkS * kBlkS];
+  __shared__ T cs[2][4];
   const int s = a.s;
   const int t = threadIdx.x;
   const int r = t / kBlkS, c = t % kBlkS;   // tile element of this thread
   for (int q = t; q < 2 * 4; q += kThreads) {
     const int o = q / 4, i = q % 4;
-    cs[o][i] = (o < a.nout && i < a.nin) ? eval_cf(a.c[o][i], rd.S) : 0.0;
+    cs[o][i] = (o < a.nout && i < a.nin) ? (T)eval_cf(a.c[o][i], rd.S) : T(0);
   }
   for (int o = 0; o < a.nout; ++o)
     for (int i = 0; i < a.nin; ++i)
@@ -102,7 +112,7 @@ k_block(BlkArgs a, Red rd) {
         for (int q = t; q < s * s; q += kThreads) {
           const int b = q / s, cc = q % s;
           const int src = a.trans[o][i] ? cc * s + b : b * s + cc;
-          mat[o][i][q] = rd.S[a.mslot[o][i] + src];
+          mat[o][i][q] = (T)rd.S[a.mslot[o][i] + src];
         }
   __syncthreads();
   double gacc[2] = {0.0, 0.0};
@@ -119,30 +129,30 @@ k_block(BlkArgs a, Red rd) {
       const long long row = row0 + rr;
       const bool valid = c < s && row < a.n;
       for (int i = 0; i < a.nin; ++i)
-        tile[i][rr][c] = valid ? a.in[i][row * s + c] : 0.0;
+        tile[i][rr][c] = valid ? a.in[i][row * s + c] : T(0);
     }
     __syncthreads();
     // Outputs: for each term the s-by-s matrix column c is read once into
     // registers and serves all kBlkSub rows of this thread; every element's
     // terms are accumulated in input order, as before.
     for (int o = 0; o < a.nout; ++o) {
-      double y[kBlkSub];
+      T y[kBlkSub];
       bool first = true;
       for (int i = 0; i < a.nin; ++i) {
         const CfH& cf = a.c[o][i];
         if (!cf.op) continue;
         if (a.mslot[o][i] >= 0) {
-          double mc[kBlkS];
+          T mc[kBlkS];
 #pragma unroll
-          for (int b = 0; b < kBlkS; ++b) mc[b] = b < s ? mat[o][i][b * s + c] : 0.0;
+          for (int b = 0; b < kBlkS; ++b) mc[b] = b < s ? mat[o][i][b * s + c] : T(0);
 #pragma unroll
           for (int k = 0; k < kBlkSub; ++k) {
             const int rr = r + (kThreads / kBlkS) * k;
-            double z = 0.0;
+            T z = T(0);
 #pragma unroll
             for (int b = 0; b < kBlkS; ++b)
               if (b < s) z = fma_rn(tile[i][rr][b], mc[b], z);
-            const double term = cs[o][i] * z;
+            const T term = cs[o][i] * z;
             y[k] = first ? term : add_rn(y[k], term);
           }
         } else {
@@ -157,7 +167,7 @@ k_block(BlkArgs a, Red rd) {
       }
       if (first) {
 #pragma unroll
-        for (int k = 0; k < kBlkSub; ++k) y[k] = 0.0;
+        for (int k = 0; k < kBlkSub; ++k) y[k] = T(0);
       }
 #pragma unroll
       for (int k = 0; k < kBlkSub; ++k) {
@@ -165,7 +175,7 @@ k_block(BlkArgs a, Red rd) {
         const long long row = row0 + rr;
         const bool valid = c < s && row < a.n;
         if (valid) a.out[o][row * s + c] = y[k];
-        tile[4 + o][rr][c] = valid ? y[k] : 0.0;
+        tile[4 + o][rr][c] = valid ? y[k] : T(0);
       }
     }
     __syncthreads();
@@ -177,7 +187,8 @@ k_block(BlkArgs a, Red rd) {
       if (r < s && c < s) {
         double z = gacc[g];
 #pragma unroll 8
-        for (int q = 0; q < kBlkTileRows; ++q) z = fma_rn(tile[tu][q][r], tile[tv][q][c], z);
+        for (int q = 0; q < kBlkTileRows; ++q)
+          z = fma_rn((double)tile[tu][q][r], (double)tile[tv][q][c], z);
         gacc[g] = z;
       }
     }
@@ -188,12 +199,12 @@ k_block(BlkArgs a, Red rd) {
 #pragma unroll
       for (int k = 0; k < kBlkSub; ++k) {
         const int rr = r + (kThreads / kBlkS) * k;
-        dacc[d] = fma_rn(tile[tu][rr][c], tile[tv][rr][c], dacc[d]);
+        dacc[d] = fma_rn((double)tile[tu][rr][c], (double)tile[tv][rr][c], dacc[d]);
       }
     }
     __syncthreads();
   }
-  if (a.ng > 0 || a.nd > 0 || rd.epi) blk_finish(gacc, a.ng, s, dacc, a.nd, a, rd);
+  if (a.ng > 0 || a.nd > 0 || rd.epi) blk_finish(gacc, a.ng, s, dacc, a.nd, a.gslot, rd);
 }
 
 // Deterministic reduction of per-thread Gram entries (thread t owns entry t
@@ -202,7 +213,7 @@ k_block(BlkArgs a, Red rd) {
 // part[(slot) * kMaxBlocks + block], slots 0..2*256-1 Grams, 512.. dots.
 __device__ __forceinline__ void blk_finish(const double* g, int ng, int s,
                                            const double* dd, int nd,
-                                           const BlkArgs& a, const Red& rd) {
+                                           const short* gslot, const Red& rd) {
   __shared__ double wsum[2][kWarps];
   __shared__ int is_last;
   const int t = threadIdx.x;
@@ -231,7 +242,7 @@ __device__ __forceinline__ void blk_finish(const double* g, int ng, int s,
   for (int q = 0; q < ng; ++q) {
     double v = 0.0;
     for (int b = 0; b < nb; ++b) v += __ldcg(rd.part + (q * 256 + t) * kMaxBlocks + b);
-    if (r < s && c < s) rd.S[a.gslot[q] + r * s + c] = v;
+    if (r < s && c < s) rd.S[gslot[q] + r * s + c] = v;
   }
   if (t < nd) {
     double v = 0.0;

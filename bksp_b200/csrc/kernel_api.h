@@ -246,6 +246,9 @@ struct ShiftArgsH {
 };
 void launch_shift(const ShiftArgsH& a, const RedH& rd, cudaStream_t st);
 // Block methods (k_block.cuh): row-major n x s blocks, s <= 16.
+// prec 0: FP64 blocks and values; 1: FP32 blocks and values (A's FP32
+// copy), the pointers then pointing to floats.  Dots and Gram products
+// accumulate in FP64 either way.
 struct SpmmH {
   const double* X;
   double* Y;
@@ -254,6 +257,7 @@ struct SpmmH {
   double alpha;
   int mode, s, nd;   // mode 0: Y = alpha A X; 1: Y = C + alpha A X;
                      // nd dots: (Y, W), (Y, Y)
+  int prec;
 };
 struct BlkH {
   const double* in[4];
@@ -268,6 +272,7 @@ struct BlkH {
   short gslot[2];
   int nd;
   unsigned char dot[2][2];
+  int prec;
 };
 void launch_spmm(const CsrH& A, const SpmmH& a, const RedH& rd, cudaStream_t st);
 void launch_block(const BlkH& a, const RedH& rd, cudaStream_t st);

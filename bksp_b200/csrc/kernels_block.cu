@@ -34,26 +34,45 @@ void launch_shift(const ShiftArgsH& a, const RedH& rd, cudaStream_t st) {
 void launch_spmm(const CsrH& A, const SpmmH& a, const RedH& rd, cudaStream_t st) {
   if (g_prog_rec) prog_unsupported("block / shifted kernel");
   ++launch_count();
-  SpmmArgs s{a.X, a.Y, a.C, a.W, a.alpha, a.mode, a.s, a.nd};
   const int g = grid_for((long long)A.n * kBlkS);
+  if (a.prec == 1) {
+    SpmmArgs<float> s{reinterpret_cast<const float*>(a.X), reinterpret_cast<float*>(a.Y),
+                      reinterpret_cast<const float*>(a.C), reinterpret_cast<const float*>(a.W),
+                      a.alpha, a.mode, a.s, a.nd, a.prec};
+    switch (a.nd) {
+      case 0: launch_k(k_spmm<float, 0>, g, kThreads, 0, st, A, s, rd); break;
+      case 1: launch_k(k_spmm<float, 1>, g, kThreads, 0, st, A, s, rd); break;
+      default: launch_k(k_spmm<float, 2>, g, kThreads, 0, st, A, s, rd); break;
+    }
+    return;
+  }
+  SpmmArgs<double> s{a.X, a.Y, a.C, a.W, a.alpha, a.mode, a.s, a.nd, a.prec};
   switch (a.nd) {
-    case 0: launch_k(k_spmm<0>, g, kThreads, 0, st, A, s, rd); break;
-    case 1: launch_k(k_spmm<1>, g, kThreads, 0, st, A, s, rd); break;
-    default: launch_k(k_spmm<2>, g, kThreads, 0, st, A, s, rd); break;
+    case 0: launch_k(k_spmm<double, 0>, g, kThreads, 0, st, A, s, rd); break;
+    case 1: launch_k(k_spmm<double, 1>, g, kThreads, 0, st, A, s, rd); break;
+    default: launch_k(k_spmm<double, 2>, g, kThreads, 0, st, A, s, rd); break;
   }
 }
 
 void launch_block(const BlkH& a, const RedH& rd, cudaStream_t st) {
   if (g_prog_rec) prog_unsupported("block / shifted kernel");
   ++launch_count();
-  BlkArgs b;
-  static_assert(sizeof(BlkArgs) == sizeof(BlkH), "BlkArgs layout");
-  memcpy(&b, &a, sizeof(b));
+  static_assert(sizeof(BlkArgs<double>) == sizeof(BlkH), "BlkArgs layout");
+  static_assert(sizeof(BlkArgs<float>) == sizeof(BlkH), "BlkArgs layout");
   const long long tiles = (a.n + kBlkTileRows - 1) / kBlkTileRows;
-  const int cap = resident_grid(reinterpret_cast<const void*>(k_block));   // one wave
+  if (a.prec == 1) {
+    BlkArgs<float> b;
+    memcpy(&b, &a, sizeof(b));
+    const int cap = resident_grid(reinterpret_cast<const void*>(k_block<float>));
+    int g = (int)(tiles < cap ? tiles : cap);
+    launch_k(k_block<float>, g < 1 ? 1 : g, kThreads, 0, st, b, rd);
+    return;
+  }
+  BlkArgs<double> b;
+  memcpy(&b, &a, sizeof(b));
+  const int cap = resident_grid(reinterpret_cast<const void*>(k_block<double>));   // one wave
   int g = (int)(tiles < cap ? tiles : cap);
-  if (g < 1) g = 1;
-  launch_k(k_block, g, kThreads, 0, st, b, rd);
+  launch_k(k_block<double>, g < 1 ? 1 : g, kThreads, 0, st, b, rd);
 }
 
 // Column-major n x s (leading dimension n) <-> row-major np x s.

@@ -219,6 +219,22 @@ int bksp_gpu_cg_mixed(bksp_gpu_matrix *A, const double *b, double *x,
 int bksp_dcg_mixed(dspmat *A, double *b, const bksp_gpu_mixed_opts *opts,
                    double *x);
 
+/* Block CG and Block BiCGSTAB(l) (l = opts->l) in mixed precision, with
+ * dblcg's / dblbicgstabl's host arrays: an outer FP64 iterative refinement
+ * (R = B - A X with the FP64 operator) around inner solves of the same
+ * method in FP32 (blocks and operator values; Gram products, dots and the
+ * s-by-s factorisations in FP64), each to a relative Frobenius residual of
+ * opts->delta (0: 1e-4); stops when every column's FP64 true relative
+ * residual ||b_j - A x_j|| / ||b_j|| is <= opts->target.  opts->precond and
+ * opts->model are not used.  Returns the total inner iterations minus one
+ * at convergence, NOT_CONVERGED (budget opts->max_iter spent, or the
+ * refinement stagnates), DIVERGENCE, INVALID_MATRIX_TYPE (Block CG with a
+ * non-"symmetric" matrix) or INVALID_PARAMETERS. */
+int bksp_dblcg_mixed(dspmat *A, dmat *B, const bksp_gpu_mixed_opts *opts,
+                     dmat *X);
+int bksp_dblbicgstabl_mixed(dspmat *A, dmat *B, const bksp_gpu_mixed_opts *opts,
+                            dmat *X);
+
 /* ------------------------------------------------------------ batches */
 
 /* Many independent systems in one call, each solved as bksp_gpu_solve_mixed

@@ -1,0 +1,90 @@
+"""GPU parity at the full sizes of the block and shifted benchmark
+configurations, against the compiled reference's outputs at those sizes
+(tests/golden/reference_full.json, 8 OpenBLAS threads):
+
+* Block CG and Block BiCGSTAB(2), 3D Poisson 64^3 (n = 262,144), 16
+  Gaussian right-hand sides (seed 2), tol 1e-8;
+* shifted BiCGSTAB(4), 2D convection-diffusion 1024^2 (n = 1,048,576), 32
+  log-spaced shifts 1e-3..1, b ~ U[-1,1] (seed 3), tol 1e-8.
+
+Criteria: return index within max(2, 5 %) (Block BiCGSTAB(l): 10 %, its QR
+is a Cholesky QR with a non-negative R diagonal where the reference calls
+LAPACK's Householder QR, which changes the rounding of every block step);
+convergence-test history within 1e-6 relative over the first 20 tests while
+the reference value is above 1e-8 (block: 1e-5); the worst column's / the
+worst shift's FP64 true residual within 10x the reference's."""
+import json
+import os
+
+import numpy as np
+import pytest
+import scipy.sparse as sp
+
+from conftest import GOLDEN, hist_close, iters_close
+from bksp_b200 import problems as P
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def full():
+    with open(os.path.join(GOLDEN, "reference_full.json")) as f:
+        return json.load(f)
+
+
+def _col_res(A, B, X):
+    return [float(np.linalg.norm(B[:, j] - A @ X[:, j]) / np.linalg.norm(B[:, j]))
+            for j in range(B.shape[1])]
+
+
+@pytest.fixture(scope="module")
+def poisson64():
+    rp, c, v, n = P.poisson3d(64)
+    lrp, lc, lv, _ = P.lower_triangle(rp, c, v, n)
+    A = sp.csr_matrix((v, c, rp), shape=(n, n))
+    Bm = np.random.default_rng(2).standard_normal((n, 16))
+    return rp, c, v, lrp, lc, lv, n, A, Bm
+
+
+def test_block_cg_poisson64(gpu, full, poisson64):
+    B = gpu
+    rp, c, v, lrp, lc, lv, n, A, Bm = poisson64
+    X = np.zeros((n, 16))
+    with B.record(hist_cap=6000) as st:
+        ret = B.dblcg(B.CsrMatrix(lrp, lc, lv, symmetric=True), Bm, 1e-8, 5000, X)
+    g = full["cfg3/blcg_p64"]
+    assert iters_close(ret, g["ret"]), (ret, g["ret"])
+    hist_close(st["hist"], g["hist"], k=20, rtol=1e-5, floor=1e-8)
+    assert max(_col_res(A, Bm, X)) <= 10 * max(g["true_res_cols"])
+
+
+def test_block_bicgstabl2_poisson64(gpu, full, poisson64):
+    B = gpu
+    rp, c, v, lrp, lc, lv, n, A, Bm = poisson64
+    X = np.zeros((n, 16))
+    with B.record(hist_cap=6000) as st:
+        ret = B.dblbicgstabl(B.CsrMatrix(rp, c, v), Bm, 2, 1e-8, 5000, X)
+    g = full["cfg3/blbicgstabl2_p64"]
+    assert iters_close(ret, g["ret"], rel=0.1), (ret, g["ret"])
+    hist_close(st["hist"], g["hist"], k=20, rtol=1e-5, floor=1e-8)
+    assert max(_col_res(A, Bm, X)) <= 10 * max(g["true_res_cols"])
+
+
+def test_shifted_bicgstabl4_convdiff1024(gpu, full):
+    B = gpu
+    rp, c, v, n = P.convdiff2d(1024)
+    A = sp.csr_matrix((v, c, rp), shape=(n, n))
+    b = P.uniform(n, 3)
+    sig = P.log_shifts(32)
+    x = np.zeros(33 * n)
+    with B.record(hist_cap=6000) as st:
+        ret = B.dshbicgstabl(B.CsrMatrix(rp, c, v), b, 4, sig, 1e-8, 5000, x)
+    g = full["cfg4/shbicgstabl4_cd1024"]
+    assert iters_close(ret, g["ret"]), (ret, g["ret"])
+    hist_close(st["hist"], g["hist"], k=20, rtol=1e-6, floor=1e-8)
+    nb = np.linalg.norm(b)
+    seed = np.linalg.norm(b - A @ x[:n]) / nb
+    assert seed <= 10 * g["true_res_seed"]
+    worst = max(np.linalg.norm(b - (A @ x[(k + 1) * n:(k + 2) * n] + s * x[(k + 1) * n:(k + 2) * n])) / nb
+                for k, s in enumerate(sig))
+    assert worst <= 10 * max(g["true_res_shifts"]), (worst, max(g["true_res_shifts"]))
