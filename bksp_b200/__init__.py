@@ -88,6 +88,8 @@ def _load():
         f = getattr(L, name)
         f.argtypes = argt
         f.restype = C.c_int
+    L.bksp_gpu_dcsrmm.argtypes = [sp, C.c_char, i, d, _dp, d, _dp]
+    L.bksp_gpu_dcsrmm.restype = i
     L.read_matrix_market.argtypes = [C.c_char_p]
     L.read_matrix_market.restype = sp
     L.bksp_gpu_record.argtypes = [C.POINTER(Stats)]
@@ -255,6 +257,18 @@ def dshbicgstabl(A, b, l, sigma, tol, max_iter, x):
     return lib.dshbicgstabl(A.ptr, b.ctypes.data_as(_dp), l,
                             s.ctypes.data_as(_dp), int(s.size), tol,
                             max_iter, _inplace(x))
+
+
+def dcsrmm(A, Bm, C, alpha=1.0, beta=0.0, trans="n"):
+    """C = beta C + alpha A B on the GPU (bksp_gpu_dcsrmm); C (n-by-s) is
+    updated in place."""
+    Bf = np.asfortranarray(Bm, dtype=np.float64)
+    Cf = np.asfortranarray(C, dtype=np.float64)
+    rc = lib.bksp_gpu_dcsrmm(A.ptr, trans.encode(), Bf.shape[1], float(alpha),
+                             Bf.ctypes.data_as(_dp), float(beta),
+                             Cf.ctypes.data_as(_dp))
+    C[...] = Cf
+    return rc
 
 
 def myqr(V):

@@ -582,3 +582,60 @@ extern "C" int bksp_gpu_dcsrmv(dspmat* A, char trans, const double* x,
     return INVALID_PARAMETERS;
   }
 }
+
+// C = beta C + alpha A B on the GPU with host arrays (reference
+// src/matvec.c:130-172 dcsrgemm1 / 219-247 dcsrsymm1, via mkl_dcsrmm),
+// B and C column-major n x s: the product runs on row-major device blocks
+// (the block methods' layout) with the SpMM kernel the block methods use --
+// the diagonal-form kernel for stencil operators, the CSR kernel otherwise.
+extern "C" int bksp_gpu_dcsrmm(dspmat* A, char trans, int s, double alpha,
+                               const double* B, double beta, double* C) {
+  if (check_matrix(A) != 0 || !B || !C) return INVALID_PARAMETERS;
+  if ((trans != 'n' && trans != 's') || s < 1 || s > kBlockMaxS) return INVALID_PARAMETERS;
+  try {
+    Ctx& cx = Ctx::get();
+    cudaStream_t st = cx.st;
+    const int n = *A->row_size;
+    DevCsr dA;
+    upload_operator(A, trans == 's', false, dA, st);
+    const long long np = pad64(n);
+    std::vector<double> cb((size_t)n * s);
+    for (size_t q = 0; q < cb.size(); ++q) cb[q] = beta * C[q];
+    double* tmp = dalloc_n<double>((long long)n * s, st);
+    double* dB = dalloc_n<double>(np * s, st);
+    double* dC = dalloc_n<double>(np * s, st);
+    BK_CHECK(cudaMemsetAsync(dB, 0, sizeof(double) * np * s, st));
+    BK_CHECK(cudaMemsetAsync(dC, 0, sizeof(double) * np * s, st));
+    BK_CHECK(cudaMemcpyAsync(tmp, B, sizeof(double) * n * s, cudaMemcpyHostToDevice, st));
+    launch_cm2rm(tmp, dB, n, s, st);
+    BK_CHECK(cudaMemcpyAsync(tmp, cb.data(), sizeof(double) * n * s, cudaMemcpyHostToDevice, st));
+    launch_cm2rm(tmp, dC, n, s, st);
+    SolveState ss;
+    ss.create(0, st);
+    ss.start(0, 1, 0.0, st);
+    SpmmH a;
+    std::memset(&a, 0, sizeof(a));
+    a.X = dB;
+    a.Y = dC;
+    a.C = dC;
+    a.alpha = alpha;
+    a.mode = 1;
+    a.s = s;
+    launch_spmm(dA.h64(), a, ss.red(kD, E_NONE), st);
+    BK_CHECK(cudaGetLastError());
+    launch_rm2cm(dC, tmp, n, s, st);
+    BK_CHECK(cudaMemcpyAsync(C, tmp, sizeof(double) * n * s, cudaMemcpyDeviceToHost, st));
+    BK_CHECK(cudaStreamSynchronize(st));
+    ss.release(st);
+    dfree(tmp, st);
+    dfree(dB, st);
+    dfree(dC, st);
+    dA.release(st);
+    BK_CHECK(cudaStreamSynchronize(st));
+    return 0;
+  } catch (const std::exception& e) {
+    if (std::getenv("BKSP_GPU_VERBOSE")) std::fprintf(stderr, "bksp: %s\n", e.what());
+    cudaGetLastError();
+    return INVALID_PARAMETERS;
+  }
+}

@@ -156,7 +156,9 @@ static __device__ bool qr_pass(double* S, int pass) {
     double tr = 0.0;
     for (int i = 0; i < s; ++i) tr += G[i * s + i];
     const double m = S[kBkRows];
-    shift = 11.0 * (m * s + s * (s + 1.0)) * 1.1102230246251565e-16 * tr;
+    // unit roundoff of the data: FP64 blocks, or FP32 blocks (mixed solves)
+    const double u = S[kBkU] > 0.0 ? S[kBkU] : 1.1102230246251565e-16;
+    shift = 11.0 * (m * s + s * (s + 1.0)) * u * tr;
   }
   if (!dm_chol(G, Rp, s, shift)) return false;
   dm_triinv(Rp, S + kBkRinv, s);

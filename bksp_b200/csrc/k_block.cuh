@@ -64,6 +64,71 @@ k_spmm(CsrH A, SpmmArgs<T> a, Red rd) {
   if (ND > 0 || rd.epi) finish_reduction<ND>(acc, rd);
 }
 
+// SpMM on the diagonal form (stencil operators): each row's s values are
+// handled by s / V threads with 16-byte loads and stores (V = 2 doubles or
+// 4 floats per thread), the row's diagonal value loaded once per diagonal
+// and shared by those threads; entries in ascending diagonal (= column)
+// order with the reference's rounding (y += (alpha a_k) x_k), so the
+// result equals k_spmm's.  Needs s % V == 0 and 16-byte aligned blocks.
+template <typename T> struct Vec16;
+template <> struct Vec16<double> { using V = double2; static constexpr int N = 2; };
+template <> struct Vec16<float> { using V = float4; static constexpr int N = 4; };
+
+template <typename T, int ND>
+__global__ void __launch_bounds__(kThreads, 4)
+k_spmm_dia(CsrH A, SpmmArgs<T> a, Red rd) {
+  if (skip(rd)) return;
+  using PV = typename Vec16<T>::V;
+  constexpr int VN = Vec16<T>::N;
+  const T* __restrict__ V = static_cast<const T*>(A.dia.val);
+  const long long stride = A.dia.stride;
+  const int s = a.s, nd = A.dia.nd, n = A.n;
+  const int tpr = s / VN;                       // threads per row
+  const int rows_per_pass = kThreads / tpr;
+  const int q = threadIdx.x % tpr, rloc = threadIdx.x / tpr;
+  const bool active = rloc < rows_per_pass;     // kThreads % tpr leftovers idle
+  const T alpha = (T)a.alpha;
+  double acc[ND > 0 ? ND : 1];
+#pragma unroll
+  for (int d = 0; d < ND; ++d) acc[d] = 0.0;
+  for (long long row = (long long)blockIdx.x * rows_per_pass + rloc; active && row < n;
+       row += (long long)gridDim.x * rows_per_pass) {
+    const unsigned m = __ldg(A.dia.mask + row);
+    T y[VN];
+#pragma unroll
+    for (int e = 0; e < VN; ++e) y[e] = T(0);
+#pragma unroll
+    for (int d = 0; d < kDiaMax; ++d) {
+      if (d < nd && ((m >> d) & 1u)) {
+        const T av = mul_rn(alpha, __ldg(V + d * stride + row));
+        const long long j = row + A.dia.off[d];
+        T xv[VN];
+        unpack<T>(__ldg(reinterpret_cast<const PV*>(a.X + j * s) + q), xv);
+#pragma unroll
+        for (int e = 0; e < VN; ++e) y[e] = add_rn(y[e], mul_rn(av, xv[e]));
+      }
+    }
+    const long long o = row * s + q * VN;
+    if (a.mode == 1) {
+      T cv[VN];
+      unpack<T>(reinterpret_cast<const PV*>(a.C + o)[0], cv);
+#pragma unroll
+      for (int e = 0; e < VN; ++e) y[e] = add_rn(cv[e], y[e]);
+    }
+    reinterpret_cast<PV*>(a.Y + o)[0] = repack<T>(y);
+    if (ND > 0) {
+      T wv[VN];
+      unpack<T>(reinterpret_cast<const PV*>(a.W + o)[0], wv);
+#pragma unroll
+      for (int e = 0; e < VN; ++e) acc[0] += (double)y[e] * (double)wv[e];
+    }
+    if (ND > 1)
+#pragma unroll
+      for (int e = 0; e < VN; ++e) acc[1] += (double)y[e] * (double)y[e];
+  }
+  if (ND > 0 || rd.epi) finish_reduction<ND>(acc, rd);
+}
+
 // ---------------------------------------------- block linear combination
 // out[o] = sum_i term(o, i) with term = c * in[i] (scalar) or
 // c * in[i] * M (M s-by-s from slots, optionally transposed); then up to
@@ -121,17 +186,34 @@ k_block(BlkArgs<T> a, Red rd) {
   // tile (k < kBlkSub), column c: all of a tile's loads are issued before
   // its first use.
   const long long ntiles = (a.n + kBlkTileRows - 1) / kBlkTileRows;
-  for (long long tl = blockIdx.x; tl < ntiles; tl += gridDim.x) {
+  // The next tile's inputs are loaded into registers while the current tile
+  // is computed, so each tile's global loads overlap the previous tile's
+  // work instead of starting after it.
+  T pre[4][kBlkSub];
+  auto fetch = [&](long long tl) {
     const long long row0 = tl * kBlkTileRows;
 #pragma unroll
     for (int k = 0; k < kBlkSub; ++k) {
       const int rr = r + (kThreads / kBlkS) * k;
       const long long row = row0 + rr;
-      const bool valid = c < s && row < a.n;
-      for (int i = 0; i < a.nin; ++i)
-        tile[i][rr][c] = valid ? a.in[i][row * s + c] : T(0);
+      const bool valid = c < s && row < a.n && tl < ntiles;
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+        pre[i][k] = (i < a.nin && valid) ? a.in[i][row * s + c] : T(0);
+    }
+  };
+  fetch(blockIdx.x);
+  for (long long tl = blockIdx.x; tl < ntiles; tl += gridDim.x) {
+    const long long row0 = tl * kBlkTileRows;
+#pragma unroll
+    for (int k = 0; k < kBlkSub; ++k) {
+      const int rr = r + (kThreads / kBlkS) * k;
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+        if (i < a.nin) tile[i][rr][c] = pre[i][k];
     }
     __syncthreads();
+    fetch(tl + gridDim.x);
     // Outputs: for each term the s-by-s matrix column c is read once into
     // registers and serves all kBlkSub rows of this thread; every element's
     // terms are accumulated in input order, as before.
@@ -216,9 +298,14 @@ __device__ __forceinline__ void blk_finish(const double* g, int ng, int s,
                                            const short* gslot, const Red& rd) {
   __shared__ double wsum[2][kWarps];
   __shared__ int is_last;
+  // Block-major partials (block b's kBlkPart values contiguous), so both
+  // the writes here and the last block's reads are coalesced, and a
+  // thread's reads of consecutive blocks are independent loads the loop
+  // keeps in flight together.
+  constexpr int kBlkPart = 514;
   const int t = threadIdx.x;
-  for (int q = 0; q < ng; ++q)
-    rd.part[(q * 256 + t) * kMaxBlocks + blockIdx.x] = g[q];
+  double* mine = rd.part + (long long)blockIdx.x * kBlkPart;
+  for (int q = 0; q < ng; ++q) mine[q * 256 + t] = g[q];
   for (int d = 0; d < nd; ++d) {
     const double v = warp_sum(dd[d]);
     if ((t & 31) == 0) wsum[d][t >> 5] = v;
@@ -228,7 +315,7 @@ __device__ __forceinline__ void blk_finish(const double* g, int ng, int s,
     for (int d = 0; d < nd; ++d) {
       double v = 0.0;
       for (int w = 0; w < kWarps; ++w) v += wsum[d][w];
-      rd.part[(512 + d) * kMaxBlocks + blockIdx.x] = v;
+      mine[512 + d] = v;
     }
     __threadfence();
     const unsigned tk = atomicAdd(rd.ticket, 1u);
@@ -241,12 +328,14 @@ __device__ __forceinline__ void blk_finish(const double* g, int ng, int s,
   const int r = t / kBlkS, c = t % kBlkS;
   for (int q = 0; q < ng; ++q) {
     double v = 0.0;
-    for (int b = 0; b < nb; ++b) v += __ldcg(rd.part + (q * 256 + t) * kMaxBlocks + b);
+#pragma unroll 16
+    for (int b = 0; b < nb; ++b) v += __ldcg(rd.part + (long long)b * kBlkPart + q * 256 + t);
     if (r < s && c < s) rd.S[gslot[q] + r * s + c] = v;
   }
   if (t < nd) {
     double v = 0.0;
-    for (int b = 0; b < nb; ++b) v += __ldcg(rd.part + (512 + t) * kMaxBlocks + b);
+#pragma unroll 16
+    for (int b = 0; b < nb; ++b) v += __ldcg(rd.part + (long long)b * kBlkPart + 512 + t);
     rd.S[rd.out + t] = v;
   }
   __syncthreads();

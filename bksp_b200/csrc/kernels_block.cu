@@ -31,9 +31,47 @@ void launch_shift(const ShiftArgsH& a, const RedH& rd, cudaStream_t st) {
 
 // --------------------------------------------------------- block methods
 
+// BKSP_GPU_SPMM=csr forces the CSR kernel (for comparisons).
+static bool spmm_dia_off() {
+  static const bool off = [] {
+    const char* e = std::getenv("BKSP_GPU_SPMM");
+    return e && std::strcmp(e, "csr") == 0;
+  }();
+  return off;
+}
+
 void launch_spmm(const CsrH& A, const SpmmH& a, const RedH& rd, cudaStream_t st) {
   if (g_prog_rec) prog_unsupported("block / shifted kernel");
   ++launch_count();
+  // Diagonal form: 16-byte row segments (s a multiple of the vector width,
+  // aligned blocks); else the CSR kernel.
+  auto al = [](const void* p) { return ((uintptr_t)p & 15u) == 0; };
+  const int vn = a.prec == 1 ? 4 : 2;
+  if (A.dia.nd > 0 && a.s % vn == 0 && al(a.X) && al(a.Y) && al(a.C) && al(a.W) &&
+      !spmm_dia_off()) {
+    const long long rows = A.n;
+    const long long per = kThreads / (a.s / vn);
+    const long long items = rows * (a.s / vn);
+    if (a.prec == 1) {
+      SpmmArgs<float> s{reinterpret_cast<const float*>(a.X), reinterpret_cast<float*>(a.Y),
+                        reinterpret_cast<const float*>(a.C), reinterpret_cast<const float*>(a.W),
+                        a.alpha, a.mode, a.s, a.nd, a.prec};
+      switch (a.nd) {
+        case 0: launch_k(k_spmm_dia<float, 0>, grid_wave(k_spmm_dia<float, 0>, items), kThreads, 0, st, A, s, rd); break;
+        case 1: launch_k(k_spmm_dia<float, 1>, grid_wave(k_spmm_dia<float, 1>, items), kThreads, 0, st, A, s, rd); break;
+        default: launch_k(k_spmm_dia<float, 2>, grid_wave(k_spmm_dia<float, 2>, items), kThreads, 0, st, A, s, rd); break;
+      }
+    } else {
+      SpmmArgs<double> s{a.X, a.Y, a.C, a.W, a.alpha, a.mode, a.s, a.nd, a.prec};
+      switch (a.nd) {
+        case 0: launch_k(k_spmm_dia<double, 0>, grid_wave(k_spmm_dia<double, 0>, items), kThreads, 0, st, A, s, rd); break;
+        case 1: launch_k(k_spmm_dia<double, 1>, grid_wave(k_spmm_dia<double, 1>, items), kThreads, 0, st, A, s, rd); break;
+        default: launch_k(k_spmm_dia<double, 2>, grid_wave(k_spmm_dia<double, 2>, items), kThreads, 0, st, A, s, rd); break;
+      }
+    }
+    (void)per;
+    return;
+  }
   const int g = grid_for((long long)A.n * kBlkS);
   if (a.prec == 1) {
     SpmmArgs<float> s{reinterpret_cast<const float*>(a.X), reinterpret_cast<float*>(a.Y),

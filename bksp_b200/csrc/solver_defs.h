@@ -15,6 +15,7 @@ enum : short {
   kL = 2,        // degree l (BiCGSTAB(l) family), stored as a double
   kNs = 3,       // number of shifts
   kTrue = 4,     // scratch: true-residual norms etc.
+  kBkU = 5,      // block methods: unit roundoff of the block elements
   kD = 8,        // dot outputs D0..D7
   kUser = 16,    // first method-specific slot
 };

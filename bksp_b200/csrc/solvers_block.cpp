@@ -124,6 +124,7 @@ void BlockCtx::start(int max_iter, double tol) {
   ss.start(0, max_iter, tol, st);
   ss.set_scalar(kBkS, (double)s, st);
   ss.set_scalar(kBkRows, (double)n, st);
+  ss.set_scalar(kBkU, unit, st);
 }
 
 // Passes 2 and 3 of the Cholesky-QR of V (pass 1's epilogue ran on the
@@ -159,6 +160,7 @@ template <typename T>
 SolveOut blcg(BlockCtx& bc, const DevCsr& A, const T* B, T* X, double tol,
               int max_iter) {
   constexpr int PR = prec_of<T>();
+  bc.unit = PR ? 5.9604644775390625e-08 : 1.1102230246251565e-16;
   cudaStream_t st = bc.st;
   const int s = bc.s;
   const long long rows = bc.np;
@@ -217,6 +219,7 @@ template <typename T>
 SolveOut blbicgstab(BlockCtx& bc, const DevCsr& A, const T* B, T* X, double tol,
                     int max_iter) {
   constexpr int PR = prec_of<T>();
+  bc.unit = PR ? 5.9604644775390625e-08 : 1.1102230246251565e-16;
   cudaStream_t st = bc.st;
   const int s = bc.s;
   const long long rows = bc.np;
@@ -299,6 +302,7 @@ template <typename T>
 SolveOut blbicgstabl(BlockCtx& bc, const DevCsr& A, const T* B, T* X, int l,
                      double tol, int max_iter, double* true_res_out) {
   constexpr int PR = prec_of<T>();
+  bc.unit = PR ? 5.9604644775390625e-08 : 1.1102230246251565e-16;
   if (l < 1 || l > kBlMaxL) throw CudaError("blbicgstabl: l out of range");
   cudaStream_t st = bc.st;
   const int s = bc.s;

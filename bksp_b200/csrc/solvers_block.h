@@ -18,6 +18,7 @@ struct BlockCtx {
   SolveState& ss;
   cudaStream_t st;
   double* bpart = nullptr;
+  double unit = 1.1102230246251565e-16;   // unit roundoff of the blocks (QR shift)
   std::vector<void*> owned;
   BlockCtx(int n, int s, SolveState& ss, cudaStream_t st);
   ~BlockCtx();

@@ -57,6 +57,16 @@ int bksp_gpu_device_count(void);
  * fused multiply-add). */
 int bksp_gpu_dcsrmv(dspmat *A, char trans, const double *x, double *y);
 
+/* The block product with host arrays: C = beta C + alpha A B, B and C
+ * column-major n x s (s <= 16), trans 'n' (A as stored; the reference's
+ * dcsrgemm1 / mkl_dcsrmm) or 's' (the mirrored one-triangle operator,
+ * dcsrsymm1).  Runs the block methods' SpMM kernel: diagonal form with
+ * 16-byte row segments for stencil operators, CSR otherwise; entries in
+ * ascending column order, y += (alpha a_k) x_k, then C added.  Returns 0 or
+ * INVALID_PARAMETERS. */
+int bksp_gpu_dcsrmm(dspmat *A, char trans, int s, double alpha,
+                    const double *B, double beta, double *C);
+
 /* ------------------------------------------------ device-resident solves */
 
 typedef struct bksp_gpu_matrix bksp_gpu_matrix;
