@@ -115,6 +115,7 @@ def _load():
                                     C.POINTER(Stats)]
     L.bksp_dcg_mixed.argtypes = [sp, _dp, C.POINTER(MixedOpts), _dp]
     L.bksp_dblcg_mixed.argtypes = [sp, mp, C.POINTER(MixedOpts), mp]
+    L.bksp_dshbicgstabl_mixed.argtypes = [sp, _dp, _dp, i, C.POINTER(MixedOpts), _dp]
     L.bksp_dblbicgstabl_mixed.argtypes = [sp, mp, C.POINTER(MixedOpts), mp]
     L.bksp_gpu_solve_mixed_batch.argtypes = [C.POINTER(vp), C.POINTER(vp),
                                              C.POINTER(vp), i,
@@ -539,6 +540,17 @@ def dblbicgstabl_mixed(A, B, l, X, target=1e-8, max_iter=10000, inner_tol=0.0):
     """bksp_dblbicgstabl_mixed: Block BiCGSTAB(l), as dblcg_mixed."""
     o = MixedOpts(l, target, max_iter, 0, None, inner_tol, 0, 0)
     return _block(lib.bksp_dblbicgstabl_mixed, A, B, (C.byref(o),), X)
+
+
+def dshbicgstabl_mixed(A, b, l, sigma, x, target=1e-8, max_iter=10000):
+    """bksp_dshbicgstabl_mixed: FP32 shift vectors, FP64 per-shift
+    polishing; x (n * (len(sigma) + 1), seed first) updated in place."""
+    b = _vec(b)
+    s = _vec(sigma)
+    o = MixedOpts(l, target, max_iter, 0, None, 0.0, 0, 0)
+    return lib.bksp_dshbicgstabl_mixed(A.ptr, b.ctypes.data_as(_dp),
+                                       s.ctypes.data_as(_dp), int(s.size),
+                                       C.byref(o), _inplace(x))
 
 
 def _batch_args(mats, bs, xs):

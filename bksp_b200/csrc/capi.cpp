@@ -420,8 +420,9 @@ int myqr(int m, int n, double* mat, double* r) {
 
 namespace {
 
+// mixed: the mixed-precision shifted BiCGSTAB(l) (tol = FP64 target).
 int solve_shifted(bool stab, dspmat* A, double* b, int l, double* sigma,
-                  int ns, double tol, int max_iter, double* x) {
+                  int ns, double tol, int max_iter, double* x, bool mixed = false) {
   if (check_matrix(A) != 0 || !b || !x || ns < 0 || ns > kMaxShifts ||
       (ns > 0 && !sigma))
     return INVALID_PARAMETERS;
@@ -432,7 +433,7 @@ int solve_shifted(bool stab, dspmat* A, double* b, int l, double* sigma,
     Timer tm(st);
     const int n = *A->row_size;
     DevCsr dA, dAt;
-    upload_operator(A, false, false, dA, st);
+    upload_operator(A, false, mixed, dA, st);
     if (!stab) {
       HostCsr t = transpose(n, A->row, A->col, A->value);
       upload_csr(n, t.rowptr.data(), t.col.data(), t.val.data(), false, dAt, st);
@@ -442,11 +443,23 @@ int solve_shifted(bool stab, dspmat* A, double* b, int l, double* sigma,
     SolveState ss;
     ss.create(hist_cap_for(max_iter), st);
     tm.begin_solve();
-    SolveOut o = stab ? bk::shbicgstabl(dA, db, l, sigma, ns, dx, tol, max_iter, ss, st)
-                      : bk::shbicg(dA, dAt, db, sigma, ns, dx, tol, max_iter, ss, st);
+    SolveOut o;
+    MixedOut mo;
+    if (mixed) {
+      mo = bk::shbicgstabl_mixed(dA, db, l, sigma, ns, dx, tol, max_iter, ss, st);
+      o = mo;
+    } else {
+      o = stab ? bk::shbicgstabl(dA, db, l, sigma, ns, dx, tol, max_iter, ss, st)
+               : bk::shbicg(dA, dAt, db, sigma, ns, dx, tol, max_iter, ss, st);
+    }
     tm.end_solve();
     download_vec(x, dx, n, (long long)ns + 1, st);
-    tm.report(o.ret, &ss, o.iters);
+    tm.report(o.ret, mixed ? nullptr : &ss, o.iters);
+    if (mixed && g_stats) {
+      g_stats->true_res = mo.true_res;
+      g_stats->inner_iters = mo.iters;
+      g_stats->sweeps = mo.replacements;
+    }
     ss.release(st);
     dfree(db, st);
     dfree(dx, st);
@@ -473,6 +486,14 @@ int dshbicg(dspmat* A, double* b, double* sigma, int sigma_size, double tol,
 int dshbicgstabl(dspmat* A, double* b, int l, double* sigma, int sigma_size,
                  double tol, int max_iter, double* x) {
   return solve_shifted(true, A, b, l, sigma, sigma_size, tol, max_iter, x);
+}
+
+int bksp_dshbicgstabl_mixed(dspmat* A, double* b, double* sigma, int sigma_size,
+                            const bksp_gpu_mixed_opts* o, double* x) {
+  if (!o) return INVALID_PARAMETERS;
+  return solve_shifted(true, A, b, o->l, sigma, sigma_size,
+                       o->target > 0 ? o->target : 1e-8,
+                       o->max_iter > 0 ? o->max_iter : 10000, x, true);
 }
 
 }  // extern "C"

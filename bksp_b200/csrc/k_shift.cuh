@@ -22,19 +22,24 @@ namespace bk {
 //   3  shifted BiCGSTAB(l), update (before the seed r0 update):
 //                               x_k += sum_i cx_k[i] r[i];
 //                               p_k[0] = (p_k[0] - w[l-1] p_k[l] - sum_{i<l} w[i-1] p_k[i]) / psi_k
+// PT: storage type of the shift vectors p_k (double, or float in the
+// mixed-precision shifted solve, where they are the bulk of the traffic);
+// every update is computed in FP64 and rounded to PT when stored.  The seed
+// vectors and x_k are always FP64.
+template <typename PT>
 struct ShiftArgs {
   const double* r;   // seed r[0..l] (stride np)
   const double* p;   // seed p[0..l]
   double* x;         // seed x
   double* xs;        // x_k at xs + k * np
-  double* ps;        // p_k[i] at ps + (k * (l + 1) + i) * np
+  PT* ps;            // p_k[i] at ps + (k * (l + 1) + i) * np
   long long np;
   int ns, l, j, mode;
 };
 
-template <int MODE>
+template <int MODE, typename PT>
 __global__ void __launch_bounds__(kThreads, 4)
-k_shift(ShiftArgs a, Red rd) {
+k_shift(ShiftArgs<PT> a, Red rd) {
   if (skip(rd)) return;
   __shared__ double c0[kMaxShifts], c1[kMaxShifts], c2[kMaxShifts],
       c3[kMaxShifts], c4[kMaxShifts];
@@ -69,9 +74,9 @@ k_shift(ShiftArgs a, Red rd) {
       r[0] = a.r[i];
       a.x[i] = fma_rn(alpha, a.p[i], a.x[i]);
       for (int k = 0; k < ns; ++k) {
-        double* pk = a.ps + (long long)k * np;
-        const double pv = fma_rn(c1[k], r[0], mul_rn(c0[k], pk[i]));
-        pk[i] = pv;
+        PT* pk = a.ps + (long long)k * np;
+        const double pv = (double)(PT)fma_rn(c1[k], r[0], mul_rn(c0[k], (double)pk[i]));
+        pk[i] = (PT)pv;
         double* xk = a.xs + (long long)k * np;
         xk[i] = fma_rn(c2[k], pv, xk[i]);
       }
@@ -79,38 +84,39 @@ k_shift(ShiftArgs a, Red rd) {
       for (int q = 0; q <= j; ++q) r[q] = a.r[q * np + i];
       a.x[i] = fma_rn(alpha, a.p[i], a.x[i]);
       for (int k = 0; k < ns; ++k) {
-        double* pk = a.ps + (long long)k * (l + 1) * np;
+        PT* pk = a.ps + (long long)k * (l + 1) * np;
         double p0 = 0.0;
         for (int q = 0; q <= j; ++q) {
-          const double pv = fma_rn(c1[k], r[q], mul_rn(c0[k], pk[q * np + i]));
-          pk[q * np + i] = pv;
+          const double pv =
+              (double)(PT)fma_rn(c1[k], r[q], mul_rn(c0[k], (double)pk[q * np + i]));
+          pk[q * np + i] = (PT)pv;
           if (q == 0) p0 = pv;
         }
-        pk[(j + 1) * np + i] = mul_rn(r[j], c3[k]);
+        pk[(j + 1) * np + i] = (PT)mul_rn(r[j], c3[k]);
         double* xk = a.xs + (long long)k * np;
         xk[i] = fma_rn(c2[k], p0, xk[i]);
       }
     } else if (MODE == 2) {
       const double rj = a.r[j * np + i];
       for (int k = 0; k < ns; ++k) {
-        double* pk = a.ps + (long long)k * (l + 1) * np;
-        double v = fma_rn(c0[k], rj, pk[(j + 1) * np + i]);
+        PT* pk = a.ps + (long long)k * (l + 1) * np;
+        double v = fma_rn(c0[k], rj, (double)pk[(j + 1) * np + i]);
         v = mul_rn(v, c1[k]);
-        pk[(j + 1) * np + i] = fma_rn(c2[k], pk[j * np + i], v);
+        pk[(j + 1) * np + i] = (PT)fma_rn(c2[k], (double)pk[j * np + i], v);
       }
     } else {
       for (int q = 0; q < l; ++q) r[q] = a.r[q * np + i];
       for (int k = 0; k < ns; ++k) {
-        double* pk = a.ps + (long long)k * (l + 1) * np;
+        PT* pk = a.ps + (long long)k * (l + 1) * np;
         double* xk = a.xs + (long long)k * np;
         double xv = fma_rn(cx[k][0], r[0], xk[i]);
-        double p0 = fma_rn(-om[l - 1], pk[l * np + i], pk[i]);
+        double p0 = fma_rn(-om[l - 1], (double)pk[l * np + i], (double)pk[i]);
         for (int q = 1; q < l; ++q) {
-          p0 = fma_rn(-om[q - 1], pk[q * np + i], p0);
+          p0 = fma_rn(-om[q - 1], (double)pk[q * np + i], p0);
           xv = fma_rn(cx[k][q], r[q], xv);
         }
         xk[i] = xv;
-        pk[i] = mul_rn(p0, c4[k]);
+        pk[i] = (PT)mul_rn(p0, c4[k]);
       }
     }
   }

@@ -118,6 +118,7 @@ k_spmv(CsrH A, SpmvH<XT> io, Red rd) {
       __syncthreads();
     }
     if (row >= 0) {
+      if (io.shift != 0.0) sum = add_rn(sum, mul_rn((XT)io.shift, io.x[row]));
       XT y = sum;
       if (io.mode == 1) y = add_rn(bv, -sum);
       io.y[row] = y;

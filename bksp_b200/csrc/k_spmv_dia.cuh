@@ -142,6 +142,12 @@ k_spmv_dia(CsrH A, SpmvH<XT> io, Red rd) {
           if ((m >> (8 * e + d)) & 1u) sum[e] = add_rn(sum[e], mul_rn((XT)v[e], xv[e]));
       }
     }
+    if (io.shift != 0.0) {   // (A + shift I) x: + shift x_i after the row sum
+      XT xo[R];
+      load_opnd<XT>(io.x, i0, n, xo);
+#pragma unroll
+      for (int e = 0; e < R; ++e) sum[e] = add_rn(sum[e], mul_rn((XT)io.shift, xo[e]));
+    }
     XT y[R];
 #pragma unroll
     for (int e = 0; e < R; ++e) y[e] = io.mode == 1 ? add_rn(bv[e], -sum[e]) : sum[e];

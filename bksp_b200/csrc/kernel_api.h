@@ -125,6 +125,10 @@ struct SpmvH {
   int mode;   // 0: y = A x   1: y = b - A x
   int nd;
   unsigned char dot[kMaxDotsApi][2];   // 0 = y, 1 = b, 2 = w0, 3 = w1
+  // A + shift I instead of A (the row sum, then + shift x_i); only the
+  // diagonal-form and tile kernels take it (the dispatch picks the tile
+  // kernel for the others).
+  double shift;
 };
 
 // Diagonal-form product with its neighbouring vector updates fused in
@@ -243,6 +247,7 @@ struct ShiftArgsH {
   double* ps;
   long long np;
   int ns, l, j, mode;
+  float* ps32;   // non-null: the p_k are stored in FP32 here (ps unused)
 };
 void launch_shift(const ShiftArgsH& a, const RedH& rd, cudaStream_t st);
 // Block methods (k_block.cuh): row-major n x s blocks, s <= 16.

@@ -20,12 +20,22 @@ namespace bk {
 void launch_shift(const ShiftArgsH& a, const RedH& rd, cudaStream_t st) {
   if (g_prog_rec) prog_unsupported("block / shifted kernel");
   ++launch_count();
-  ShiftArgs s{a.r, a.p, a.x, a.xs, a.ps, a.np, a.ns, a.l, a.j, a.mode};
+  if (a.ps32) {
+    ShiftArgs<float> s{a.r, a.p, a.x, a.xs, a.ps32, a.np, a.ns, a.l, a.j, a.mode};
+    switch (a.mode) {
+      case 0: launch_k(k_shift<0, float>, grid_wave(k_shift<0, float>, a.np), kThreads, 0, st, s, rd); break;
+      case 1: launch_k(k_shift<1, float>, grid_wave(k_shift<1, float>, a.np), kThreads, 0, st, s, rd); break;
+      case 2: launch_k(k_shift<2, float>, grid_wave(k_shift<2, float>, a.np), kThreads, 0, st, s, rd); break;
+      default: launch_k(k_shift<3, float>, grid_wave(k_shift<3, float>, a.np), kThreads, 0, st, s, rd); break;
+    }
+    return;
+  }
+  ShiftArgs<double> s{a.r, a.p, a.x, a.xs, a.ps, a.np, a.ns, a.l, a.j, a.mode};
   switch (a.mode) {
-    case 0: launch_k(k_shift<0>, grid_wave(k_shift<0>, a.np), kThreads, 0, st, s, rd); break;
-    case 1: launch_k(k_shift<1>, grid_wave(k_shift<1>, a.np), kThreads, 0, st, s, rd); break;
-    case 2: launch_k(k_shift<2>, grid_wave(k_shift<2>, a.np), kThreads, 0, st, s, rd); break;
-    default: launch_k(k_shift<3>, grid_wave(k_shift<3>, a.np), kThreads, 0, st, s, rd); break;
+    case 0: launch_k(k_shift<0, double>, grid_wave(k_shift<0, double>, a.np), kThreads, 0, st, s, rd); break;
+    case 1: launch_k(k_shift<1, double>, grid_wave(k_shift<1, double>, a.np), kThreads, 0, st, s, rd); break;
+    case 2: launch_k(k_shift<2, double>, grid_wave(k_shift<2, double>, a.np), kThreads, 0, st, s, rd); break;
+    default: launch_k(k_shift<3, double>, grid_wave(k_shift<3, double>, a.np), kThreads, 0, st, s, rd); break;
   }
 }
 

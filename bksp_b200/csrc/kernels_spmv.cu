@@ -156,9 +156,12 @@ static void spmv_dispatch(const CsrH& A, const SpmvH<XT>& io, const RedH& rd,
   int var = spmv_override();
   if (var < 0) var = A.variant;
   if (g_prog_rec) {
+    if (io.shift != 0.0) prog_unsupported("shifted product");
     spmv_record<VT, XT>(A, io, rd, var);
     return;
   }
+  // A shifted product runs on the diagonal-form or tile kernel only.
+  if (io.shift != 0.0 && var != 7) var = 0;
   if (var == 7) {
     if (dia_usable(A, io)) {
       byte_count() += spmv_bytes<VT, XT>(A, io, true);

@@ -561,9 +561,36 @@ BlockMixedOut block_mixed(int method, const DevCsr& A, const double* B,
     used += o.ret >= 0 ? o.ret + 1 : o.iters;
     out.inner_iters = used;
     ++out.sweeps;
-    if (o.ret == kDivergence) {   // the FP32 inner solve broke down: keep X
-      out.ret = kDivergence;
-      break;
+    if (o.ret == kDivergence) {
+      // The FP32 inner solve broke down (Krylov blocks whose conditioning
+      // FP32 cannot represent): this sweep's correction in FP64 instead.
+      double* E64 = dalloc_n<double>(ne, st);
+      BK_CHECK(cudaMemsetAsync(E64, 0, sizeof(double) * ne, st));
+      SolveOut o64;
+      {
+        BlockCtx bc(n, s, ss, st);
+        const int budget = max_iter - used;
+        if (method == 0)
+          o64 = blcg<double>(bc, A, R64, E64, inner_tol, budget);
+        else
+          o64 = blbicgstabl<double>(bc, A, R64, E64, l, inner_tol, budget, nullptr);
+        bc.release();
+      }
+      used += o64.ret >= 0 ? o64.ret + 1 : o64.iters;
+      out.inner_iters = used;
+      ++out.fp64_sweeps;
+      if (o64.ret == kDivergence) {
+        dfree(E64, st);
+        out.ret = kDivergence;
+        break;
+      }
+      Lc<double> u(ne);
+      const int ix = u.in(X), ie = u.in(E64);
+      const int ox = u.out(X);
+      u.term(ox, ix, cf_const(1)).term(ox, ie, cf_const(1));
+      u.launch(ss.red_after(kD, E_NONE), st);
+      dfree(E64, st);
+      continue;
     }
     launch_mx_accum(X, E32, E32, ne, ss.red_after(kD, E_NONE), st);
     BK_CHECK(cudaGetLastError());

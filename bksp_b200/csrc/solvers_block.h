@@ -56,6 +56,7 @@ SolveOut blbicgstabl(BlockCtx& bc, const DevCsr& A, const T* B, T* X, int l,
 struct BlockMixedOut {
   int ret = kNotConverged;
   int sweeps = 0;
+  int fp64_sweeps = 0;   // sweeps whose FP32 inner solve broke down
   int inner_iters = 0;
   double true_res = 0.0;
 };

@@ -12,6 +12,7 @@
 //     captured iteration, behind a device-side guard;
 //   * convergence is decided on that FP64 true residual only.
 #include <algorithm>
+#include <cmath>
 #include <cstdlib>
 #include <cstring>
 
@@ -62,10 +63,12 @@ MixedOut bicgstabl_mixed(const DevCsr& A, const DevCsr* M, const double* b,
   ss.set_scalar(kMxPeriod, (double)std::max(1, o.period), st);
 
   // r64 = b - A x0 (FP64), ||b||; r0 = p0 = rs = fl32(r64), (rs, r0).
+  // (A + o.shift I throughout when a shift is given.)
   {
     SpmvH<double> io = spmv_io<double>(x, r64);
     io.b = b;
     io.mode = 1;
+    io.shift = o.shift;
     set_dot(io, 0, Y, Y);
     set_dot(io, 1, B, B);
     spmv(A, io, ss.red(kD, E_MX_INIT), st);
@@ -80,6 +83,7 @@ MixedOut bicgstabl_mixed(const DevCsr& A, const DevCsr* M, const double* b,
       src = t;
     }
     SpmvH<float> io = spmv_io<float>(src, dst);
+    io.shift = o.shift;
     if (dot) {
       io.w0 = rs;
       set_dot(io, 0, W0, Y);
@@ -209,6 +213,7 @@ MixedOut bicgstabl_mixed(const DevCsr& A, const DevCsr* M, const double* b,
         SpmvH<double> io = spmv_io<double>(x, r64);
         io.b = b;
         io.mode = 1;
+        io.shift = o.shift;
         set_dot(io, 0, Y, Y);
         spmv(A, io, ss.red_if(kMxDoRep, kD, E_MX_TRUE), s2);
       }
@@ -484,6 +489,62 @@ MixedOut cg_mixed(const DevCsr& A, const DevCsr* M, const double* b, double* x,
   out.true_res = ss.get_scalar(kMxTrue, st);
   dfree(w, st);
   dfree(r64, st);
+  return out;
+}
+
+// FP64 ||b - (A + shift I) x|| / ||b|| of padded device vectors.
+static double shifted_residual(const DevCsr& A, const double* b, const double* x,
+                               double shift, cudaStream_t st) {
+  const long long np = pad64(A.n);
+  double* r = dalloc_n<double>(np, st);
+  SolveState t;
+  t.create(0, st);
+  t.start(0, 1, 0.0, st);
+  SpmvH<double> io = spmv_io<double>(x, r);
+  io.b = b;
+  io.mode = 1;
+  io.shift = shift;
+  set_dot(io, 0, Y, Y);
+  set_dot(io, 1, B, B);
+  spmv(A, io, t.red(kD, E_NONE), st);
+  const double rr = t.get_scalar(kD, st), bb = t.get_scalar(kD + 1, st);
+  t.release(st);
+  dfree(r, st);
+  return std::sqrt(rr) / std::sqrt(bb);
+}
+
+MixedOut shbicgstabl_mixed(const DevCsr& A, const double* b, int l,
+                           const double* sigma_host, int ns, double* x,
+                           double target, int max_iter, SolveState& ss,
+                           cudaStream_t st) {
+  if (!A.v32) throw CudaError("mixed solve: FP32 values missing");
+  MixedOut out;
+  const SolveOut o = shbicgstabl(A, b, l, sigma_host, ns, x, target, max_iter, ss,
+                                 st, /*fp32_ps=*/true);
+  out.ret = o.ret;
+  out.iters = 0;
+  const long long np = pad64(A.n);
+  double worst = 0.0;
+  for (int k = -1; k < ns; ++k) {
+    const double sg = k < 0 ? 0.0 : sigma_host[k];
+    double* xk = x + (long long)(k + 1) * np;
+    double res = shifted_residual(A, b, xk, sg, st);
+    if (!(res <= target)) {
+      MixedOpts mo;
+      mo.target = target;
+      mo.shift = sg;
+      SolveState ps;
+      ps.create(0, st);
+      const MixedOut p = bicgstabl_mixed(A, nullptr, b, l, xk, max_iter, mo, ps, st);
+      ps.release(st);
+      out.iters += p.iters;
+      out.replacements += p.replacements;
+      res = p.true_res;
+      if (p.ret < 0 && out.ret >= 0) out.ret = kNotConverged;
+    }
+    worst = std::isfinite(res) ? std::max(worst, res) : res;
+  }
+  out.true_res = worst;
   return out;
 }
 

@@ -99,7 +99,8 @@ SolveOut shbicg(const DevCsr& A, const DevCsr& At, const double* b,
 // --------------------------------------------------- shifted BiCGSTAB(l)
 SolveOut shbicgstabl(const DevCsr& A, const double* b, int l,
                      const double* sigma_host, int ns, double* x, double tol,
-                     int max_iter, SolveState& ss, cudaStream_t st) {
+                     int max_iter, SolveState& ss, cudaStream_t st,
+                     bool fp32_ps) {
   if (l < 1 || l > kBlMaxL) throw CudaError("shbicgstabl: l out of range");
   if (ns < 0 || ns > kMaxShifts) throw CudaError("shbicgstabl: too many shifts");
   SolveOut o;
@@ -108,7 +109,9 @@ SolveOut shbicgstabl(const DevCsr& A, const double* b, int l,
   auto R = [&](int i) { return w + i * np; };
   auto P = [&](int i) { return w + (l + 1 + i) * np; };
   double* rs = w + 2 * (l + 1) * np;
-  double* ps = zeros<double>((long long)std::max(ns, 1) * (l + 1) * np, st);
+  const long long nps = (long long)std::max(ns, 1) * (l + 1) * np;
+  double* ps = fp32_ps ? nullptr : zeros<double>(nps, st);
+  float* ps32 = fp32_ps ? zeros<float>(nps, st) : nullptr;
   ss.start(0, max_iter, tol, st);
   ss.set_scalar(kL, (double)l, st);
   ss.set_scalar(kNs, (double)ns, st);
@@ -146,7 +149,7 @@ SolveOut shbicgstabl(const DevCsr& A, const double* b, int l,
           spmv(A, a, ss.red(kD, E_SHL_ALPHA), s);
         }
         {  // :108, :123-133  x, p_k[0..j+1], x_k
-          ShiftArgsH sa{R(0), P(0), x, x + np, ps, np, ns, l, j, 1};
+          ShiftArgsH sa{R(0), P(0), x, x + np, ps, np, ns, l, j, 1, ps32};
           launch_shift(sa, ss.red(kD, E_NONE), s);
         }
         {  // :137-139  r_i -= alpha p_{i+1}
@@ -168,7 +171,7 @@ SolveOut shbicgstabl(const DevCsr& A, const double* b, int l,
           }
         }
         {  // :146-161  p_k[j+1] completion, then scalar rotation
-          ShiftArgsH sa{R(0), P(0), x, x + np, ps, np, ns, l, j, 2};
+          ShiftArgsH sa{R(0), P(0), x, x + np, ps, np, ns, l, j, 2, ps32};
           launch_shift(sa, ss.red(kD, E_SHL_ROTATE, j + 1 < l ? 1 : 0), s);
         }
       }
@@ -221,7 +224,7 @@ SolveOut shbicgstabl(const DevCsr& A, const double* b, int l,
         u.launch(ss.red(kD, E_NONE), s);
       }
       {  // :202-237  every shift's x_k and p_k[0]
-        ShiftArgsH sa{R(0), P(0), x, x + np, ps, np, ns, l, 0, 3};
+        ShiftArgsH sa{R(0), P(0), x, x + np, ps, np, ns, l, 0, 3, ps32};
         launch_shift(sa, ss.red(kD, E_NONE), s);
       }
       {  // :240-247  seed r0, error test; next rho / beta (:88-92)
@@ -243,6 +246,7 @@ SolveOut shbicgstabl(const DevCsr& A, const double* b, int l,
   }
   dfree(w, st);
   dfree(ps, st);
+  dfree(ps32, st);
   return o;
 }
 

@@ -245,6 +245,21 @@ int bksp_dblcg_mixed(dspmat *A, dmat *B, const bksp_gpu_mixed_opts *opts,
 int bksp_dblbicgstabl_mixed(dspmat *A, dmat *B, const bksp_gpu_mixed_opts *opts,
                             dmat *X);
 
+/* Shifted BiCGSTAB(l) (l = opts->l) in mixed precision, with dshbicgstabl's
+ * host arrays (x: n * (sigma_size + 1) values, seed first, shifted parts
+ * zero on entry): the shifted solve stores the per-shift direction vectors
+ * p_k -- its bulk traffic -- in FP32 (seed vectors, x_k and every scalar in
+ * FP64) and runs to the seed tolerance opts->target; then each system
+ * (A + sigma_k I) x_k = b, and the seed, whose FP64 true relative residual
+ * is above opts->target is polished from its x_k by the mixed-precision
+ * BiCGSTAB(l) on the shifted operator, so every solution ends at the FP64
+ * target.  (A shift-invariant Krylov space excludes a preconditioner:
+ * opts->precond and opts->model are not used.)  Returns the seed's
+ * converging iteration, NOT_CONVERGED (a solve or polish missed the
+ * target), DIVERGENCE or INVALID_PARAMETERS. */
+int bksp_dshbicgstabl_mixed(dspmat *A, double *b, double *sigma, int sigma_size,
+                            const bksp_gpu_mixed_opts *opts, double *x);
+
 /* ------------------------------------------------------------ batches */
 
 /* Many independent systems in one call, each solved as bksp_gpu_solve_mixed
