@@ -319,6 +319,8 @@ def record(hist_cap=0):
         out["true_res"] = st.true_res
         out["launches"] = st.launches
         out["alg_bytes"] = st.alg_bytes
+        out["inner_iters"] = st.inner_iters
+        out["sweeps"] = st.sweeps
 
 
 def version():

@@ -73,6 +73,9 @@ k_shift(ShiftArgs<PT> a, Red rd) {
     if (MODE == 0) {
       r[0] = a.r[i];
       a.x[i] = fma_rn(alpha, a.p[i], a.x[i]);
+      // Four shifts per pass: their loads are in flight together (one
+      // shift at a time left the kernel bound by load latency).
+#pragma unroll 4
       for (int k = 0; k < ns; ++k) {
         PT* pk = a.ps + (long long)k * np;
         const double pv = (double)(PT)fma_rn(c1[k], r[0], mul_rn(c0[k], (double)pk[i]));
@@ -83,6 +86,9 @@ k_shift(ShiftArgs<PT> a, Red rd) {
     } else if (MODE == 1) {
       for (int q = 0; q <= j; ++q) r[q] = a.r[q * np + i];
       a.x[i] = fma_rn(alpha, a.p[i], a.x[i]);
+      // Four shifts per pass: their loads are in flight together (one
+      // shift at a time left the kernel bound by load latency).
+#pragma unroll 4
       for (int k = 0; k < ns; ++k) {
         PT* pk = a.ps + (long long)k * (l + 1) * np;
         double p0 = 0.0;
@@ -98,6 +104,9 @@ k_shift(ShiftArgs<PT> a, Red rd) {
       }
     } else if (MODE == 2) {
       const double rj = a.r[j * np + i];
+      // Four shifts per pass: their loads are in flight together (one
+      // shift at a time left the kernel bound by load latency).
+#pragma unroll 4
       for (int k = 0; k < ns; ++k) {
         PT* pk = a.ps + (long long)k * (l + 1) * np;
         double v = fma_rn(c0[k], rj, (double)pk[(j + 1) * np + i]);
@@ -106,6 +115,9 @@ k_shift(ShiftArgs<PT> a, Red rd) {
       }
     } else {
       for (int q = 0; q < l; ++q) r[q] = a.r[q * np + i];
+      // Four shifts per pass: their loads are in flight together (one
+      // shift at a time left the kernel bound by load latency).
+#pragma unroll 4
       for (int k = 0; k < ns; ++k) {
         PT* pk = a.ps + (long long)k * (l + 1) * np;
         double* xk = a.xs + (long long)k * np;
