@@ -76,7 +76,8 @@ def args_():
                    help=argparse.SUPPRESS)
     p.add_argument("--x-out", default=None, help=argparse.SUPPRESS)
     p.add_argument("--profile", default=None,
-                   choices=["plain_fp64", "mixed_none", "mixed_learned", "spmv"],
+                   choices=["plain_fp64", "mixed_none", "mixed_learned", "spmv",
+                            "block_cg", "persist_cg"],
                    help="profiling driver: set up, run one warm solve, then "
                         "one solve (or SpMV launches) between "
                         "cudaProfilerStart/Stop, print nothing else")
@@ -785,65 +786,194 @@ def run_batch(a):
 
 
 def run_configs(a):
-    """The survey's configurations 1, 3 and 4 through the drop-in bksp.h
-    calls (host arrays: upload, device solve, download), each timed on its
-    second call: CG on the 2D Poisson 64^2 operator in one-triangle storage
-    (tol 1e-10, also timed with the compiled reference); Block CG and Block
-    BiCGSTAB(2) with 16 right-hand sides on 3D Poisson 64^3 and 128^3 (tol
-    1e-8); shifted BiCGSTAB(4) with 32 shifts 10^-3..1 on the 2D
-    convection-diffusion 1024^2 operator (tol 1e-8)."""
+    """The survey's configurations 1, 3 and 4, each as plain FP64 against
+    mixed precision, both to an FP64 true relative residual of 1e-8 (every
+    column / every shift):
+
+    * cfg 1: CG on the 2D Poisson 64^2 operator (b ~ U[-1,1], seed 0),
+      device-resident (CUDA events, median of five) and through the bksp.h
+      host-array calls (one triangle stored); mixed = FP32 vectors, FP64
+      reliable replacement, the learned preconditioner symmetrised (trained
+      beforehand on 16^2..32^2 Poisson systems, outside the timing); the
+      compiled reference's bksp_dcg beside it;
+    * cfg 3: Block CG and Block BiCGSTAB(2), 16 Gaussian right-hand sides
+      (seed 2), 3D Poisson 64^3 and 128^3, through dblcg / dblbicgstabl and
+      their mixed counterparts (FP64 refinement around FP32 inner solves);
+    * cfg 4: shifted BiCGSTAB(4), 32 shifts 1e-3..1, 2D convection-diffusion
+      1024^2, dshbicgstabl against bksp_dshbicgstabl_mixed (FP32 shift
+      vectors, per-shift FP64 polishing).
+
+    Prints one JSON line; worst residuals are recomputed on the host in FP64."""
     import scipy.sparse as sp
+    import torch
     import bksp_b200 as B
     from bksp_b200 import problems as P
     res = {}
 
-    def run(name, fn, reps=2):
+    def host_run(fn, reps=2):
         for _ in range(reps):
             with B.record() as st:
                 t0 = time.perf_counter()
                 r = fn()
                 dt = time.perf_counter() - t0
-        res[name] = {"ret": r, "e2e_s": dt, "solve_s": st["solve_ms"] / 1e3}
+        return r, dt, st
+
+    def pair(name, plain, mixed):
+        p_, m_ = res[name]["plain_fp64"], res[name]["mixed"]
+        res[name]["speedup_mixed_vs_plain"] = p_["solve_s"] / m_["solve_s"]
         log(f"{name}: {res[name]}")
 
+    # ---- cfg 1
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    sp_ = stream.cuda_stream
     rp, c, v, n = P.poisson2d(64)
-    lrp, lc, lv, _ = P.lower_triangle(rp, c, v, n)
+    A = sp.csr_matrix((v, c, rp), shape=(n, n))
     b = P.uniform(n, 0)
+    mats = [B.GpuMatrix(B.CsrMatrix(*P.poisson2d(k)[:3]), B.FP32) for k in (16, 24, 32)]
+    model = B.SpaiModel(seed=5)
+    model.train(mats, epochs=150, probes=8, lr=3e-3, seed=9)
+    for m_ in mats:
+        m_.close()
+    G = B.GpuMatrix(B.CsrMatrix(rp, c, v), B.FP32)
+    bd = torch.from_numpy(b).cuda()
+    xd = torch.zeros_like(bd)
+
+    def dev_time(f, k=5):
+        for _ in range(3):
+            f()
+        ms = []
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        for _ in range(k):
+            e0.record(stream)
+            r = f()
+            e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        return float(np.median(ms)) / 1e3, r
+
+    def resid(x):
+        return float(np.linalg.norm(b - A @ x) / np.linalg.norm(b))
+
+    def plain1():
+        xd.zero_()
+        return G.solve(B.CG, bd.data_ptr(), xd.data_ptr(), 1e-8, 10000, stream=sp_)
+    t, (r, st) = dev_time(plain1)
+    e1 = {"solve_s": t, "ret": r, "true_residual": resid(xd.cpu().numpy()),
+          "launches": st["launches"]}
+    out = {}
+    for pc, nm in ((0, "mixed_none"), (2, "mixed")):
+        def mixed1():
+            xd.zero_()
+            return G.solve_mixed(bd.data_ptr(), xd.data_ptr(), target=1e-8, precond=pc,
+                                 model=model, stream=sp_, method="cg")
+        t, (r, st) = dev_time(mixed1)
+        out[nm] = {"solve_s": t, "ret": r, "true_residual": resid(xd.cpu().numpy()),
+                   "launches": st["launches"], "replacements": st["replacements"]}
+    lrp, lc, lv, _ = P.lower_triangle(rp, c, v, n)
     A1 = B.CsrMatrix(lrp, lc, lv, symmetric=True)
-    run("cfg1_cg_poisson64", lambda: B.bksp_dcg(A1, b, 1e-10, 10000, np.zeros(n)))
+    xh = np.zeros(n)
+    r, dt, _ = host_run(lambda: (xh.fill(0.0), B.bksp_dcg(A1, b, 1e-8, 10000, xh))[1])
+    e1["e2e_s"] = dt
+    xh2 = np.zeros(n)
+    r, dt, _ = host_run(lambda: (xh2.fill(0.0), B.dcg_mixed(A1, b, xh2, precond=B.PRECOND_LEARNED,
+                                                           model=model))[1])
+    out["mixed"]["e2e_s"] = dt
+    res["cfg1_cg_poisson64"] = {"plain_fp64": e1, **out}
     from oracle import ref as R
     if R.available():
         Ar = R.Matrix(lrp, lc, lv, n, symmetric=True)
         t0 = time.perf_counter()
-        r = R.call("bksp_dcg", Ar, b, 1e-10, 10000, np.zeros(n))[0]
-        res["cfg1_cg_poisson64_reference"] = {"ret": int(r), "s": time.perf_counter() - t0}
+        r = R.call("bksp_dcg", Ar, b, 1e-8, 10000, np.zeros(n))[0]
+        res["cfg1_cg_poisson64"]["reference_cpu"] = {"ret": int(r), "s": time.perf_counter() - t0}
+    pair("cfg1_cg_poisson64", None, None)
+    G.close()
+    model.close()
+
+    # ---- cfg 3
     for nx in (64, 128):
         rp, c, v, n = P.poisson3d(nx)
         lrp, lc, lv, _ = P.lower_triangle(rp, c, v, n)
+        Af = sp.csr_matrix((v, c, rp), shape=(n, n))
         Bm = np.random.default_rng(2).standard_normal((n, 16))
         As = B.CsrMatrix(lrp, lc, lv, symmetric=True)
         Ag = B.CsrMatrix(rp, c, v)
-        run(f"cfg3_blcg_poisson{nx}", lambda: B.dblcg(As, Bm, 1e-8, 5000, np.zeros((n, 16))), 1)
-        X = np.zeros((n, 16))
-        run(f"cfg3_blbicgstabl2_poisson{nx}", lambda: B.dblbicgstabl(Ag, Bm, 2, 1e-8, 5000, X), 1)
-        Af = sp.csr_matrix((v, c, rp), shape=(n, n))
-        res[f"cfg3_blbicgstabl2_poisson{nx}"]["worst_true_residual"] = float(max(
-            np.linalg.norm(Bm[:, k] - Af @ X[:, k]) / np.linalg.norm(Bm[:, k]) for k in range(16)))
+
+        def worst(X):
+            return float(max(np.linalg.norm(Bm[:, k] - Af @ X[:, k]) / np.linalg.norm(Bm[:, k])
+                             for k in range(16)))
+        for meth, plain, mixed in (
+                ("blcg", lambda X: B.dblcg(As, Bm, 1e-8, 5000, X),
+                 lambda X: B.dblcg_mixed(As, Bm, X, inner_tol=1e-3)),
+                ("blbicgstabl2", lambda X: B.dblbicgstabl(Ag, Bm, 2, 1e-8, 5000, X),
+                 lambda X: B.dblbicgstabl_mixed(Ag, Bm, 2, X, inner_tol=1e-3))):
+            name = f"cfg3_{meth}_poisson{nx}"
+            res[name] = {}
+            for mode, fn in (("plain_fp64", plain), ("mixed", mixed)):
+                X = np.zeros((n, 16))
+                r, dt, st = host_run(lambda: (X.fill(0.0), fn(X))[1], reps=1)
+                res[name][mode] = {"ret": r, "solve_s": st["solve_ms"] / 1e3, "e2e_s": dt,
+                                   "worst_true_residual": worst(X)}
+            pair(name, None, None)
+
+    # ---- cfg 4
     rp, c, v, n = P.convdiff2d(1024)
+    Af = sp.csr_matrix((v, c, rp), shape=(n, n))
     b = P.uniform(n, 3)
     sig = P.log_shifts(32)
     A4 = B.CsrMatrix(rp, c, v)
-    x = np.zeros(33 * n)
+    nb = np.linalg.norm(b)
 
-    def shifted():
-        x[:] = 0.0
-        return B.dshbicgstabl(A4, b, 4, sig, 1e-8, 5000, x)
-    run("cfg4_shbicgstabl4_convdiff1024_32shifts", shifted, 1)
-    Af = sp.csr_matrix((v, c, rp), shape=(n, n))
-    res["cfg4_shbicgstabl4_convdiff1024_32shifts"]["worst_true_residual"] = float(max(
-        np.linalg.norm(b - (Af @ x[(k + 1) * n:(k + 2) * n] + s_ * x[(k + 1) * n:(k + 2) * n]))
-        / np.linalg.norm(b) for k, s_ in enumerate(sig)))
-    print(json.dumps({"workload": "configs", "unit": "s", "results": res}), flush=True)
+    def worst4(x):
+        r_ = [np.linalg.norm(b - Af @ x[:n]) / nb] + [
+            np.linalg.norm(b - (Af @ x[(k + 1) * n:(k + 2) * n] + s_ * x[(k + 1) * n:(k + 2) * n])) / nb
+            for k, s_ in enumerate(sig)]
+        return float(max(r_))
+    name = "cfg4_shbicgstabl4_convdiff1024_32shifts"
+    res[name] = {}
+    for mode, fn in (("plain_fp64", lambda x: B.dshbicgstabl(A4, b, 4, sig, 1e-8, 5000, x)),
+                     ("mixed", lambda x: B.dshbicgstabl_mixed(A4, b, 4, sig, x))):
+        x = np.zeros(33 * n)
+        r, dt, st = host_run(lambda: (x.fill(0.0), fn(x))[1])
+        res[name][mode] = {"ret": r, "solve_s": st["solve_ms"] / 1e3, "e2e_s": dt,
+                           "worst_true_residual": worst4(x),
+                           "polish_iterations": st["inner_iters"] if mode == "mixed" else 0}
+    pair(name, None, None)
+    print(json.dumps({"workload": "configs", "unit": "s",
+                      "metric": "time to 1e-8 FP64 true residual, plain FP64 vs mixed",
+                      "results": res}), flush=True)
+    return 0
+
+
+def profile_small(a):
+    """Profiling drivers that need no headline set-up: block_cg = five Block
+    CG iterations (16 Gaussian right-hand sides, 3D Poisson --nx^3; run with
+    BKSP_GPU_LOOP=poll so a launch list sees every kernel); persist_cg = one
+    CG solve of the 2D Poisson 64^2 system as a persistent launch."""
+    import bksp_b200 as B
+    P = problems_module()
+    if a.profile == "block_cg":
+        rp, c, v, n = P.poisson3d(a.nx)
+        lrp, lc, lv, _ = P.lower_triangle(rp, c, v, n)
+        Bm = np.random.default_rng(2).standard_normal((n, 16))
+        X = np.zeros((n, 16))
+        ret = B.dblcg(B.CsrMatrix(lrp, lc, lv, symmetric=True), Bm, 1e-8, 5, X)
+        print(f"profiled block_cg {a.nx}^3: ret {ret}", flush=True)
+        return 0
+    import torch
+    torch.cuda.set_device(0)
+    rp, c, v, n = P.poisson2d(64)
+    G = B.GpuMatrix(B.CsrMatrix(rp, c, v), B.FP32)
+    b = torch.from_numpy(P.uniform(n, 0)).cuda()
+    x = torch.zeros_like(b)
+    with B.loop_mode(1):
+        for _ in range(2):
+            x.zero_()
+            ret, st = G.solve(B.CG, b.data_ptr(), x.data_ptr(), 1e-10, 10000)
+    print(f"profiled persist_cg: ret {ret} launches {st['launches']}", flush=True)
+    G.close()
     return 0
 
 
@@ -851,6 +981,8 @@ def main():
     a = args_()
     if a.reference_solve_worker:
         return reference_solve_worker(a.nx, a.x_out)
+    if a.profile in ("block_cg", "persist_cg"):
+        return profile_small(a)
     if a.impl == "reference":
         return run_reference(a)
     if a.workload == "kappa_batch":
