@@ -618,7 +618,7 @@ def run_batch(a):
     f ~ N(0,1); time to an FP64 true relative residual of 1e-8 on every
     system.  value: mixed-precision BiCGSTAB(2) with the learned SPAI
     preconditioner (trained beforehand on 64 smaller systems of the same
-    family, seeds 1000+i), one CUDA-graph loop per system on eight host
+    family, seeds 1000+i, the configuration's 256), one CUDA-graph loop per system on eight host
     threads; plain_fp64_s: FP64 BiCGSTAB(2) on the Jacobi right-scaled
     systems A D^-1 y = b, x = D^-1 y, batched the same way; the modes also
     time both as one persistent launch for the whole batch (*_persistent)
@@ -662,7 +662,7 @@ def run_batch(a):
     upload_s = time.perf_counter() - t0
     t0 = time.perf_counter()
     model = B.SpaiModel(seed=3)
-    Ls = np.random.default_rng(999).integers(16, 33, 64)
+    Ls = np.random.default_rng(999).integers(16, 33, 256)
     train = [B.GpuMatrix(B.CsrMatrix(*P.kappa_diffusion3d(int(L), 1000 + i)[:3]), B.FP32)
              for i, L in enumerate(Ls)]
     loss = model.train(train, epochs=100, probes=8, lr=3e-3, seed=7)
@@ -770,7 +770,7 @@ def run_batch(a):
         "plain_fp64_s": res["plain_fp64"]["s"],
         "speedup_vs_plain_fp64": res["plain_fp64"]["s"] / res["mixed_learned"]["s"],
         "modes": res,
-        "spai_training": {"s": train_s, "final_loss": loss, "systems": "64 kappa, L U{16..32}",
+        "spai_training": {"s": train_s, "final_loss": loss, "systems": "256 kappa, L U{16..32}",
                           "epochs": 100, "probes": 8},
         "setup_s": {"generate": gen_s, "upload": upload_s},
         "clocks": clk.summary(),
