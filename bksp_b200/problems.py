@@ -81,6 +81,39 @@ def convdiff3d(nx):
     return stencil_csr(STENCIL_CONVDIFF3D, nx, nx, nx)
 
 
+def complex_convdiff2d(nx, seed=11, lo=0.2, hi=1.0):
+    """Complex non-Hermitian test operator: the 2D convection-diffusion
+    stencil plus a seeded imaginary absorption on the diagonal,
+    A = convdiff2d + i diag(d), d_i ~ U(lo, hi).  Values complex128."""
+    rowptr, col, val, n = convdiff2d(nx)
+    d = np.random.default_rng(seed).uniform(lo, hi, n)
+    rows = np.repeat(np.arange(n), np.diff(rowptr))
+    v = val.astype(np.complex128)
+    v[col == rows] += 1j * d
+    return rowptr, col, v, n
+
+
+def complex_convdiff3d(nx, seed=11, lo=0.2, hi=1.0):
+    """3D counterpart of ``complex_convdiff2d``."""
+    rowptr, col, val, n = convdiff3d(nx)
+    d = np.random.default_rng(seed).uniform(lo, hi, n)
+    rows = np.repeat(np.arange(n), np.diff(rowptr))
+    v = val.astype(np.complex128)
+    v[col == rows] += 1j * d
+    return rowptr, col, v, n
+
+
+def complex_uniform(n, seed):
+    """Seeded complex vector, real and imaginary parts U(-1, 1)."""
+    g = np.random.default_rng(seed)
+    return g.uniform(-1.0, 1.0, n) + 1j * g.uniform(-1.0, 1.0, n)
+
+
+def complex_shifts(count=8, lo=-3.0, hi=0.0, angle=0.25 * np.pi):
+    """sigma_k = 10^(lo + (hi-lo) k/(count-1)) e^{i angle}."""
+    return log_shifts(count, lo, hi) * np.exp(1j * angle)
+
+
 def csr_matvec(rowptr, col, val, x):
     """y = A x in float64 (host helper for building right-hand sides)."""
     n = rowptr.size - 1

@@ -24,6 +24,20 @@ double __wrap_cblas_dnrm2(const int n, const double *x, const int incx)
     return v;
 }
 
+/* The complex solvers' norms (src/bicg.c:159, src/bicgstabl.c:259, ...)
+ * go through cblas_dznrm2; they are recorded into the same buffer. */
+double __real_cblas_dznrm2(const int n, const void *x, const int incx);
+
+double __wrap_cblas_dznrm2(const int n, const void *x, const int incx)
+{
+    double v = __real_cblas_dznrm2(n, x, incx);
+    if (g_buf && g_len < g_cap)
+        g_buf[g_len] = v;
+    if (g_buf)
+        g_len++;
+    return v;
+}
+
 /* Zero-filled allocation for the reference's workspaces.
  *
  * dblcg reads its s-by-s beta block before writing the off-diagonal entries

@@ -174,3 +174,104 @@ def dhorner(gamma, l, sigma):
     g = _vec(gamma)
     lib().dhorner(g.ctypes.data_as(_dp), l, sigma, out.ctypes.data_as(_dp))
     return out
+
+
+# ------------------------------------------------------------ complex API
+
+class ZSpMat(C.Structure):
+    """Mirror of ``zspmat`` (include/bksp.h:115-124): complex values as
+    interleaved (re, im) doubles."""
+    _fields_ = [("row", _ip), ("col", _ip), ("nnz", _ip),
+                ("row_size", _ip), ("col_size", _ip), ("value", _dp),
+                ("format", C.c_char_p), ("type", C.c_char_p)]
+
+
+class ZMat(C.Structure):
+    """Mirror of ``zmat`` (include/bksp.h:126-130), column-major."""
+    _fields_ = [("row_size", C.c_int), ("col_size", C.c_int), ("value", _dp)]
+
+
+class ZMatrix:
+    """Keeps the NumPy buffers of a ``zspmat`` alive while C uses them."""
+
+    def __init__(self, rowptr, col, val, n):
+        self.rowptr = np.ascontiguousarray(rowptr, dtype=np.int32)
+        self.col = np.ascontiguousarray(col, dtype=np.int32)
+        self.val = np.ascontiguousarray(val, dtype=np.complex128)
+        self._nnz = C.c_int(int(self.col.size))
+        self._n = C.c_int(int(n))
+        self._m = C.c_int(int(n))
+        self.s = ZSpMat(self.rowptr.ctypes.data_as(_ip),
+                        self.col.ctypes.data_as(_ip), C.pointer(self._nnz),
+                        C.pointer(self._n), C.pointer(self._m),
+                        self.val.ctypes.data_as(_dp), b"csr", b"unsymmetric")
+
+    @property
+    def ptr(self):
+        return C.byref(self.s)
+
+
+_zsig_done = False
+
+
+def _zlib():
+    global _zsig_done
+    L = lib()
+    if not _zsig_done:
+        zp, zm = C.POINTER(ZSpMat), C.POINTER(ZMat)
+        d, i = C.c_double, C.c_int
+        sig = {
+            "zbicg": [zp, _dp, d, i, _dp],
+            "zbicgstabl": [zp, _dp, i, d, i, _dp],
+            "zblbicgstabl": [zp, zm, i, d, i, zm],
+            "zshbicgstabl": [zp, _dp, i, _dp, i, d, i, _dp],
+            "zcsrgemm0": [C.c_char, i, i, _dp, _ip, _ip, i, _dp, _dp],
+            "zqreco": [i, i, _dp, _dp],
+        }
+        for name, argt in sig.items():
+            f = getattr(L, name)
+            f.argtypes = argt
+            f.restype = C.c_int
+        _zsig_done = True
+    return L
+
+
+def zcall(name, A, *args, log_cap=1 << 20):
+    """Run complex reference solver ``name`` on ZMatrix ``A``.
+
+    Like ``call``: 1-D arrays become ``double _Complex*`` (copied), 2-D
+    arrays column-major ``zmat``; returns ``(ret, outputs, norms)`` with
+    every ``cblas_dznrm2`` / ``cblas_dnrm2`` value of the call."""
+    L = _zlib()
+    cargs, outs, keep = [], [], []
+    for a in args:
+        if isinstance(a, np.ndarray) and a.ndim == 2:
+            buf = np.asfortranarray(a, dtype=np.complex128).copy(order="F")
+            zm = ZMat(buf.shape[0], buf.shape[1], buf.ctypes.data_as(_dp))
+            keep.append((buf, zm))
+            outs.append(buf)
+            cargs.append(C.byref(zm))
+        elif isinstance(a, np.ndarray):
+            buf = np.ascontiguousarray(a, dtype=np.complex128).copy()
+            keep.append(buf)
+            outs.append(buf)
+            cargs.append(buf.ctypes.data_as(_dp))
+        else:
+            cargs.append(a)
+    log = np.zeros(log_cap)
+    with _lock:
+        L.oracle_nrm2_log_begin(log.ctypes.data_as(_dp), log_cap)
+        ret = getattr(L, name)(A.ptr, *cargs)
+        cnt = L.oracle_nrm2_log_end()
+    return ret, outs, log[:min(cnt, log_cap)].copy()
+
+
+def zspmv(A, x, trans=False):
+    """Reference ``zcsrgemm0`` (src/matvec.c:55-98): y = A x, or A^H x."""
+    x = np.ascontiguousarray(x, dtype=np.complex128)
+    y = np.zeros(A._n.value, dtype=np.complex128)
+    _zlib().zcsrgemm0(b"t" if trans else b"n", A._n.value, 1,
+                      A.val.ctypes.data_as(_dp), A.rowptr.ctypes.data_as(_ip),
+                      A.col.ctypes.data_as(_ip), A._nnz.value,
+                      x.ctypes.data_as(_dp), y.ctypes.data_as(_dp))
+    return y

@@ -3,6 +3,7 @@ that has the reference sources; the outputs are committed).
 
     make -C oracle && OPENBLAS_NUM_THREADS=1 python tests/golden/make_golden.py
     OPENBLAS_NUM_THREADS=8 OMP_NUM_THREADS=8 python tests/golden/make_golden.py --full
+    OPENBLAS_NUM_THREADS=1 python tests/golden/make_golden.py --complex
 
 * ``testmats.npz`` -- the reference's two test matrices (testmat/bfwb398.mtx,
   symmetric, one triangle; testmat/pde2961.mtx, general) as read by the
@@ -17,6 +18,11 @@ that has the reference sources; the outputs are committed).
 * ``reference_full.json`` (``--full``) -- the same records at the full sizes
   of the block and shifted benchmark configurations (3D Poisson 64^3 with 16
   right-hand sides; 2D convection-diffusion 1024^2 with 32 shifts).
+* ``reference_z.json`` (``--complex``) -- the complex solvers zbicg,
+  zshbicgstabl and zblbicgstabl on seeded complex problems
+  (bksp_b200.problems.complex_*).  zbicgstabl is not recorded: its unit
+  coefficient is a real ``double`` read as a complex scalar
+  (src/bicgstabl.c:147, 178, 196), so its result depends on stack contents.
 """
 import ctypes as C
 import json
@@ -192,8 +198,59 @@ def main_full():
         json.dump(out, f, indent=1)
 
 
+def zrecord(out, key, Aref, Aop, b, name, args, kind, sigma=None):
+    from oracle import zsolvers as Z
+    ret, outs, norms = R.zcall(name, Aref, *args)
+    xs = outs[-1]
+    h = hist_of(norms)
+    rec = {"ret": int(ret), "xnorm": float(np.linalg.norm(xs))}
+    if kind == "single":
+        rec["hist"] = h
+        rec["true_res"] = Z.true_residual(Aop, b, xs)
+    elif kind == "block":
+        Bm = args[0]
+        rec["hist"] = h[:-1]                # last norm: printed true residual
+        rec["true_res_cols"] = [float(np.linalg.norm(Bm[:, j] - Aop @ xs[:, j])
+                                      / np.linalg.norm(Bm[:, j]))
+                                for j in range(Bm.shape[1])]
+    else:
+        n = b.size
+        rec["hist"] = h
+        rec["true_res_seed"] = Z.true_residual(Aop, b, xs[:n])
+        rec["true_res_shifts"] = [Z.true_residual(Aop, b, xs[(k + 1) * n:(k + 2) * n], sg)
+                                  for k, sg in enumerate(sigma)]
+    out[key] = rec
+    print(f"{key:28s} ret={ret}")
+
+
+def main_complex():
+    out = {"threads": os.environ.get("OPENBLAS_NUM_THREADS", "default")}
+    for tag, gen, nx in (("cd2d24", P.complex_convdiff2d, 24),
+                         ("cd3d10", P.complex_convdiff3d, 10)):
+        rp, c, v, n = gen(nx)
+        Aop = csr(rp, c, v, n)
+        Ar = R.ZMatrix(rp, c, v, n)
+        b = P.complex_uniform(n, 3)
+        zrecord(out, f"zbicg/{tag}", Ar, Aop, b, "zbicg",
+                (b, 1e-10, 1000, np.zeros(n, complex)), "single")
+        sig = P.complex_shifts(4)
+        for l in (1, 2, 4):
+            zrecord(out, f"zshbicgstabl{l}/{tag}", Ar, Aop, b, "zshbicgstabl",
+                    (b, l, sig, 4, 1e-10, 1000, np.zeros(5 * n, complex)),
+                    "shift", sigma=sig)
+        rng = np.random.default_rng(7)
+        Bm = rng.uniform(-1, 1, (n, 4)) + 1j * rng.uniform(-1, 1, (n, 4))
+        for l in (1, 2, 4):
+            zrecord(out, f"zblbicgstabl{l}/{tag}", Ar, Aop, None, "zblbicgstabl",
+                    (Bm, l, 1e-10, 1000, np.zeros((n, 4), complex)), "block")
+    with open(os.path.join(HERE, "reference_z.json"), "w") as f:
+        json.dump(out, f, indent=1)
+
+
 if __name__ == "__main__":
     if "--full" in sys.argv[1:]:
         main_full()
+    elif "--complex" in sys.argv[1:]:
+        main_complex()
     else:
         main()

