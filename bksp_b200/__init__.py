@@ -63,6 +63,18 @@ class MixedOpts(C.Structure):
                 ("fallback", C.c_int)]
 
 
+class ZSpMat(C.Structure):
+    """``zspmat`` (include/bksp.h): complex values, interleaved (re, im)."""
+    _fields_ = [("row", _ip), ("col", _ip), ("nnz", _ip),
+                ("row_size", _ip), ("col_size", _ip), ("value", _dp),
+                ("format", C.c_char_p), ("type", C.c_char_p)]
+
+
+class ZMat(C.Structure):
+    """``zmat``: column-major complex values."""
+    _fields_ = [("row_size", C.c_int), ("col_size", C.c_int), ("value", _dp)]
+
+
 def _load():
     if not os.path.exists(LIB_PATH):
         raise ImportError(
@@ -88,6 +100,22 @@ def _load():
         f = getattr(L, name)
         f.argtypes = argt
         f.restype = C.c_int
+    zp, zm = C.POINTER(ZSpMat), C.POINTER(ZMat)
+    zsig = {
+        "zbicg": [zp, _dp, d, i, _dp],
+        "zbicgstabl": [zp, _dp, i, d, i, _dp],
+        "zblbicgstabl": [zp, zm, i, d, i, zm],
+        "zshbicgstabl": [zp, _dp, i, _dp, i, d, i, _dp],
+        "zqreco": [i, i, _dp, _dp],
+    }
+    for name, argt in zsig.items():
+        f = getattr(L, name)
+        f.argtypes = argt
+        f.restype = C.c_int
+    L.bksp_gpu_zcsrmv.argtypes = [zp, C.c_char, _dp, _dp]
+    L.bksp_gpu_zcsrmv.restype = i
+    L.zread_matrix_market.argtypes = [C.c_char_p]
+    L.zread_matrix_market.restype = zp
     L.bksp_gpu_dcsrmm.argtypes = [sp, C.c_char, i, d, _dp, d, _dp]
     L.bksp_gpu_dcsrmm.restype = i
     L.read_matrix_market.argtypes = [C.c_char_p]
@@ -293,6 +321,111 @@ def read_matrix_market(path):
     col = np.ctypeslib.as_array(m.col, shape=(nnz,)).copy() if nnz else np.zeros(0, np.int32)
     val = np.ctypeslib.as_array(m.value, shape=(nnz,)).copy() if nnz else np.zeros(0)
     return rowptr, col, val, n, m.type.decode()
+
+
+# ------------------------------------------------------------- complex
+
+class ZCsrMatrix:
+    """A ``zspmat`` over NumPy buffers (values complex128)."""
+
+    def __init__(self, rowptr, col, val, n=None):
+        self.rowptr = np.ascontiguousarray(rowptr, dtype=np.int32)
+        self.col = np.ascontiguousarray(col, dtype=np.int32)
+        self.val = np.ascontiguousarray(val, dtype=np.complex128)
+        nnz = int(self.rowptr[-1]) if self.rowptr.size else 0
+        if self.rowptr.ndim != 1 or self.rowptr.size < 2:
+            raise ValueError("rowptr must hold n + 1 >= 2 entries")
+        if self.col.shape != (nnz,) or self.val.shape != (nnz,):
+            raise ValueError(f"col and val must hold rowptr[-1] = {nnz} entries")
+        n = self.rowptr.size - 1 if n is None else int(n)
+        self.n = n
+        self._nnz = C.c_int(int(self.col.size))
+        self._n = C.c_int(n)
+        self._m = C.c_int(n)
+        self.s = ZSpMat(self.rowptr.ctypes.data_as(_ip),
+                        self.col.ctypes.data_as(_ip), C.pointer(self._nnz),
+                        C.pointer(self._n), C.pointer(self._m),
+                        self.val.ctypes.data_as(_dp), b"csr", b"unsymmetric")
+
+    @property
+    def ptr(self):
+        return C.byref(self.s)
+
+
+def _zinplace(x):
+    if not (isinstance(x, np.ndarray) and x.dtype == np.complex128
+            and x.flags.c_contiguous):
+        raise TypeError("x must be a C-contiguous complex128 array (updated in place)")
+    return x.ctypes.data_as(_dp)
+
+
+def _zvec(a):
+    return np.ascontiguousarray(a, dtype=np.complex128)
+
+
+def zbicg(A, b, tol, max_iter, x):
+    b = _zvec(b)
+    return lib.zbicg(A.ptr, b.ctypes.data_as(_dp), tol, max_iter, _zinplace(x))
+
+
+def zbicgstabl(A, b, l, tol, max_iter, x):
+    b = _zvec(b)
+    return lib.zbicgstabl(A.ptr, b.ctypes.data_as(_dp), l, tol, max_iter,
+                          _zinplace(x))
+
+
+def zshbicgstabl(A, b, l, sigma, tol, max_iter, x):
+    """x: n * (len(sigma) + 1) complex entries, seed first, in place."""
+    b = _zvec(b)
+    s = _zvec(sigma)
+    return lib.zshbicgstabl(A.ptr, b.ctypes.data_as(_dp), l,
+                            s.ctypes.data_as(_dp), int(s.size), tol, max_iter,
+                            _zinplace(x))
+
+
+def zblbicgstabl(A, B, l, tol, max_iter, X):
+    """X (n-by-s complex) is updated in place."""
+    Bf = np.asfortranarray(B, dtype=np.complex128)
+    Xf = np.asfortranarray(X, dtype=np.complex128)
+    bm = ZMat(Bf.shape[0], Bf.shape[1], Bf.ctypes.data_as(_dp))
+    xm = ZMat(Xf.shape[0], Xf.shape[1], Xf.ctypes.data_as(_dp))
+    rc = lib.zblbicgstabl(A.ptr, C.byref(bm), l, tol, max_iter, C.byref(xm))
+    X[...] = Xf
+    return rc
+
+
+def zcsrmv(A, x, trans="n"):
+    """y = A x ('n') or A^H x ('t') on the GPU (bksp_gpu_zcsrmv)."""
+    x = _zvec(x)
+    y = np.zeros(A.n, dtype=np.complex128)
+    rc = lib.bksp_gpu_zcsrmv(A.ptr, trans.encode(), x.ctypes.data_as(_dp),
+                             y.ctypes.data_as(_dp))
+    if rc != 0:
+        raise RuntimeError(f"bksp_gpu_zcsrmv failed ({rc})")
+    return y
+
+
+def zqreco(V):
+    """Thin QR of an m-by-n complex array; returns (Q, R, info)."""
+    Vf = np.asfortranarray(V, dtype=np.complex128).copy(order="F")
+    m, n = Vf.shape
+    R = np.zeros((n, n), dtype=np.complex128, order="F")
+    info = lib.zqreco(m, n, Vf.ctypes.data_as(_dp), R.ctypes.data_as(_dp))
+    return Vf, R, info
+
+
+def zread_matrix_market(path):
+    """Returns (rowptr, col, val, n, type) from the complex reader."""
+    p = lib.zread_matrix_market(os.fsencode(path))
+    if not p:
+        raise OSError(f"cannot read complex Matrix Market file {path}")
+    m = p.contents
+    n = m.row_size[0]
+    nnz = m.nnz[0]
+    rowptr = np.ctypeslib.as_array(m.row, shape=(n + 1,)).copy()
+    col = np.ctypeslib.as_array(m.col, shape=(nnz,)).copy()
+    raw = np.ctypeslib.as_array(m.value, shape=(2 * nnz,)).copy()
+    return rowptr, col, raw[0::2] + 1j * raw[1::2], n, m.type.decode()
 
 
 @contextlib.contextmanager

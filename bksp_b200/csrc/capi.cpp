@@ -534,22 +534,6 @@ int dvec2mat(double* x, int m, dmat* mat) {
   return 0;
 }
 
-// --------------------------------------------------------- complex (none)
-
-int zbicg(zspmat*, double _Complex*, double, int, double _Complex*) {
-  return INVALID_PARAMETERS;
-}
-int zbicgstabl(zspmat*, double _Complex*, int, double, int, double _Complex*) {
-  return INVALID_PARAMETERS;
-}
-int zblbicgstabl(zspmat*, zmat*, int, double, int, zmat*) {
-  return INVALID_PARAMETERS;
-}
-int zshbicgstabl(zspmat*, double _Complex*, int, double _Complex*, int, double,
-                 int, double _Complex*) {
-  return INVALID_PARAMETERS;
-}
-
 }  // extern "C"
 
 // ------------------------------------------------------- device utilities

@@ -6,32 +6,10 @@
 #include "dev_common.cuh"
 #include "solver_defs.h"
 #include "epi_block.cuh"
+#include "epi_common.cuh"
 
 namespace bk {
 
-// Convergence test shared by every method: `error < tol` passes (the
-// reference's `if (error < tol) break;`), a non-finite error is a breakdown,
-// otherwise the iteration index advances until max_iter.
-__device__ __forceinline__ void conv_check(const Red& rd, double err) {
-  Ctl* c = rd.ctl;
-  rd.S[kErr] = err;
-  if (c->hist && c->hist_len < c->hist_cap) c->hist[c->hist_len] = err;
-  c->hist_len++;
-  const int it = c->iter;
-  if (err < c->tol) {
-    c->done = 1;
-    c->ret = it;
-  } else if (!isfinite(err)) {
-    c->done = 1;
-    c->ret = kDivergence;
-  } else {
-    c->iter = it + 1;
-    if (it + 1 >= c->max_iter) {
-      c->done = 1;
-      c->ret = kNotConverged;
-    }
-  }
-}
 
 __device__ __forceinline__ void bl_back_substitution(double* S, int l) {
   // src/bicgstabl.c:93-109
@@ -201,10 +179,6 @@ static __device__ void qr_post(const Red& rd, int action) {
   }
 }
 
-static __device__ void fail_divergence(const Red& rd) {
-  rd.ctl->done = 1;
-  rd.ctl->ret = kDivergence;
-}
 
 // One-pass minimal-residual step of BiCGSTAB(l): the modified Gram-Schmidt
 // quantities of src/bicgstabl.c:84-91 (tau_ij, sigma_j, omega'_j) from the

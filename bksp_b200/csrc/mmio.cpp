@@ -45,24 +45,27 @@ bool parse_num(const char*& p, const char* e, T& v) {
 }
 
 // Entry lines [b, e): appends coordinates and values; false on a bad line.
-bool parse_chunk(const char* b, const char* e, bool pattern, long long M,
-                 long long N, std::vector<int>& ri, std::vector<int>& ci,
-                 std::vector<double>& vv) {
+bool parse_chunk(const char* b, const char* e, bool pattern, bool cplx,
+                 long long M, long long N, std::vector<int>& ri,
+                 std::vector<int>& ci, std::vector<double>& vv,
+                 std::vector<double>& vi) {
   const char* p = b;
   while (p < e) {
     const char* q = skip_blank(p, e);
     if (q < e && *q == '\n') { p = q + 1; continue; }   // blank line
     if (q >= e) break;
     long long i = 0, j = 0;
-    double v = 1.0;
+    double v = 1.0, w = 0.0;
     if (!parse_num(q, e, i) || !parse_num(q, e, j)) return false;
     if (!pattern && !parse_num(q, e, v)) return false;
+    if (cplx && !parse_num(q, e, w)) return false;
     if (i < 1 || i > M || j < 1 || j > N) return false;
     q = skip_blank(q, e);
     if (q < e && *q != '\n') return false;
     ri.push_back((int)(i - 1));
     ci.push_back((int)(j - 1));
     vv.push_back(v);
+    if (cplx) vi.push_back(w);
     p = q < e ? q + 1 : e;
   }
   return true;
@@ -70,7 +73,7 @@ bool parse_chunk(const char* b, const char* e, bool pattern, long long M,
 
 }  // namespace
 
-bool mm_parse(const char* path, MmData& out) {
+bool mm_parse(const char* path, MmData& out, bool complex_field) {
   FILE* f = std::fopen(path, "rb");
   if (!f) return false;
   std::string buf;
@@ -102,7 +105,7 @@ bool mm_parse(const char* path, MmData& out) {
       lower(b2) != "coordinate")
     return false;
   const std::string field = lower(b3), sym = lower(b4);
-  if (field == "complex") return false;
+  if ((field == "complex") != complex_field) return false;
   const bool pattern = field == "pattern";
   long long M = 0, N = 0, nz = 0;
   for (;;) {
@@ -129,14 +132,16 @@ bool mm_parse(const char* path, MmData& out) {
     cut[c] = nl ? nl + 1 : end;
   }
   std::vector<std::vector<int>> ri(nchunk), ci(nchunk);
-  std::vector<std::vector<double>> vv(nchunk);
+  std::vector<std::vector<double>> vv(nchunk), vi(nchunk);
   std::vector<char> ok(nchunk, 0);
   auto work = [&](size_t c) {
     const size_t guess = (size_t)(nz / (long long)nchunk + 16);
     ri[c].reserve(guess);
     ci[c].reserve(guess);
     vv[c].reserve(guess);
-    ok[c] = parse_chunk(cut[c], cut[c + 1], pattern, M, N, ri[c], ci[c], vv[c]);
+    if (complex_field) vi[c].reserve(guess);
+    ok[c] = parse_chunk(cut[c], cut[c + 1], pattern, complex_field, M, N, ri[c],
+                        ci[c], vv[c], vi[c]);
   };
   std::vector<std::thread> th;
   for (size_t c = 1; c < nchunk; ++c) th.emplace_back(work, c);
@@ -154,6 +159,7 @@ bool mm_parse(const char* path, MmData& out) {
   out.ri.clear();
   out.ci.clear();
   out.vv.clear();
+  out.vi.clear();
   out.ri.reserve(total);
   out.ci.reserve(total);
   out.vv.reserve(total);
@@ -161,6 +167,7 @@ bool mm_parse(const char* path, MmData& out) {
     out.ri.insert(out.ri.end(), ri[c].begin(), ri[c].end());
     out.ci.insert(out.ci.end(), ci[c].begin(), ci[c].end());
     out.vv.insert(out.vv.end(), vv[c].begin(), vv[c].end());
+    out.vi.insert(out.vi.end(), vi[c].begin(), vi[c].end());
   }
   return true;
 }

@@ -139,4 +139,63 @@ enum : short {
   E_COUNT_BASE,
 };
 
+// ---------------------------------------------------------------- complex
+// Complex solves (zsolvers.cpp): a complex scalar occupies the slot pair
+// (k, k + 1) = (re, im); a complex dot d of a reduction lands in
+// S[kD + 2d], S[kD + 2d + 1].  The common slots kFnb .. kBkU keep their
+// meaning.
+enum : short {
+  kZBkS = 6,          // block width s (as a double)
+  kZBkRows = 7,       // block rows (as a double)
+  kZAlpha = 16, kZBeta = 18, kZRdot = 20, kZG0 = 22, kZG1 = 24,
+  kZAlphaOld = 26, kZRho = 28,
+  kZOmega = 32,       // omega[0..l]       (l + 1 <= 9 pairs)
+  kZOmegaD = 50,      // omega'[0..l]
+  kZOmegaDD = 68,     // omega''[0..l]
+  kZSigma = 86,       // sigma[0..l]
+  kZTau = 104,        // tau[i], (l + 1)^2 <= 81 pairs, to 265
+  kZBkPiv = 280,      // pivots of the complex block LU (s doubles)
+  // shifted BiCGSTAB(l): per-shift arrays of kZMaxShifts pairs
+  kZMaxShifts = 128,
+  kZShSigma = 1024, kZShPi = 1280, kZShPiOld = 1536, kZShPiNew = 1792,
+  kZShAlpha = 2048, kZShTheta = 2304, kZShCb = 2560, kZShCr = 2816,
+  kZShCq = 3072, kZShCn = 3328, kZShCs = 3584, kZShCp = 3840,
+  kZShCx = 4096,      // [k][i], kBlMaxL pairs per shift, to 6143
+};
+
+// Complex s-by-s matrices (row-major pairs) of the complex block method in
+// cells of 512 slots (kZBkG2 doubles as epilogue scratch).
+constexpr short zbk_cell(int m) { return (short)(512 + 512 * m); }
+enum : short {
+  kZBkG1 = zbk_cell(0), kZBkG2 = zbk_cell(1), kZBkAlpha = zbk_cell(2),
+  kZBkBeta = zbk_cell(3), kZBkGam0 = zbk_cell(4), kZBkGam1 = zbk_cell(5),
+  kZBkXi = zbk_cell(6), kZBkT = zbk_cell(7), kZBkTinv = zbk_cell(8),
+  kZBkLU = zbk_cell(9), kZBkXiOld = zbk_cell(10), kZBkR = zbk_cell(11),
+  kZBkScr = zbk_cell(12), kZBkRinv = zbk_cell(13), kZBkATinv = zbk_cell(14),
+};
+
+// Complex epilogue codes (zepilogues.cuh), dispatched from run_epilogue.
+enum : short {
+  EZ_BASE = 200,
+  EZ_SET_FNB = EZ_BASE,   // S[kFnb] = sqrt(re D0)
+  // zbicg (src/bicg.c:91-177)
+  EZ_BICG_INIT, EZ_BICG_ALPHA, EZ_BICG_CHECK,
+  // zbicgstabl (src/bicgstabl.c:141-276)
+  EZ_BL_BETA0, EZ_BL_ALPHA, EZ_BL_BETA, EZ_BL_TAU, EZ_BL_SIG, EZ_BL_CHECK,
+  // zshbicgstabl (src/shbicgstabl.c:288-592)
+  EZ_SH_INIT, EZ_SH_ALPHA, EZ_SH_STEP, EZ_SH_TAU, EZ_SH_SIG, EZ_SH_CHECK,
+  // complex Cholesky-QR passes (a0: action after pass 3) and zblbicgstabl
+  // (src/blbicgstabl.c:255-486)
+  EZ_QR1, EZ_QR2, EZ_QR3,
+  EZ_BB_INIT, EZ_BB_BETA, EZ_BB_ALPHA, EZ_BB_TAU, EZ_BB_SIG, EZ_BB_CHECK,
+  EZ_END,
+};
+
+// Actions after the third complex Cholesky-QR pass (EZ_QR3's a0).
+enum : short {
+  ZQR_POST_NONE = 0,
+  ZQR_POST_INIT = 1,   // xi = R
+  ZQR_POST_T = 2,      // t = R: xi_old = xi, xi = t xi, t^-1, alpha t^-1
+};
+
 }  // namespace bk

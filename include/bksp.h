@@ -162,10 +162,9 @@ int dshbicgstabl(dspmat *A, double *b, int l, double *sigma, int sigma_size,
 
 /* ----------------------------------------------------- complex variants */
 
-/* Complex-valued structs and solvers of the reference (include/bksp.h
- * :115-182).  Declared so existing programs compile and link; this build
- * implements the real methods only, and every z* solver returns
- * INVALID_PARAMETERS without touching its arguments. */
+/* Complex-valued structs, helpers and solvers of the reference
+ * (include/bksp.h:111-182), run on the GPU like the real methods
+ * (capi_z.cpp).  Values are double _Complex, interleaved (re, im). */
 typedef struct {
     int *row;
     int *col;
@@ -182,6 +181,16 @@ typedef struct {
     int col_size;
     double _Complex *value;
 } zmat;
+
+/* A "matrix coordinate complex" Matrix Market file as CSR (entries in file
+ * order within each row); NULL if the file cannot be read or is not
+ * complex (the reference exits the process). */
+zspmat *zread_matrix_market(char *filename);
+/* Thin QR of the column-major m-by-n mat (n <= 16): mat <- Q, r <- R
+ * (column-major, upper triangular, real positive diagonal); 0 on success. */
+int zqreco(int m, int n, double _Complex *mat, double _Complex *r);
+zmat *zmat_create(int m, int n);
+int zmat_free(zmat *mat);
 
 int zbicg(zspmat *A, double _Complex *b, double tol, int max_iter,
           double _Complex *x);

@@ -67,6 +67,14 @@ int bksp_gpu_dcsrmv(dspmat *A, char trans, const double *x, double *y);
 int bksp_gpu_dcsrmm(dspmat *A, char trans, int s, double alpha,
                     const double *B, double beta, double *C);
 
+/* The complex product with host arrays (the reference's zcsrgemm0,
+ * src/matvec.c:55-98): y = A x (trans 'n') or y = A^H x ('t', the
+ * reference's 't' conjugates).  Each row is summed left to right from zero
+ * with the C99 complex multiply and no fused multiply-add, so the result is
+ * bit-identical to zcsrgemm0.  Returns 0 or INVALID_PARAMETERS. */
+int bksp_gpu_zcsrmv(zspmat *A, char trans, const double _Complex *x,
+                    double _Complex *y);
+
 /* ------------------------------------------------ device-resident solves */
 
 typedef struct bksp_gpu_matrix bksp_gpu_matrix;

@@ -133,3 +133,76 @@ def test_read_matrix_market_edge_cases(tmp_path):
     order = np.argsort(rows, kind="stable")
     assert np.array_equal(c, cols[order]) and np.array_equal(v, vals[order])
     assert np.array_equal(np.diff(rp), np.bincount(rows, minlength=n))
+
+
+def test_complex_api_is_declared():
+    names = _declared()
+    for f in ["zbicg", "zbicgstabl", "zblbicgstabl", "zshbicgstabl",
+              "zread_matrix_market", "zqreco", "zmat_create", "zmat_free",
+              "bksp_gpu_zcsrmv"]:
+        assert f in names, f
+
+
+def test_zread_matrix_market_matches_reference_reader(tmp_path):
+    """Complex files: the library's reader and the reference's
+    (src/read_matrix.c:176-301, through oracle/_ref) give the same CSR with
+    entries in file order within each row; real files are refused."""
+    from oracle import ref as R
+    rng = np.random.default_rng(5)
+    n, nz = 300, 2000
+    rows = rng.integers(0, n, nz)
+    cols = rng.integers(0, n, nz)
+    vals = rng.standard_normal(nz) + 1j * rng.standard_normal(nz)
+    p = tmp_path / "z.mtx"
+    with open(p, "w") as f:
+        f.write("%%MatrixMarket matrix coordinate complex general\n% c\n")
+        f.write(f"{n} {n} {nz}\n")
+        for i, j, a in zip(rows, cols, vals):
+            f.write(f"{i + 1} {j + 1} {float(a.real)!r} {float(a.imag)!r}\n")
+    rp, c, v, n2, t = B.zread_matrix_market(str(p))
+    assert n2 == n and t == "unsymmetric"
+    L = R._zlib()
+    L.zread_matrix_market.argtypes = [C.c_char_p]
+    L.zread_matrix_market.restype = C.POINTER(R.ZSpMat)
+    m = L.zread_matrix_market(os.fsencode(str(p))).contents
+    rr = np.ctypeslib.as_array(m.row, shape=(n + 1,))
+    cr = np.ctypeslib.as_array(m.col, shape=(nz,))
+    vr = np.ctypeslib.as_array(m.value, shape=(2 * nz,))
+    assert np.array_equal(rp, rr) and np.array_equal(c, cr)
+    assert np.array_equal(v.real, vr[0::2]) and np.array_equal(v.imag, vr[1::2])
+    (tmp_path / "real.mtx").write_text(
+        "%%MatrixMarket matrix coordinate real general\n2 2 1\n1 1 2.0\n")
+    with pytest.raises(OSError):
+        B.zread_matrix_market(str(tmp_path / "real.mtx"))
+
+
+def test_complex_invalid_arguments_are_rejected_without_gpu_work():
+    rp = np.array([0, 1, 2], np.int32)
+    A = B.ZCsrMatrix(rp, np.array([0, 1], np.int32), np.array([1.0, 1.0j]))
+    x = np.zeros(2, complex)
+    b = np.ones(2, complex)
+    assert B.zbicgstabl(A, b, 0, 1e-8, 10, x) == B.INVALID_PARAMETERS
+    assert B.zbicgstabl(A, b, 9, 1e-8, 10, x) == B.INVALID_PARAMETERS
+    assert B.zshbicgstabl(A, b, 0, [0.1], 1e-8, 10, np.zeros(4, complex)) == \
+        B.INVALID_PARAMETERS
+    assert B.zshbicgstabl(A, b, 2, np.zeros(129), 1e-8, 10,
+                          np.zeros(2 * 130, complex)) == B.INVALID_PARAMETERS
+    Bm = np.ones((2, 17), complex)
+    assert B.zblbicgstabl(A, Bm, 2, 1e-8, 10, np.zeros((2, 17), complex)) == \
+        B.INVALID_PARAMETERS
+    bad = B.ZCsrMatrix(rp, np.array([0, 1], np.int32), np.array([1.0, 1.0j]))
+    bad._nnz.value = 3
+    assert B.zbicg(bad, b, 1e-8, 10, x) == B.INVALID_PARAMETERS
+    assert B.lib.zqreco(2, 17, None, None) == B.INVALID_PARAMETERS
+
+
+def test_zmat_helpers():
+    f = B.lib.zmat_create
+    f.restype = C.POINTER(B.ZMat)
+    f.argtypes = [C.c_int, C.c_int]
+    m = f(4, 3)
+    assert (m.contents.row_size, m.contents.col_size) == (4, 3)
+    vals = np.ctypeslib.as_array(m.contents.value, shape=(24,))
+    assert np.all(vals == 0.0)
+    B.lib.zmat_free.argtypes = [C.POINTER(B.ZMat)]
+    assert B.lib.zmat_free(m) == 0
