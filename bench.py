@@ -66,18 +66,21 @@ def args_():
     p.add_argument("--nx", type=int, default=NX)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--workload", default="convdiff3d",
-                   choices=["convdiff3d", "kappa_batch", "configs"],
+                   choices=["convdiff3d", "kappa_batch", "configs", "complex"],
                    help="kappa_batch: the batched workload (64 kappa-diffusion "
                         "systems, BiCGSTAB(2)); configs: the other survey "
-                        "configurations through the bksp.h calls; each prints "
-                        "one JSON line of its own")
+                        "configurations through the bksp.h calls; complex: "
+                        "the complex solvers against the compiled reference's; "
+                        "each prints one JSON line of its own")
     p.add_argument("--batch-count", type=int, default=64)
     p.add_argument("--reference-solve-worker", action="store_true",
                    help=argparse.SUPPRESS)
     p.add_argument("--x-out", default=None, help=argparse.SUPPRESS)
+    p.add_argument("--complex-reference-worker", default=None,
+                   help=argparse.SUPPRESS)
     p.add_argument("--profile", default=None,
                    choices=["plain_fp64", "mixed_none", "mixed_learned", "spmv",
-                            "block_cg", "persist_cg"],
+                            "block_cg", "persist_cg", "zbicgstabl"],
                    help="profiling driver: set up, run one warm solve, then "
                         "one solve (or SpMV launches) between "
                         "cudaProfilerStart/Stop, print nothing else")
@@ -947,6 +950,119 @@ def run_configs(a):
     return 0
 
 
+def complex_reference_worker(spec):
+    """One compiled-reference complex solve (oracle/_ref) in this process;
+    prints {"s": seconds, "ret": ret}."""
+    from oracle import ref as R
+    P = problems_module()
+    d = json.loads(spec)
+    rp, c, v, n = P.complex_convdiff3d(d["nx"])
+    A = R.ZMatrix(rp, c, v, n)
+    b = P.complex_uniform(n, 3)
+    m = d["method"]
+    t0 = time.perf_counter()
+    if m == "zbicg":
+        ret, _, _ = R.zcall("zbicg", A, b, 1e-8, d["max_iter"], np.zeros(n, complex))
+    elif m == "zshbicgstabl":
+        sig = P.complex_shifts(d["ns"])
+        ret, _, _ = R.zcall("zshbicgstabl", A, b, d["l"], sig, d["ns"], 1e-8,
+                            d["max_iter"], np.zeros(n * (d["ns"] + 1), complex))
+    else:
+        Bm = np.random.default_rng(7).uniform(-1, 1, (n, d["s"])) \
+            + 1j * np.random.default_rng(8).uniform(-1, 1, (n, d["s"]))
+        ret, _, _ = R.zcall("zblbicgstabl", A, Bm, d["l"], 1e-8, d["max_iter"],
+                            np.zeros((n, d["s"]), complex))
+    print(json.dumps({"s": time.perf_counter() - t0, "ret": int(ret)}), flush=True)
+    return 0
+
+
+def run_complex(a):
+    """The complex solvers on the complex 3D convection-diffusion operator
+    (complex_convdiff3d, --nx^3, seeded right-hand sides), each to a relative
+    residual of 1e-8 through the bksp.h calls: GPU device time of the call
+    (bksp_gpu_record) and its FP64 true residual, beside the compiled
+    reference's complex solver on this host's cores (a child process, the
+    same call; zbicgstabl has no reference timing: its reference result
+    depends on stack contents).  Prints one JSON line."""
+    import scipy.sparse as sp
+    import bksp_b200 as B
+    P = problems_module()
+    nx = a.nx if a.nx != NX else 64
+    rp, c, v, n = P.complex_convdiff3d(nx)
+    As = sp.csr_matrix((v, c, rp), shape=(n, n))
+    A = B.ZCsrMatrix(rp, c, v)
+    b = P.complex_uniform(n, 3)
+    ns, s_blk = 8, 8
+    sig = P.complex_shifts(ns)
+    rng7, rng8 = np.random.default_rng(7), np.random.default_rng(8)
+    Bm = rng7.uniform(-1, 1, (n, s_blk)) + 1j * rng8.uniform(-1, 1, (n, s_blk))
+    cores = usable_cores()
+    out = {}
+
+    def gpu(name, fn, check):
+        best = None
+        for _ in range(3):
+            with B.record() as st:
+                ret, xv = fn()
+            if best is None or st["solve_ms"] < best[0]:
+                best = (st["solve_ms"], ret, st["total_ms"], st["launches"], xv)
+        ms, ret, tot, launches, xv = best
+        out[name] = {"gpu_solve_s": ms / 1e3, "gpu_call_s": tot / 1e3, "ret": ret,
+                     "launches": launches, "worst_true_residual": check(xv)}
+
+    def ref(name, spec, budget=600):
+        env = dict(os.environ, OPENBLAS_NUM_THREADS=str(cores),
+                   OMP_NUM_THREADS=str(cores))
+        cmd = [sys.executable, os.path.abspath(__file__),
+               "--complex-reference-worker", json.dumps(spec)]
+        try:
+            r = subprocess.run(cmd, env=env, capture_output=True, text=True,
+                               timeout=budget)
+            d = json.loads(r.stdout.strip().splitlines()[-1])
+            out[name]["reference_s"] = d["s"]
+            out[name]["reference_ret"] = d["ret"]
+            out[name]["gpu_speedup_vs_reference"] = d["s"] / out[name]["gpu_call_s"]
+        except (subprocess.TimeoutExpired, ValueError, IndexError, KeyError) as e:
+            out[name]["reference_s"] = None
+            out[name]["reference_note"] = f"not measured: {type(e).__name__}"
+
+    def tr(x, sigma=0.0):
+        return float(np.linalg.norm(b - As @ x - sigma * x) / np.linalg.norm(b))
+
+    def run_zbicg():
+        x = np.zeros(n, complex)
+        return B.zbicg(A, b, 1e-8, 5000, x), x
+    gpu("zbicg", run_zbicg, tr)
+    ref("zbicg", {"method": "zbicg", "nx": nx, "max_iter": 5000})
+
+    def run_zbl():
+        x = np.zeros(n, complex)
+        return B.zbicgstabl(A, b, 4, 1e-8, 5000, x), x
+    gpu("zbicgstabl4", run_zbl, tr)
+
+    def run_zsh():
+        x = np.zeros(n * (ns + 1), complex)
+        return B.zshbicgstabl(A, b, 4, sig, 1e-8, 5000, x), x
+    gpu("zshbicgstabl4_8shifts", run_zsh, lambda x: max(
+        [tr(x[:n])] + [tr(x[(k + 1) * n:(k + 2) * n], sg) for k, sg in enumerate(sig)]))
+    ref("zshbicgstabl4_8shifts", {"method": "zshbicgstabl", "nx": nx, "l": 4,
+                                  "ns": ns, "max_iter": 5000})
+
+    def run_zblk():
+        X = np.zeros((n, s_blk), complex)
+        return B.zblbicgstabl(A, Bm, 2, 1e-8, 5000, X), X
+    gpu("zblbicgstabl2_s8", run_zblk, lambda X: max(
+        float(np.linalg.norm(Bm[:, j] - As @ X[:, j]) / np.linalg.norm(Bm[:, j]))
+        for j in range(s_blk)))
+    ref("zblbicgstabl2_s8", {"method": "zblbicgstabl", "nx": nx, "l": 2,
+                             "s": s_blk, "max_iter": 5000})
+    line = {"metric": "complex solves to a relative residual of 1e-8",
+            "workload": f"complex_convdiff3d_{nx}^3", "n": n, "nnz": int(rp[-1]),
+            "reference_cores": cores, "methods": out}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def profile_small(a):
     """Profiling drivers that need no headline set-up: block_cg = five Block
     CG iterations (16 Gaussian right-hand sides, 3D Poisson --nx^3; run with
@@ -954,6 +1070,14 @@ def profile_small(a):
     CG solve of the 2D Poisson 64^2 system as a persistent launch."""
     import bksp_b200 as B
     P = problems_module()
+    if a.profile == "zbicgstabl":
+        rp, c, v, n = P.complex_convdiff3d(a.nx)
+        A = B.ZCsrMatrix(rp, c, v)
+        b = P.complex_uniform(n, 3)
+        x = np.zeros(n, complex)
+        ret = B.zbicgstabl(A, b, 4, 1e-10, 3, x)
+        print(f"profiled zbicgstabl {a.nx}^3: ret {ret}", flush=True)
+        return 0
     if a.profile == "block_cg":
         rp, c, v, n = P.poisson3d(a.nx)
         lrp, lc, lv, _ = P.lower_triangle(rp, c, v, n)
@@ -981,7 +1105,9 @@ def main():
     a = args_()
     if a.reference_solve_worker:
         return reference_solve_worker(a.nx, a.x_out)
-    if a.profile in ("block_cg", "persist_cg"):
+    if a.complex_reference_worker:
+        return complex_reference_worker(a.complex_reference_worker)
+    if a.profile in ("block_cg", "persist_cg", "zbicgstabl"):
         return profile_small(a)
     if a.impl == "reference":
         return run_reference(a)
@@ -989,6 +1115,8 @@ def main():
         return run_batch(a)
     if a.workload == "configs":
         return run_configs(a)
+    if a.workload == "complex":
+        return run_complex(a)
     return run_ours(a)
 
 

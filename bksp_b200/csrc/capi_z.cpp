@@ -89,6 +89,16 @@ int fail(const std::exception& e) {
   return INVALID_PARAMETERS;
 }
 
+// Launches and algorithmic bytes of the call, into the recorded stats.
+struct Counts {
+  long long l0 = launch_count(), y0 = byte_count();
+  void report() const {
+    if (!g_stats) return;
+    g_stats->launches = launch_count() - l0;
+    g_stats->alg_bytes = byte_count() - y0;
+  }
+};
+
 enum class ZMethod { BICG, BICGSTABL };
 
 int zsolve_single(ZMethod m, zspmat* A, double _Complex* b, int l, double tol,
@@ -99,6 +109,7 @@ int zsolve_single(ZMethod m, zspmat* A, double _Complex* b, int l, double tol,
     Ctx& cx = Ctx::get();
     cudaStream_t st = cx.st;
     Timer tm(st);
+    const Counts cnt;
     const int n = *A->row_size;
     ZDevCsr dA, dAH;
     upload_zcsr(n, A->row, A->col, dv(A->value), false, dA, st);
@@ -114,6 +125,7 @@ int zsolve_single(ZMethod m, zspmat* A, double _Complex* b, int l, double tol,
     tm.end_solve();
     zdownload(dv(x), dx, n, 1, st);
     tm.report(o.ret, &ss, o.iters);
+    cnt.report();
     ss.release(st);
     dfree(db, st);
     dfree(dx, st);
@@ -150,6 +162,7 @@ int zshbicgstabl(zspmat* A, double _Complex* b, int l, double _Complex* sigma,
     Ctx& cx = Ctx::get();
     cudaStream_t st = cx.st;
     Timer tm(st);
+    const Counts cnt;
     const int n = *A->row_size;
     ZDevCsr dA;
     upload_zcsr(n, A->row, A->col, dv(A->value), false, dA, st);
@@ -163,6 +176,7 @@ int zshbicgstabl(zspmat* A, double _Complex* b, int l, double _Complex* sigma,
     tm.end_solve();
     zdownload(dv(x), dx, n, sigma_size + 1, st);
     tm.report(o.ret, &ss, o.iters);
+    cnt.report();
     ss.release(st);
     dfree(db, st);
     dfree(dx, st);
@@ -186,6 +200,7 @@ int zblbicgstabl(zspmat* A, zmat* B, int ell, double tol, int max_iter,
     Ctx& cx = Ctx::get();
     cudaStream_t st = cx.st;
     Timer tm(st);
+    const Counts cnt;
     ZDevCsr dA;
     upload_zcsr(n, A->row, A->col, dv(A->value), false, dA, st);
     double2* dB = zupload_block(dv(B->value), n, s, st);
@@ -208,6 +223,7 @@ int zblbicgstabl(zspmat* A, zmat* B, int ell, double tol, int max_iter,
                 ell, it, err, true_res);
     std::fflush(stdout);
     tm.report(o.ret, &ss, o.iters);
+    cnt.report();
     if (g_stats) g_stats->true_res = true_res;
     ss.release(st);
     dfree(dB, st);

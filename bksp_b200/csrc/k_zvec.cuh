@@ -61,12 +61,14 @@ __device__ __forceinline__ double2 eval_zcf(const ZCfH& c, const double* S) {
 }
 
 // ------------------------------------------------------------- k_zlc
-// One element per thread and sweep, grid-stride over reps x n.  Inputs are
-// read once each; every output accumulates its terms in input order.  The
-// operand pointers, rep offsets and coefficients are staged in shared memory
-// first; MO bounds the outputs, the dots are reduced as kZDots pairs (unused
-// ones are zero).
-template <int MO>
+// Grid-stride over reps x n, one element per thread and sweep.  All of an
+// element's inputs are loaded before the first is used (MI bounds the
+// inputs, MO the outputs, both compile-time so the operands stay in
+// registers and the loads are in flight together); every output then adds
+// its terms in input order.  The operand pointers and the coefficients are
+// staged in shared memory first; the dots are reduced as kZDots pairs
+// (unused ones are zero).
+template <int MI, int MO>
 __global__ void __launch_bounds__(kThreads)
 k_zlc(ZLcH a, Red rd) {
   if (skip(rd)) return;
@@ -102,48 +104,51 @@ k_zlc(ZLcH a, Red rd) {
   for (int d = 0; d < 2 * kZDots; ++d) acc[d] = 0.0;
   const long long n = a.n;
   const int nin = a.nin, nout = a.nout, nd = a.nd;
+  const unsigned irep = a.in_rep_mask, orep = a.out_rep_mask;
   const long long step = (long long)gridDim.x * kThreads;
   for (int rep = 0; rep < a.reps; ++rep) {
     const long long ioff = rep * a.stride;
     for (long long e = (long long)blockIdx.x * kThreads + t; e < n; e += step) {
+      double2 v[MI];
+#pragma unroll
+      for (int i = 0; i < MI; ++i)
+        v[i] = i < nin ? __ldg(ip[i] + (((irep >> i) & 1u) ? ioff : 0) + e)
+                       : make_double2(0.0, 0.0);
       double2 y[MO];
-      bool any[MO];
-#pragma unroll
-      for (int o = 0; o < MO; ++o) { y[o] = make_double2(0.0, 0.0); any[o] = false; }
-      double2 du[kZDots], dv[kZDots];
-#pragma unroll
-      for (int d = 0; d < kZDots; ++d) { du[d] = make_double2(0.0, 0.0); dv[d] = du[d]; }
-      for (int i = 0; i < nin; ++i) {
-        const long long off = ((a.in_rep_mask >> i) & 1u) ? ioff : 0;
-        const double2 v = __ldg(ip[i] + off + e);
-#pragma unroll
-        for (int o = 0; o < MO; ++o) {
-          if (o < nout && ((used[o] >> i) & 1u)) {
-            y[o] = any[o] ? zfma(cs[o][i], v, y[o]) : zmul_f(cs[o][i], v);
-            any[o] = true;
-          }
-        }
-#pragma unroll
-        for (int d = 0; d < kZDots; ++d) {
-          if (dcode[d][0] == i) du[d] = v;
-          if (dcode[d][1] == i) dv[d] = v;
-        }
-      }
 #pragma unroll
       for (int o = 0; o < MO; ++o) {
+        y[o] = make_double2(0.0, 0.0);
         if (o < nout) {
-          const long long off = ((a.out_rep_mask >> o) & 1u) ? ioff : 0;
-          op[o][off + e] = y[o];
+          const unsigned u = used[o];
+          bool any = false;
 #pragma unroll
-          for (int d = 0; d < kZDots; ++d) {
-            if (dcode[d][0] == 100 + o) du[d] = y[o];
-            if (dcode[d][1] == 100 + o) dv[d] = y[o];
+          for (int i = 0; i < MI; ++i) {
+            if ((u >> i) & 1u) {
+              y[o] = any ? zfma(cs[o][i], v[i], y[o]) : zmul_f(cs[o][i], v[i]);
+              any = true;
+            }
           }
+          op[o][(((orep >> o) & 1u) ? ioff : 0) + e] = y[o];
         }
       }
 #pragma unroll
-      for (int d = 0; d < kZDots; ++d)
-        if (d < nd) zdot_acc(du[d], dv[d], dconj[d] != 0, acc[2 * d], acc[2 * d + 1]);
+      for (int d = 0; d < kZDots; ++d) {
+        if (d < nd) {
+          double2 du = make_double2(0.0, 0.0), dv = du;
+          const int c0 = dcode[d][0], c1 = dcode[d][1];
+#pragma unroll
+          for (int i = 0; i < MI; ++i) {
+            if (c0 == i) du = v[i];
+            if (c1 == i) dv = v[i];
+          }
+#pragma unroll
+          for (int o = 0; o < MO; ++o) {
+            if (c0 == 100 + o) du = y[o];
+            if (c1 == 100 + o) dv = y[o];
+          }
+          zdot_acc(du, dv, dconj[d] != 0, acc[2 * d], acc[2 * d + 1]);
+        }
+      }
     }
   }
   if (nd > 0 || rd.epi) finish_reduction<2 * kZDots>(acc, rd);

@@ -30,10 +30,13 @@ void launch_zlc(const ZLcH& d, const RedH& rd, cudaStream_t st) {
   for (int o = 0; o < d.nout; ++o) vecs += (d.out_rep_mask >> o) & 1u ? d.reps : 1;
   byte_count() += vecs * d.n * 16;
   ++launch_count();
-  if (d.nout <= 2)
-    launch_k(k_zlc<2>, grid_wave(k_zlc<2>, d.n), kThreads, 0, st, d, rd);
+  if (d.nin <= 4 && d.nout <= 2)
+    launch_k(k_zlc<4, 2>, grid_wave(k_zlc<4, 2>, d.n), kThreads, 0, st, d, rd);
+  else if (d.nin <= 8 && d.nout <= 4)
+    launch_k(k_zlc<8, 4>, grid_wave(k_zlc<8, 4>, d.n), kThreads, 0, st, d, rd);
   else
-    launch_k(k_zlc<6>, grid_wave(k_zlc<6>, d.n), kThreads, 0, st, d, rd);
+    launch_k(k_zlc<kZLcIn, kZLcOut>, grid_wave(k_zlc<kZLcIn, kZLcOut>, d.n), kThreads,
+             0, st, d, rd);
 }
 
 void launch_zspmv(const CsrH& A, const ZSpmvH& io, const RedH& rd,

@@ -131,9 +131,14 @@ def test_zblbicgstabl_matches_reference(gpu, tag, l, capfd):
     g = GOLD[f"zblbicgstabl{l}/{tag}"]
     assert abs(ret - g["ret"]) <= max(2, 0.15 * g["ret"]), (ret, g["ret"])
     hist_close(st["hist"], g["hist"], k=2 if l == 4 else 4, rtol=1e-6)
+    # The test stops on the whole block (||xi||_F / ||B||_F < tol), so a
+    # column's residual is bounded by the tolerance scaled to its share of
+    # ||B||_F, or sits near the reference's where that iterated further.
     for j in range(4):
-        tr = np.linalg.norm(B[:, j] - As @ X[:, j]) / np.linalg.norm(B[:, j])
-        assert tr <= 10 * max(g["true_res_cols"][j], 1e-12), (j, tr)
+        cn = np.linalg.norm(B[:, j])
+        tr = np.linalg.norm(B[:, j] - As @ X[:, j]) / cn
+        bound = max(10 * g["true_res_cols"][j], 10 * 1e-10 * np.linalg.norm(B) / cn)
+        assert tr <= bound, (j, tr, bound)
     out = capfd.readouterr().out
     assert f"Block BiCGSTAB({l}) has converged at:" in out
 
