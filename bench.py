@@ -66,11 +66,15 @@ def args_():
     p.add_argument("--nx", type=int, default=NX)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--workload", default="convdiff3d",
-                   choices=["convdiff3d", "kappa_batch", "configs", "complex"],
+                   choices=["convdiff3d", "kappa_batch", "configs", "complex",
+                            "spmv_general"],
                    help="kappa_batch: the batched workload (64 kappa-diffusion "
                         "systems, BiCGSTAB(2)); configs: the other survey "
                         "configurations through the bksp.h calls; complex: "
                         "the complex solvers against the compiled reference's; "
+                        "spmv_general: every SpMV kernel on the benchmark "
+                        "operator under a random symmetric permutation (no "
+                        "diagonal form); "
                         "each prints one JSON line of its own")
     p.add_argument("--batch-count", type=int, default=64)
     p.add_argument("--reference-solve-worker", action="store_true",
@@ -80,7 +84,7 @@ def args_():
                    help=argparse.SUPPRESS)
     p.add_argument("--profile", default=None,
                    choices=["plain_fp64", "mixed_none", "mixed_learned", "spmv",
-                            "block_cg", "persist_cg", "zbicgstabl"],
+                            "block_cg", "persist_cg", "zbicgstabl", "spmv_perm"],
                    help="profiling driver: set up, run one warm solve, then "
                         "one solve (or SpMV launches) between "
                         "cudaProfilerStart/Stop, print nothing else")
@@ -950,6 +954,60 @@ def run_configs(a):
     return 0
 
 
+def run_spmv_general(a):
+    """Every SpMV kernel on the 3D convection-diffusion --nx^3 operator under
+    a seeded random symmetric permutation (problems.permuted: same rows and
+    entries, no diagonal form), hot, CUDA events over 50 launches: time and
+    fraction of the measured copy bandwidth on the CSR algorithmic bytes
+    nnz (w + 4) + 4 (n + 1) + 2 w n.  Prints one JSON line."""
+    import torch
+    import bksp_b200 as B
+    P = problems_module()
+    rp, c, v, n = P.permuted(*P.convdiff3d(a.nx))
+    G = B.GpuMatrix(B.CsrMatrix(rp, c, v), B.FP32)
+    tuned = G.variant()
+    torch.cuda.set_device(0)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    sp_ = stream.cuda_stream
+    x64 = torch.rand(n, dtype=torch.float64, device="cuda")
+    y64 = torch.empty_like(x64)
+    x32 = x64.float()
+    y32 = torch.empty_like(x32)
+    peak = peaks()[0]
+    nnz = int(rp[-1])
+    out = {}
+    for vid, name in G.SPMV_VARIANTS.items():
+        if name == "dia":
+            continue
+        G.variant(vid)
+        row = {}
+        for f32, xx, yy, w in ((False, x64, y64, 8), (True, x32, y32, 4)):
+            for _ in range(5):
+                G.spmv(xx.data_ptr(), yy.data_ptr(), f32, sp_)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(50):
+                G.spmv(xx.data_ptr(), yy.data_ptr(), f32, sp_)
+            e1.record(stream)
+            e1.synchronize()
+            us = e0.elapsed_time(e1) / 50 * 1e3
+            alg = nnz * (w + 4) + 4 * (n + 1) + 2 * w * n
+            key = "fp32" if f32 else "fp64"
+            row[key + "_us"] = us
+            row[key + "_frac"] = alg / (us * 1e-6) / 1e9 / peak
+        out[name] = row
+    G.variant(tuned)
+    line = {"metric": "SpMV time on an operator without a diagonal form",
+            "workload": f"permuted convdiff3d {a.nx}^3", "n": n, "nnz": nnz,
+            "peak_gbs": peak, "autotuned": G.SPMV_VARIANTS[tuned],
+            "variants": out, "timing": "hot, CUDA events, 50 launches"}
+    print(json.dumps(line), flush=True)
+    G.close()
+    return 0
+
+
 def complex_reference_worker(spec):
     """One compiled-reference complex solve (oracle/_ref) in this process;
     prints {"s": seconds, "ret": ret}."""
@@ -1070,6 +1128,23 @@ def profile_small(a):
     CG solve of the 2D Poisson 64^2 system as a persistent launch."""
     import bksp_b200 as B
     P = problems_module()
+    if a.profile == "spmv_perm":
+        import torch
+        rp, c, v, n = P.permuted(*P.convdiff3d(a.nx))
+        G = B.GpuMatrix(B.CsrMatrix(rp, c, v), B.FP32)
+        x64 = torch.rand(n, dtype=torch.float64, device="cuda")
+        y64 = torch.empty_like(x64)
+        x32 = x64.float()
+        y32 = torch.empty_like(x32)
+        for var in (0, 8):
+            G.variant(var)
+            for _ in range(2):
+                G.spmv(x64.data_ptr(), y64.data_ptr(), False)
+                G.spmv(x32.data_ptr(), y32.data_ptr(), True)
+        torch.cuda.synchronize()
+        print(f"profiled spmv_perm {a.nx}^3", flush=True)
+        G.close()
+        return 0
     if a.profile == "zbicgstabl":
         rp, c, v, n = P.complex_convdiff3d(a.nx)
         A = B.ZCsrMatrix(rp, c, v)
@@ -1107,7 +1182,7 @@ def main():
         return reference_solve_worker(a.nx, a.x_out)
     if a.complex_reference_worker:
         return complex_reference_worker(a.complex_reference_worker)
-    if a.profile in ("block_cg", "persist_cg", "zbicgstabl"):
+    if a.profile in ("block_cg", "persist_cg", "zbicgstabl", "spmv_perm"):
         return profile_small(a)
     if a.impl == "reference":
         return run_reference(a)
@@ -1117,6 +1192,8 @@ def main():
         return run_configs(a)
     if a.workload == "complex":
         return run_complex(a)
+    if a.workload == "spmv_general":
+        return run_spmv_general(a)
     return run_ours(a)
 
 

@@ -550,7 +550,7 @@ class GpuMatrix:
                      "inner_iters": st.inner_iters, "sweeps": st.sweeps}
 
     SPMV_VARIANTS = {0: "tile", 1: "tma", 2: "vec4", 3: "vec8", 4: "vec16",
-                     5: "vec32", 6: "wtile", 7: "dia"}
+                     5: "vec32", 6: "wtile", 7: "dia", 8: "sell"}
 
     def diagonals(self):
         """Column offsets of the operator's diagonal form ([] when none)."""

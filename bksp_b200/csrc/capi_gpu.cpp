@@ -109,7 +109,7 @@ int bksp_gpu_matrix_destroy(bksp_gpu_matrix* m) {
 
 int bksp_gpu_matrix_variant(bksp_gpu_matrix* m, int variant) {
   if (!m) return INVALID_PARAMETERS;
-  if (variant > 7) return INVALID_PARAMETERS;
+  if (variant > 8) return INVALID_PARAMETERS;
   if (variant >= 0) {
     m->A.variant = variant;
     m->At.variant = variant;

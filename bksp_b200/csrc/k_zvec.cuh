@@ -246,6 +246,71 @@ k_zspmv(CsrH A, ZSpmvH io, Red rd) {
   if (ND > 0 || rd.epi) finish_reduction<2 * ND>(acc, rd);
 }
 
+// Complex sliced-ELL product (CsrH::sell with double2 values): one warp
+// per 32-row slice, one lane per row walking its entries in CSR order with
+// the reference's complex multiply and add, so the result equals k_zspmv's
+// (and zcsrgemm0's) bit for bit; coalesced column/value loads, four
+// entries' gathers in flight per lane, padding (column -1) skipped.
+template <int ND>
+__global__ void __launch_bounds__(kThreads)
+k_zspmv_sell(CsrH A, ZSpmvH io, Red rd) {
+  if (skip(rd)) return;
+  const int* __restrict__ sptr = A.sell.ptr;
+  const int* __restrict__ scol = A.sell.col;
+  const double2* __restrict__ sval = static_cast<const double2*>(A.sell.val);
+  const double2* __restrict__ x = io.x;
+  double acc[ND > 0 ? 2 * ND : 1];
+#pragma unroll
+  for (int d = 0; d < 2 * ND; ++d) acc[d] = 0.0;
+  const int lane = threadIdx.x & 31;
+  const long long gw = ((long long)blockIdx.x * kThreads + threadIdx.x) >> 5;
+  const long long nw = ((long long)gridDim.x * kThreads) >> 5;
+  const double2 z0 = make_double2(0.0, 0.0);
+  for (long long sl = gw; sl < A.sell.nslice; sl += nw) {
+    const int p0 = __ldg(sptr + sl), p1 = __ldg(sptr + sl + 1);
+    const int width = (p1 - p0) >> 5;
+    const long long row = sl * 32 + lane;
+    const int* cp = scol + p0 + lane;
+    const double2* vp = sval + p0 + lane;
+    double2 sum = z0;
+    int k = 0;
+    for (; k + 4 <= width; k += 4) {
+      int c[4];
+      double2 v[4], xv[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        c[u] = __ldg(cp + 32 * (k + u));
+        v[u] = __ldg(vp + 32 * (k + u));
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) xv[u] = c[u] >= 0 ? __ldg(x + c[u]) : z0;
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (c[u] >= 0) sum = zadd_rn(sum, zmul_rn(v[u], xv[u]));
+    }
+    for (; k < width; ++k) {
+      const int c = __ldg(cp + 32 * k);
+      if (c >= 0) sum = zadd_rn(sum, zmul_rn(__ldg(vp + 32 * k), __ldg(x + c)));
+    }
+    if (row < A.n) {
+      const double2 bv = io.b ? io.b[row] : z0;
+      double2 y = sum;
+      if (io.mode == 1) y = make_double2(__dadd_rn(bv.x, -sum.x), __dadd_rn(bv.y, -sum.y));
+      io.y[row] = y;
+      if (io.y2) io.y2[row] = y;
+      if (ND > 0) {
+        const double2 w0 = io.w0 ? io.w0[row] : z0;
+#pragma unroll
+        for (int d = 0; d < ND; ++d)
+          zdot_acc(zspmv_operand(io.dot[d][0], y, bv, w0),
+                   zspmv_operand(io.dot[d][1], y, bv, w0), io.dconj[d] != 0,
+                   acc[2 * d], acc[2 * d + 1]);
+      }
+    }
+  }
+  if (ND > 0 || rd.epi) finish_reduction<2 * ND>(acc, rd);
+}
+
 // ----------------------------------------------------------- k_zspmm
 // Y = beta C + alpha A X on row-major complex blocks, one thread per
 // (row, column), s <= 16 columns per row group: y = beta c, then

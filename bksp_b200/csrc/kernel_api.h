@@ -73,6 +73,18 @@ struct DiaH {
   int off[kDiaMax];            // their column offsets j - i, ascending
 };
 
+// Sliced-ELL copy of a CSR operator (k_spmv_sell.cuh): slices of 32
+// consecutive rows; slice s holds width_s = (ptr[s+1] - ptr[s]) / 32 entry
+// columns, stored column-major inside the slice (entry k of the slice's row
+// r at ptr[s] + 32 k + r) in each row's CSR order, padded with column -1.
+// nslice = 0: none.
+struct SellH {
+  const int* ptr;     // nslice + 1 entry offsets
+  const int* col;
+  const void* val;    // same precision as CsrH::val
+  int nslice;
+};
+
 // Device CSR matrix (one value precision).
 struct CsrH {
   const int* rowptr;
@@ -84,6 +96,7 @@ struct CsrH {
   int variant;   // SpMV kernel variant (kernels.cu: spmv_dispatch)
   DiaH dia;
   int nnz;       // stored entries (host-side byte accounting only)
+  SellH sell;
 };
 
 // One linear-combination launch: out[o] = sum_i c[o][i] * in[i], terms
@@ -231,6 +244,14 @@ void launch_csr2dia_d(const CsrH& A, const double* val, double* dval,
                       unsigned char* mask, cudaStream_t st);
 void launch_csr2dia_f(const CsrH& A, const float* val, float* dval,
                       unsigned char* mask, cudaStream_t st);
+// Fill a sliced-ELL copy (SellH) from the CSR arrays (sptr built by the
+// host from the row lengths).
+void launch_csr2sell_d(const int* rowptr, const int* col, const double* val,
+                       int n, int nslice, const int* sptr, int* scol,
+                       double* sval, cudaStream_t st);
+void launch_csr2sell_f(const int* rowptr, const int* col, const float* val,
+                       int n, int nslice, const int* sptr, int* scol,
+                       float* sval, cudaStream_t st);
 // Mixed precision: o0 (= o1 = o2 when given) = fl32(in), with the dot
 // (w, o0) when nd = 1 (w == nullptr: (o0, o0)); and x64 += t32, y32 = 0.
 void launch_mx_d2f(const double* in, float* o0, float* o1, float* o2,

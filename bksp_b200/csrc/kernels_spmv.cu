@@ -13,6 +13,7 @@
 #include "k_spmv_vec.cuh"
 #include "k_spmv_wtile.cuh"
 #include "k_spmv_dia.cuh"
+#include "k_spmv_sell.cuh"
 #include "kernel_api.h"
 #include "launch_util.h"
 
@@ -23,9 +24,10 @@ namespace bk {
 // SpMV kernel variants (every one sums a row in the reference's order):
 //   0 tile (register-staged products), 1 tile with TMA bulk copies,
 //   2..5 vector CSR with 4, 8, 16, 32 lanes per row, 6 warp tile,
-//   7 diagonal form (operators that have one; else the tile kernel).
+//   7 diagonal form (operators that have one; else the tile kernel),
+//   8 sliced ELL (operators that have the copy; else the tile kernel).
 // CsrH.variant carries the choice made for the operator (autotuner);
-// BKSP_GPU_SPMV=tile|tma|vec4|vec8|vec16|vec32|wtile|dia overrides it.
+// BKSP_GPU_SPMV=tile|tma|vec4|vec8|vec16|vec32|wtile|dia|sell overrides it.
 static int parse_spmv_override() {
   const char* e = std::getenv("BKSP_GPU_SPMV");
   if (!e) return -1;
@@ -38,6 +40,7 @@ static int parse_spmv_override() {
   if (s == "vec32") return 5;
   if (s == "wtile") return 6;
   if (s == "dia") return 7;
+  if (s == "sell") return 8;
   return -1;
 }
 static int spmv_override() {
@@ -171,6 +174,15 @@ static void spmv_dispatch(const CsrH& A, const SpmvH<XT>& io, const RedH& rd,
     var = 0;
   }
   byte_count() += spmv_bytes<VT, XT>(A, io, false);
+  if (var == 8 && A.sell.nslice > 0) {
+    const long long threads = (long long)A.sell.nslice * 32;
+    switch (io.nd) {
+      case 0: launch_k(k_spmv_sell<VT, XT, 0>, grid_wave(k_spmv_sell<VT, XT, 0>, threads), kThreads, 0, st, A, io, rd); return;
+      case 1: launch_k(k_spmv_sell<VT, XT, 1>, grid_wave(k_spmv_sell<VT, XT, 1>, threads), kThreads, 0, st, A, io, rd); return;
+      case 2: launch_k(k_spmv_sell<VT, XT, 2>, grid_wave(k_spmv_sell<VT, XT, 2>, threads), kThreads, 0, st, A, io, rd); return;
+      default: launch_k(k_spmv_sell<VT, XT, 3>, grid_wave(k_spmv_sell<VT, XT, 3>, threads), kThreads, 0, st, A, io, rd); return;
+    }
+  }
   switch (var) {
     case 1:
       switch (io.nd) {
@@ -280,6 +292,21 @@ void launch_csr2dia_f(const CsrH& A, const float* val, float* dval,
   ++launch_count();
   byte_count() += csr2dia_bytes<float>(A, mask != nullptr);
   launch_k(k_csr2dia<float>, (A.n + 255) / 256, 256, 0, st, A, val, dval, mask);
+}
+
+void launch_csr2sell_d(const int* rowptr, const int* col, const double* val,
+                       int n, int nslice, const int* sptr, int* scol,
+                       double* sval, cudaStream_t st) {
+  const long long rows = (long long)nslice * 32;
+  k_csr2sell<double><<<(unsigned)((rows + 255) / 256), 256, 0, st>>>(
+      rowptr, col, val, n, nslice, sptr, scol, sval);
+}
+void launch_csr2sell_f(const int* rowptr, const int* col, const float* val,
+                       int n, int nslice, const int* sptr, int* scol,
+                       float* sval, cudaStream_t st) {
+  const long long rows = (long long)nslice * 32;
+  k_csr2sell<float><<<(unsigned)((rows + 255) / 256), 256, 0, st>>>(
+      rowptr, col, val, n, nslice, sptr, scol, sval);
 }
 
 }  // namespace bk

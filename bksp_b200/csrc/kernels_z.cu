@@ -1,6 +1,7 @@
 // Launch wrappers of the complex kernels (k_zvec.cuh; interface in
 // zkernel_api.h).  Complex launches have no persistent-loop form: a
 // recording solve falls back to its graph loop.
+#include <cstdlib>
 #include <cstring>
 
 #include "dev_common.cuh"
@@ -17,6 +18,16 @@ namespace {
 
 void no_record(const char* what) {
   if (g_prog_rec) prog_unsupported(what);
+}
+
+// BKSP_GPU_SPMV=tile keeps the complex product on the tile kernel even
+// when the operator has a sliced-ELL copy.
+bool zspmv_tile_forced() {
+  static const bool v = [] {
+    const char* e = std::getenv("BKSP_GPU_SPMV");
+    return e && std::strcmp(e, "tile") == 0;
+  }();
+  return v;
 }
 
 }  // namespace
@@ -44,6 +55,15 @@ void launch_zspmv(const CsrH& A, const ZSpmvH& io, const RedH& rd,
   no_record("complex SpMV");
   byte_count() += (long long)A.nnz * 20 + 4LL * (A.n + 1) + 32LL * A.n;
   ++launch_count();
+  if (A.sell.nslice > 0 && !zspmv_tile_forced()) {
+    const long long threads = (long long)A.sell.nslice * 32;
+    switch (io.nd) {
+      case 0: launch_k(k_zspmv_sell<0>, grid_wave(k_zspmv_sell<0>, threads), kThreads, 0, st, A, io, rd); return;
+      case 1: launch_k(k_zspmv_sell<1>, grid_wave(k_zspmv_sell<1>, threads), kThreads, 0, st, A, io, rd); return;
+      case 2: launch_k(k_zspmv_sell<2>, grid_wave(k_zspmv_sell<2>, threads), kThreads, 0, st, A, io, rd); return;
+      default: launch_k(k_zspmv_sell<3>, grid_wave(k_zspmv_sell<3>, threads), kThreads, 0, st, A, io, rd); return;
+    }
+  }
   const int g = A.nrb < kMaxBlocks ? (A.nrb > 0 ? A.nrb : 1) : kMaxBlocks;
   switch (io.nd) {
     case 0: launch_k(k_zspmv<0>, g, kThreads, 0, st, A, io, rd); break;

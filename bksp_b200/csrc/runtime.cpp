@@ -57,6 +57,14 @@ void DevCsr::release(cudaStream_t st) {
   dfree(d32, st);
   dfree(ddiag, st);
   ddiag = nullptr;
+  dfree(sptr, st);
+  dfree(scol, st);
+  dfree(s64, st);
+  dfree(s32, st);
+  sptr = scol = nullptr;
+  s64 = nullptr;
+  s32 = nullptr;
+  nslice = 0;
   if (owns_dmask) dfree(dmask, st);
   rowptr = col = rb = nullptr;
   v64 = nullptr;
@@ -198,6 +206,41 @@ static void build_dia(DevCsr& A, cudaStream_t st) {
 
 // SpMV variant without timing: the diagonal form when there is one, else
 // vector CSR with the smallest lane count that covers a typical row.
+// Sliced-ELL copy of an uploaded operator without a diagonal form (host
+// rowptr: slice widths and offsets; the entries are placed on the GPU).
+// Skipped when the padding would exceed half the stored entries or the
+// offsets would overflow 32 bits.
+static void build_sell(DevCsr& A, const int* rowptr, cudaStream_t st) {
+  const int n = A.n;
+  const int nslice = (n + 31) / 32;
+  std::vector<int> ptr((size_t)nslice + 1, 0);
+  long long total = 0;
+  for (int s = 0; s < nslice; ++s) {
+    int w = 0;
+    const int r1 = std::min(n, (s + 1) * 32);
+    for (int r = s * 32; r < r1; ++r) w = std::max(w, rowptr[r + 1] - rowptr[r]);
+    total += 32LL * w;
+    if (total > 0x7fffff00LL) return;
+    ptr[s + 1] = (int)total;
+  }
+  if (total > (long long)A.nnz * 3 / 2 + 64) return;
+  A.sptr = dalloc_n<int>(nslice + 1, st);
+  A.scol = dalloc_n<int>(total, st);
+  A.s64 = dalloc_n<double>(total, st);
+  BK_CHECK(cudaMemcpyAsync(A.sptr, ptr.data(), sizeof(int) * (nslice + 1),
+                           cudaMemcpyHostToDevice, st));
+  launch_csr2sell_d(A.rowptr, A.col, A.v64, n, nslice, A.sptr, A.scol, A.s64, st);
+  BK_CHECK(cudaGetLastError());
+  if (A.v32) {
+    A.s32 = dalloc_n<float>(total, st);
+    launch_csr2sell_f(A.rowptr, A.col, A.v32, n, nslice, A.sptr, A.scol, A.s32, st);
+    BK_CHECK(cudaGetLastError());
+  }
+  A.nslice = nslice;
+  // ptr (a host vector) must outlive its copy.
+  BK_CHECK(cudaStreamSynchronize(st));
+}
+
 static int heuristic_variant(int n, int nnz, bool dia) {
   if (dia) return 7;
   const double avg = n > 0 ? (double)nnz / n : 0.0;
@@ -210,10 +253,10 @@ static int heuristic_variant(int n, int nnz, bool dia) {
 namespace {
 struct TuneKey {
   int n, nnz, dev;
-  bool fp32, dia;
+  bool fp32, dia, sell;
   bool operator==(const TuneKey& o) const {
     return n == o.n && nnz == o.nnz && dev == o.dev && fp32 == o.fp32 &&
-           dia == o.dia;
+           dia == o.dia && sell == o.sell;
   }
 };
 struct TuneHash {
@@ -236,7 +279,7 @@ void autotune_spmv(DevCsr& A, cudaStream_t st) {
   int dev = 0;
   cudaGetDevice(&dev);
   const bool f32 = A.v32 != nullptr;
-  const TuneKey key{A.n, A.nnz, dev, f32, A.ndia > 0};
+  const TuneKey key{A.n, A.nnz, dev, f32, A.ndia > 0, A.nslice > 0};
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tune_cache.find(key);
@@ -261,6 +304,7 @@ void autotune_spmv(DevCsr& A, cudaStream_t st) {
   int cands[8] = {0, 6, 1, 2, 3, 4};
   int kC = 6;
   if (A.ndia > 0) cands[kC++] = 7;
+  if (A.nslice > 0) cands[kC++] = 8;
   float best_of[8];
   for (int c = 0; c < kC; ++c) best_of[c] = 1e30f;
   for (int round = 0; round < 3; ++round) {
@@ -358,6 +402,7 @@ void upload_csr(int n, const int* rowptr, const int* col, const double* val,
   }
   std::sort(out.scan.off, out.scan.off + std::min(out.scan.noff, kScanOffs));
   if (dia_wanted(out.scan, n, nnz)) build_dia(out, st);
+  if (out.ndia == 0 && n >= (1 << 16)) build_sell(out, rowptr, st);
   out.variant = heuristic_variant(n, nnz, out.ndia > 0);
   if (n >= (1 << 16)) autotune_spmv(out, st);
 }

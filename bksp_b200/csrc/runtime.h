@@ -68,10 +68,23 @@ struct DevCsr {
   // and the first stored diagonal entry of every row (device, n doubles).
   CsrScanH scan{};
   double* ddiag = nullptr;
+  // Sliced-ELL copy (kernel_api.h: SellH) for operators without a diagonal
+  // form; nslice = 0: none.
+  int nslice = 0;
+  int* sptr = nullptr;
+  int* scol = nullptr;
+  double* s64 = nullptr;
+  float* s32 = nullptr;
   CsrH h64() const { return hview(v64, d64); }
   CsrH h32() const { return hview(v32, d32); }
   CsrH hview(const void* v, const void* dv) const {
-    CsrH h{rowptr, col, v, rb, n, nrb, variant, DiaH{}, nnz};
+    CsrH h{rowptr, col, v, rb, n, nrb, variant, DiaH{}, nnz, SellH{}};
+    if (nslice > 0 && v && (v == v64 || v == v32)) {
+      h.sell.ptr = sptr;
+      h.sell.col = scol;
+      h.sell.val = v == v64 ? static_cast<const void*>(s64) : static_cast<const void*>(s32);
+      h.sell.nslice = h.sell.val ? nslice : 0;
+    }
     if (ndia > 0 && dv) {
       h.dia.val = dv;
       h.dia.mask = dmask;

@@ -66,8 +66,12 @@ void ZDevCsr::release(cudaStream_t st) {
   dfree(col, st);
   dfree(val, st);
   dfree(rb, st);
-  rowptr = col = rb = nullptr;
-  val = nullptr;
+  dfree(sptr, st);
+  dfree(scol, st);
+  dfree(sval, st);
+  rowptr = col = rb = sptr = scol = nullptr;
+  val = sval = nullptr;
+  nslice = 0;
 }
 
 void upload_zcsr(int n, const int* rowptr, const int* col, const double* val,
@@ -119,6 +123,45 @@ void upload_zcsr(int n, const int* rowptr, const int* col, const double* val,
   out.rb = dalloc_n<int>((long long)rb.size(), st);
   BK_CHECK(cudaMemcpyAsync(out.rb, rb.data(), sizeof(int) * rb.size(),
                            cudaMemcpyHostToDevice, st));
+  // Sliced-ELL copy (32-row slices, entries column-major within a slice,
+  // each row in CSR order, padding column -1) unless padding would exceed
+  // half the entries.
+  const int nslice = (n + 31) / 32;
+  std::vector<int> sp((size_t)nslice + 1, 0);
+  long long total = 0;
+  for (int s = 0; s < nslice && total <= 0x7fffff00LL; ++s) {
+    int w = 0;
+    for (int r = s * 32; r < std::min(n, s * 32 + 32); ++r) w = std::max(w, rp[r + 1] - rp[r]);
+    total += 32LL * w;
+    sp[s + 1] = (int)std::min(total, 0x7fffff00LL);
+  }
+  std::vector<int> scol;
+  std::vector<double> sval;
+  if (total <= 0x7fffff00LL && total <= (long long)nnz * 3 / 2 + 64) {
+    scol.assign((size_t)total, -1);
+    sval.assign(2 * (size_t)total, 0.0);
+    for (int r = 0; r < n; ++r) {
+      const int s = r >> 5, lane = r & 31;
+      for (int k = rp[r]; k < rp[r + 1]; ++k) {
+        const size_t o = (size_t)sp[s] + 32 * (size_t)(k - rp[r]) + lane;
+        scol[o] = cc[k];
+        sval[2 * o] = vv[2 * (size_t)k];
+        sval[2 * o + 1] = vv[2 * (size_t)k + 1];
+      }
+    }
+    out.sptr = dalloc_n<int>(nslice + 1, st);
+    out.scol = dalloc_n<int>(total, st);
+    out.sval = dalloc_n<double2>(total, st);
+    BK_CHECK(cudaMemcpyAsync(out.sptr, sp.data(), sizeof(int) * (nslice + 1),
+                             cudaMemcpyHostToDevice, st));
+    if (total > 0) {
+      BK_CHECK(cudaMemcpyAsync(out.scol, scol.data(), sizeof(int) * total,
+                               cudaMemcpyHostToDevice, st));
+      BK_CHECK(cudaMemcpyAsync(out.sval, sval.data(), sizeof(double2) * total,
+                               cudaMemcpyHostToDevice, st));
+    }
+    out.nslice = nslice;
+  }
   // The host vectors above must outlive the copies.
   BK_CHECK(cudaStreamSynchronize(st));
 }

@@ -21,6 +21,11 @@ struct ZDevCsr {
   int* col = nullptr;
   double2* val = nullptr;
   int* rb = nullptr;
+  // Sliced-ELL copy (kernel_api.h: SellH); nslice = 0: none.
+  int nslice = 0;
+  int* sptr = nullptr;
+  int* scol = nullptr;
+  double2* sval = nullptr;
   CsrH h() const {
     CsrH c{};
     c.rowptr = rowptr;
@@ -30,6 +35,7 @@ struct ZDevCsr {
     c.n = n;
     c.nrb = nrb;
     c.nnz = nnz;
+    c.sell = SellH{sptr, scol, sval, nslice};
     return c;
   }
   void release(cudaStream_t st);

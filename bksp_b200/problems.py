@@ -114,6 +114,22 @@ def complex_shifts(count=8, lo=-3.0, hi=0.0, angle=0.25 * np.pi):
     return log_shifts(count, lo, hi) * np.exp(1j * angle)
 
 
+def permuted(rowptr, col, val, n, seed=21):
+    """P A P^T for a seeded random permutation P, columns ascending within
+    each row: the same operator without a diagonal form (a stand-in for an
+    unstructured matrix of the same size and row lengths)."""
+    perm = np.random.default_rng(seed).permutation(n)    # new index of row i
+    rows = np.repeat(np.arange(n), np.diff(rowptr))
+    r2 = perm[rows]
+    c2 = perm[col]
+    order = np.lexsort((c2, r2))
+    counts = np.bincount(r2, minlength=n)
+    rp = np.zeros(n + 1, dtype=np.int64)
+    np.cumsum(counts, out=rp[1:])
+    return (rp.astype(np.int32), c2[order].astype(np.int32),
+            np.asarray(val)[order].copy(), n)
+
+
 def csr_matvec(rowptr, col, val, x):
     """y = A x in float64 (host helper for building right-hand sides)."""
     n = rowptr.size - 1

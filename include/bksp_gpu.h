@@ -113,7 +113,10 @@ int bksp_gpu_solve(bksp_gpu_matrix *A, int method, int l, const double *b,
  * copies, 2..5 vector CSR with 4, 8, 16, 32 lanes per row, 6 warp tile
  * (each warp streams and sums its own 32 rows), 7 diagonal form (operators
  * without one, and calls whose result / operand vectors are not 16-byte
- * aligned, run the tile kernel).  variant < 0 queries, otherwise sets.
+ * aligned, run the tile kernel), 8 sliced ELL (32-row slices, one lane per
+ * row; built at upload for operators of >= 65,536 rows without a diagonal
+ * form whose padding stays under half the entries; others run the tile
+ * kernel).  variant < 0 queries, otherwise sets.
  * Returns the variant set.  The library picks one by timing all of them
  * when it uploads an operator of >= 65,536 rows (below that: the diagonal
  * form when there is one, else by mean row length). */

@@ -27,12 +27,15 @@ def problem(gpu, tag):
     return gpu.ZCsrMatrix(rp, c, v), sp.csr_matrix((v, c, rp), shape=(n, n)), n
 
 
-def random_complex_csr(n, per_row, seed):
-    """Unsorted columns, empty rows, one long row (> the 2048-entry tile)."""
+def random_complex_csr(n, per_row, seed, long_row=True):
+    """Unsorted columns, empty rows, one long row (> the 2048-entry tile)
+    when long_row (the tile kernel then serves it: its sliced-ELL copy would
+    be mostly padding)."""
     g = np.random.default_rng(seed)
     counts = g.integers(0, per_row + 1, n)
     counts[n // 3] = 0
-    counts[n // 2] = 3000
+    if long_row:
+        counts[n // 2] = 3000
     rp = np.zeros(n + 1, dtype=np.int32)
     np.cumsum(counts, out=rp[1:])
     col = g.integers(0, n, int(rp[-1])).astype(np.int32)
@@ -41,18 +44,19 @@ def random_complex_csr(n, per_row, seed):
 
 
 @pytest.mark.parametrize("trans", ["n", "t"])
-def test_zspmv_bit_identical_to_reference(gpu, trans):
+@pytest.mark.parametrize("long_row", [True, False])
+def test_zspmv_bit_identical_to_reference(gpu, trans, long_row):
+    """Tile kernel (long_row: a 3000-entry row) and sliced-ELL kernel."""
     n = 5000
-    rp, col, val = random_complex_csr(n, 12, 4)
+    rp, col, val = random_complex_csr(n, 12, 4, long_row)
     x = P.complex_uniform(n, 9)
     A = gpu.ZCsrMatrix(rp, col, val)
     y = gpu.zcsrmv(A, x, trans)
     yr = R.zspmv(R.ZMatrix(rp, col, val, n), x, trans == "t")
-    long_row = n // 2
     mask = np.ones(n, bool)
-    if trans == "n":
-        mask[long_row] = False    # strided CTA sum for a row over the tile
-        assert abs(y[long_row] - yr[long_row]) <= 1e-12 * np.abs(yr).max()
+    if trans == "n" and long_row:
+        mask[n // 2] = False      # strided CTA sum for a row over the tile
+        assert abs(y[n // 2] - yr[n // 2]) <= 1e-12 * np.abs(yr).max()
     assert np.array_equal(y[mask].view(np.float64), yr[mask].view(np.float64))
 
 
