@@ -182,6 +182,23 @@ typedef struct {
     double _Complex *value;
 } zmat;
 
+/* Accessors of the reference (include/bksp.h:134-161); zmat_get returns
+ * the real part, as the reference's declares a double result. */
+static inline int zspmat_rowsize(zspmat *mat) { return *mat->row_size; }
+static inline int zspmat_colsize(zspmat *mat) { return *mat->col_size; }
+static inline int zmat_set(zmat *mat, int m, int n, double _Complex *num)
+{
+    mat->value[n * mat->row_size + m] = *num;
+    return 0;
+}
+static inline double zmat_get(zmat *mat, int m, int n)
+{
+    return __real__ mat->value[n * mat->row_size + m];
+}
+static inline int zmat_rowsize(zmat *mat) { return mat->row_size; }
+static inline int zmat_colsize(zmat *mat) { return mat->col_size; }
+static inline double _Complex *zmat_value(zmat *mat) { return mat->value; }
+
 /* A "matrix coordinate complex" Matrix Market file as CSR (entries in file
  * order within each row); NULL if the file cannot be read or is not
  * complex (the reference exits the process). */

@@ -206,3 +206,37 @@ def test_zmat_helpers():
     assert np.all(vals == 0.0)
     B.lib.zmat_free.argtypes = [C.POINTER(B.ZMat)]
     assert B.lib.zmat_free(m) == 0
+
+
+def test_mex_front_ends_link_and_check_arguments_without_gpu():
+    """The reference's MATLAB front-ends, compiled unchanged against
+    include/bksp.h and libbksp.so (tests/mex/Makefile), load and report
+    argument errors back to the caller (MATLAB-API stand-in
+    tests/mex/mexshim.c); their solves run in tests/test_gpu_mex.py."""
+    build = os.path.join(ROOT, "tests", "mex", "_build")
+    if not os.path.exists(os.path.join(build, "bicg.so")):
+        pytest.skip("MEX front-ends not built (no reference sources here)")
+    shim = C.CDLL(os.path.join(build, "libmexshim.so"), mode=C.RTLD_GLOBAL)
+    shim.shim_dense.restype = C.c_void_p
+    shim.shim_dense.argtypes = [C.c_size_t, C.c_size_t, C.POINTER(C.c_double),
+                                C.POINTER(C.c_double)]
+    shim.shim_call.restype = C.c_int
+    shim.shim_call.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_void_p),
+                               C.c_int, C.POINTER(C.c_void_p)]
+    shim.shim_error.restype = C.c_char_p
+    one = np.ones(4)
+    dense = shim.shim_dense(2, 2, one.ctypes.data_as(C.POINTER(C.c_double)), None)
+    vec = shim.shim_dense(2, 1, one.ctypes.data_as(C.POINTER(C.c_double)), None)
+    sc = shim.shim_dense(1, 1, one.ctypes.data_as(C.POINTER(C.c_double)), None)
+    for name, nargs in (("bicg", 4), ("bicgstabl", 5), ("shbicgstabl", 6),
+                        ("blbicgstabl", 5)):
+        L = C.CDLL(os.path.join(build, f"{name}.so"))
+        fn = C.cast(L.mexFunction, C.c_void_p).value
+        plhs = (C.c_void_p * 1)()
+        few = (C.c_void_p * 1)(dense)
+        assert shim.shim_call(fn, 1, plhs, 1, few) == 1
+        assert b"BKSP:" in shim.shim_error()
+        args = (C.c_void_p * nargs)(*([dense, vec] + [sc] * (nargs - 2)))
+        if name != "blbicgstabl":   # the block front-end checks sizes only
+            assert shim.shim_call(fn, 1, plhs, nargs, args) == 1
+            assert b"sparse square matrix" in shim.shim_error(), name
