@@ -624,8 +624,10 @@ def run_batch(a):
     finite volumes on L^3 grids, L ~ U{32..96} (seed 4), kappa = exp(GRF),
     f ~ N(0,1); time to an FP64 true relative residual of 1e-8 on every
     system.  value: mixed-precision BiCGSTAB(2) with the learned SPAI
-    preconditioner (trained beforehand on 64 smaller systems of the same
-    family, seeds 1000+i, the configuration's 256), one CUDA-graph loop per system on eight host
+    preconditioner (trained beforehand on the configuration's 256 smaller
+    systems of the same family, seeds 1000+i, in four rounds whose logged
+    iteration counts on three held-out systems pick the kept parameters),
+    one CUDA-graph loop per system on eight host
     threads; plain_fp64_s: FP64 BiCGSTAB(2) on the Jacobi right-scaled
     systems A D^-1 y = b, x = D^-1 y, batched the same way; the modes also
     time both as one persistent launch for the whole batch (*_persistent)
@@ -672,7 +674,15 @@ def run_batch(a):
     Ls = np.random.default_rng(999).integers(16, 33, 256)
     train = [B.GpuMatrix(B.CsrMatrix(*P.kappa_diffusion3d(int(L), 1000 + i)[:3]), B.FP32)
              for i, L in enumerate(Ls)]
-    loss = model.train(train, epochs=100, probes=8, lr=3e-3, seed=7)
+    # Held-out probe systems (seeds 5000+i) whose logged iteration counts
+    # choose among the training rounds.
+    probe = []
+    for i, L in enumerate((20, 28, 36)):
+        prp, pc, pv, pn = P.kappa_diffusion3d(L, 5000 + i)[:4]
+        probe.append((B.CsrMatrix(prp, pc, pv), np.random.default_rng(5100 + i).standard_normal(pn)))
+    tlog = model.train_logged(train, probe, rounds=4, epochs=25, probes=8,
+                              lr=3e-3, seed=7, l=2)
+    loss = tlog["rounds"][tlog["best_round"]]["loss"] if tlog["best_round"] >= 0 else None
     for m in train:
         m.close()
     train_s = time.perf_counter() - t0
@@ -778,6 +788,7 @@ def run_batch(a):
         "speedup_vs_plain_fp64": res["plain_fp64"]["s"] / res["mixed_learned"]["s"],
         "modes": res,
         "spai_training": {"s": train_s, "final_loss": loss, "systems": "256 kappa, L U{16..32}",
+                          "logged_iterations": tlog,
                           "epochs": 100, "probes": 8},
         "setup_s": {"generate": gen_s, "upload": upload_s},
         "clocks": clk.summary(),

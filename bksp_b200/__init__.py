@@ -621,6 +621,35 @@ class SpaiModel:
             raise RuntimeError(f"spai training failed ({rc})")
         return loss.value
 
+    def train_logged(self, systems, probe_systems, rounds=4, epochs=25,
+                     probes=8, lr=1e-3, seed=1, l=2, target=1e-8):
+        """Training with logged iteration counts: `rounds` rounds of
+        `epochs` epochs of the ||(I - M A) Z||_F loss (train); after each
+        round the learned mixed BiCGSTAB(l) solves every probe system
+        ((CsrMatrix, b) pairs held out from `systems`) to the FP64 target
+        and its iteration counts are logged.  The gradient comes from the
+        loss (iteration counts are not differentiable); the logged counts
+        pick the round whose parameters the model keeps (fewest total
+        iterations; a round with a failed solve is never picked).  Returns
+        {"best_round", "rounds": [{"loss", "iters"}, ...]}."""
+        log, best, best_total, best_p = [], -1, None, None
+        for r in range(rounds):
+            loss = self.train(systems, epochs=epochs, probes=probes, lr=lr,
+                              seed=seed + r)
+            iters = []
+            for A, b in probe_systems:
+                x = np.zeros(A.n)
+                ret = dbicgstabl_mixed(A, b, x, l=l, target=target,
+                                       precond=PRECOND_LEARNED, model=self,
+                                       fallback=0)
+                iters.append(int(ret))
+            log.append({"loss": float(loss), "iters": iters})
+            if min(iters) >= 0 and (best_total is None or sum(iters) < best_total):
+                best, best_total, best_p = r, sum(iters), self.params()
+        if best_p is not None:
+            self.set_params(best_p)
+        return {"best_round": best, "rounds": log}
+
     def loss_grad(self, A, Z=None, probes=8, seed=1):
         """Loss and gradient; Z: (probes, n) float32 or None (seeded)."""
         g = np.zeros(self.nparams, dtype=np.float32)

@@ -308,3 +308,33 @@ def test_mixed_cg_fused_matches_unfused(gpu, torch_cuda, poisson_model, precond)
     r0, l0 = [int(t) for t in out.stdout.split()[-2:]]
     assert r0 >= 0 and abs(r0 - ret) <= 2, (r0, ret)
     assert st["launches"] < l0, (st["launches"], l0)
+
+
+def test_training_with_logged_iteration_counts(gpu):
+    """SpaiModel.train_logged: the loss drives training; the learned solve's
+    iteration counts on held-out systems are logged after every round and
+    pick the parameters kept (the round with the fewest total iterations),
+    which then reproduce that round's counts."""
+    from bksp_b200 import problems as P
+    train = [gpu.GpuMatrix(gpu.CsrMatrix(*P.kappa_diffusion3d(L, 1000 + i)[:3]), gpu.FP32)
+             for i, L in enumerate((12, 14, 16, 18))]
+    probe = []
+    for i, L in enumerate((16, 20)):
+        rp, c, v, n = P.kappa_diffusion3d(L, 5000 + i)
+        probe.append((gpu.CsrMatrix(rp, c, v), np.random.default_rng(i).standard_normal(n)))
+    model = gpu.SpaiModel(seed=3)
+    log = model.train_logged(train, probe, rounds=3, epochs=10, probes=4,
+                             lr=3e-3, seed=7, l=2)
+    assert len(log["rounds"]) == 3
+    totals = [sum(r["iters"]) for r in log["rounds"]]
+    assert all(min(r["iters"]) >= 0 for r in log["rounds"])
+    assert log["best_round"] == int(np.argmin(totals))
+    again = []
+    for A, b in probe:
+        x = np.zeros(A.n)
+        again.append(gpu.dbicgstabl_mixed(A, b, x, l=2, target=1e-8,
+                                          precond=gpu.PRECOND_LEARNED,
+                                          model=model, fallback=0))
+    assert again == log["rounds"][log["best_round"]]["iters"]
+    for m in train:
+        m.close()
