@@ -4,7 +4,7 @@
 // the reference's order and rounding (y = 0; y += a_k x_k, no FMA) and the
 // product is bit-identical to dcsrgemm0 and to the tile kernel.  Entry k of
 // the 32 rows sits in 32 consecutive words, so the column and value loads
-// of a warp are single coalesced transactions; four entries' loads (and
+// of a warp are single coalesced transactions; eight entries' loads (and
 // their x gathers) are issued before the first is added, to keep several
 // gathers in flight per lane.  Padding (column -1) is skipped, never added.
 // Epilogue as the tile kernel (k_spmv.cuh): b - A x, a copy, + shift x,
@@ -16,7 +16,7 @@
 namespace bk {
 
 template <typename VT, typename XT, int ND>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 4)
 k_spmv_sell(CsrH A, SpmvH<XT> io, Red rd) {
   if (skip(rd)) return;
   const int* __restrict__ sptr = A.sell.ptr;
@@ -36,25 +36,24 @@ k_spmv_sell(CsrH A, SpmvH<XT> io, Red rd) {
     const int* cp = scol + p0 + lane;
     const VT* vp = sval + p0 + lane;
     XT sum = XT(0);
-    int k = 0;
-    for (; k + 4 <= width; k += 4) {
-      int c[4];
-      VT v[4];
-      XT xv[4];
+    // Eight entries per round: all column and value loads of the round,
+    // then all x gathers, then the ordered adds -- one load round trip per
+    // round (one per slice for rows of up to eight entries).
+    for (int k0 = 0; k0 < width; k0 += 8) {
+      int c[8];
+      VT v[8];
+      XT xv[8];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        c[u] = __ldg(cp + 32 * (k + u));
-        v[u] = __ldg(vp + 32 * (k + u));
+      for (int u = 0; u < 8; ++u) {
+        const bool in = k0 + u < width;
+        c[u] = in ? __ldg(cp + 32 * (k0 + u)) : -1;
+        v[u] = in ? __ldg(vp + 32 * (k0 + u)) : VT(0);
       }
 #pragma unroll
-      for (int u = 0; u < 4; ++u) xv[u] = c[u] >= 0 ? __ldg(x + c[u]) : XT(0);
+      for (int u = 0; u < 8; ++u) xv[u] = c[u] >= 0 ? __ldg(x + c[u]) : XT(0);
 #pragma unroll
-      for (int u = 0; u < 4; ++u)
+      for (int u = 0; u < 8; ++u)
         if (c[u] >= 0) sum = add_rn(sum, mul_rn((XT)v[u], xv[u]));
-    }
-    for (; k < width; ++k) {
-      const int c = __ldg(cp + 32 * k);
-      if (c >= 0) sum = add_rn(sum, mul_rn((XT)__ldg(vp + 32 * k), __ldg(x + c)));
     }
     if (row < A.n) {
       if (io.shift != 0.0) sum = add_rn(sum, mul_rn((XT)io.shift, x[row]));

@@ -249,10 +249,10 @@ k_zspmv(CsrH A, ZSpmvH io, Red rd) {
 // Complex sliced-ELL product (CsrH::sell with double2 values): one warp
 // per 32-row slice, one lane per row walking its entries in CSR order with
 // the reference's complex multiply and add, so the result equals k_zspmv's
-// (and zcsrgemm0's) bit for bit; coalesced column/value loads, four
+// (and zcsrgemm0's) bit for bit; coalesced column/value loads, eight
 // entries' gathers in flight per lane, padding (column -1) skipped.
 template <int ND>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 3)
 k_zspmv_sell(CsrH A, ZSpmvH io, Red rd) {
   if (skip(rd)) return;
   const int* __restrict__ sptr = A.sell.ptr;
@@ -273,24 +273,20 @@ k_zspmv_sell(CsrH A, ZSpmvH io, Red rd) {
     const int* cp = scol + p0 + lane;
     const double2* vp = sval + p0 + lane;
     double2 sum = z0;
-    int k = 0;
-    for (; k + 4 <= width; k += 4) {
-      int c[4];
-      double2 v[4], xv[4];
+    for (int k0 = 0; k0 < width; k0 += 8) {   // eight entries per round
+      int c[8];
+      double2 v[8], xv[8];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        c[u] = __ldg(cp + 32 * (k + u));
-        v[u] = __ldg(vp + 32 * (k + u));
+      for (int u = 0; u < 8; ++u) {
+        const bool in = k0 + u < width;
+        c[u] = in ? __ldg(cp + 32 * (k0 + u)) : -1;
+        v[u] = in ? __ldg(vp + 32 * (k0 + u)) : z0;
       }
 #pragma unroll
-      for (int u = 0; u < 4; ++u) xv[u] = c[u] >= 0 ? __ldg(x + c[u]) : z0;
+      for (int u = 0; u < 8; ++u) xv[u] = c[u] >= 0 ? __ldg(x + c[u]) : z0;
 #pragma unroll
-      for (int u = 0; u < 4; ++u)
+      for (int u = 0; u < 8; ++u)
         if (c[u] >= 0) sum = zadd_rn(sum, zmul_rn(v[u], xv[u]));
-    }
-    for (; k < width; ++k) {
-      const int c = __ldg(cp + 32 * k);
-      if (c >= 0) sum = zadd_rn(sum, zmul_rn(__ldg(vp + 32 * k), __ldg(x + c)));
     }
     if (row < A.n) {
       const double2 bv = io.b ? io.b[row] : z0;
