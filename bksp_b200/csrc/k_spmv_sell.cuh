@@ -101,7 +101,7 @@ __global__ void k_csr2sell(const int* __restrict__ rowptr, const int* __restrict
       sval[o] = val[k0 + k];
     } else {
       scol[o] = -1;
-      sval[o] = VT(0);
+      sval[o] = VT{};
     }
   }
 }

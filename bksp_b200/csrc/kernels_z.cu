@@ -5,6 +5,7 @@
 #include <cstring>
 
 #include "dev_common.cuh"
+#include "k_spmv_sell.cuh"
 #include "k_zvec.cuh"
 #include "kernel_api.h"
 #include "launch_util.h"
@@ -96,6 +97,14 @@ void launch_zblock(const ZBlkH& a, const RedH& rd, cudaStream_t st) {
   ++launch_count();
   const long long tiles = (a.n + kZBlkRows - 1) / kZBlkRows;
   launch_k(k_zblock, grid_wave(k_zblock, tiles * kThreads), kThreads, 0, st, a, rd);
+}
+
+void launch_csr2sell_z(const int* rowptr, const int* col, const double2* val,
+                       int n, int nslice, const int* sptr, int* scol,
+                       double2* sval, cudaStream_t st) {
+  const long long rows = (long long)nslice * 32;
+  k_csr2sell<double2><<<(unsigned)((rows + 255) / 256), 256, 0, st>>>(
+      rowptr, col, val, n, nslice, sptr, scol, sval);
 }
 
 void launch_zshift(const ZShiftH& a, const RedH& rd, cudaStream_t st) {

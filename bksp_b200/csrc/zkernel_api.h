@@ -123,5 +123,9 @@ void launch_zspmm(const CsrH& A, const ZSpmmH& a, const RedH& rd,
                   cudaStream_t st);
 void launch_zblock(const ZBlkH& a, const RedH& rd, cudaStream_t st);
 void launch_zshift(const ZShiftH& a, const RedH& rd, cudaStream_t st);
+// Fill a complex sliced-ELL copy from the device CSR (sptr from the host).
+void launch_csr2sell_z(const int* rowptr, const int* col, const double2* val,
+                       int n, int nslice, const int* sptr, int* scol,
+                       double2* sval, cudaStream_t st);
 
 }  // namespace bk

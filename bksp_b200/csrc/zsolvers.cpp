@@ -83,11 +83,16 @@ void upload_zcsr(int n, const int* rowptr, const int* col, const double* val,
     if (rowptr[i + 1] < rowptr[i]) throw CudaError("matrix: bad row pointer");
   for (int k = 0; k < nnz; ++k)
     if (col[k] < 0 || col[k] >= n) throw CudaError("matrix: column index out of range");
-  std::vector<int> rp(rowptr, rowptr + n + 1), cc(col, col + nnz);
-  std::vector<double> vv(val, val + 2 * (size_t)nnz);
+  // A^H on the host (rows of A^H in the original row order).
+  std::vector<int> trp, tc;
+  std::vector<double> tv;
+  const int* rp = rowptr;
+  const int* cc = col;
+  const double* vv = val;
   if (conj_transpose) {
-    std::vector<int> trp(n + 1, 0), tc(nnz);
-    std::vector<double> tv(2 * (size_t)nnz);
+    trp.assign(n + 1, 0);
+    tc.resize(nnz);
+    tv.resize(2 * (size_t)nnz);
     for (int k = 0; k < nnz; ++k) trp[col[k] + 1]++;
     for (int i = 0; i < n; ++i) trp[i + 1] += trp[i];
     std::vector<int> pos(trp.begin(), trp.end() - 1);
@@ -98,9 +103,9 @@ void upload_zcsr(int n, const int* rowptr, const int* col, const double* val,
         tv[2 * (size_t)p] = val[2 * (size_t)k];
         tv[2 * (size_t)p + 1] = -val[2 * (size_t)k + 1];
       }
-    rp.swap(trp);
-    cc.swap(tc);
-    vv.swap(tv);
+    rp = trp.data();
+    cc = tc.data();
+    vv = tv.data();
   }
   const long long padn = (long long)(nnz + 3) / 4 * 4 + 4;
   out.n = n;
@@ -110,22 +115,22 @@ void upload_zcsr(int n, const int* rowptr, const int* col, const double* val,
   out.val = dalloc_n<double2>(padn, st);
   BK_CHECK(cudaMemsetAsync(out.col, 0, sizeof(int) * padn, st));
   BK_CHECK(cudaMemsetAsync(out.val, 0, sizeof(double2) * padn, st));
-  BK_CHECK(cudaMemcpyAsync(out.rowptr, rp.data(), sizeof(int) * (n + 1),
+  BK_CHECK(cudaMemcpyAsync(out.rowptr, rp, sizeof(int) * (n + 1),
                            cudaMemcpyHostToDevice, st));
   if (nnz > 0) {
-    BK_CHECK(cudaMemcpyAsync(out.col, cc.data(), sizeof(int) * nnz,
+    BK_CHECK(cudaMemcpyAsync(out.col, cc, sizeof(int) * nnz,
                              cudaMemcpyHostToDevice, st));
-    BK_CHECK(cudaMemcpyAsync(out.val, vv.data(), sizeof(double2) * nnz,
+    BK_CHECK(cudaMemcpyAsync(out.val, vv, sizeof(double2) * nnz,
                              cudaMemcpyHostToDevice, st));
   }
-  std::vector<int> rb = make_row_blocks(n, rp.data());
+  std::vector<int> rb = make_row_blocks(n, rp);
   out.nrb = (int)rb.size() - 1;
   out.rb = dalloc_n<int>((long long)rb.size(), st);
   BK_CHECK(cudaMemcpyAsync(out.rb, rb.data(), sizeof(int) * rb.size(),
                            cudaMemcpyHostToDevice, st));
   // Sliced-ELL copy (32-row slices, entries column-major within a slice,
-  // each row in CSR order, padding column -1) unless padding would exceed
-  // half the entries.
+  // each row in CSR order, padding column -1), placed on the GPU, unless
+  // padding would exceed half the entries.
   const int nslice = (n + 31) / 32;
   std::vector<int> sp((size_t)nslice + 1, 0);
   long long total = 0;
@@ -135,31 +140,15 @@ void upload_zcsr(int n, const int* rowptr, const int* col, const double* val,
     total += 32LL * w;
     sp[s + 1] = (int)std::min(total, 0x7fffff00LL);
   }
-  std::vector<int> scol;
-  std::vector<double> sval;
   if (total <= 0x7fffff00LL && total <= (long long)nnz * 3 / 2 + 64) {
-    scol.assign((size_t)total, -1);
-    sval.assign(2 * (size_t)total, 0.0);
-    for (int r = 0; r < n; ++r) {
-      const int s = r >> 5, lane = r & 31;
-      for (int k = rp[r]; k < rp[r + 1]; ++k) {
-        const size_t o = (size_t)sp[s] + 32 * (size_t)(k - rp[r]) + lane;
-        scol[o] = cc[k];
-        sval[2 * o] = vv[2 * (size_t)k];
-        sval[2 * o + 1] = vv[2 * (size_t)k + 1];
-      }
-    }
     out.sptr = dalloc_n<int>(nslice + 1, st);
     out.scol = dalloc_n<int>(total, st);
     out.sval = dalloc_n<double2>(total, st);
     BK_CHECK(cudaMemcpyAsync(out.sptr, sp.data(), sizeof(int) * (nslice + 1),
                              cudaMemcpyHostToDevice, st));
-    if (total > 0) {
-      BK_CHECK(cudaMemcpyAsync(out.scol, scol.data(), sizeof(int) * total,
-                               cudaMemcpyHostToDevice, st));
-      BK_CHECK(cudaMemcpyAsync(out.sval, sval.data(), sizeof(double2) * total,
-                               cudaMemcpyHostToDevice, st));
-    }
+    launch_csr2sell_z(out.rowptr, out.col, out.val, n, nslice, out.sptr,
+                      out.scol, out.sval, st);
+    BK_CHECK(cudaGetLastError());
     out.nslice = nslice;
   }
   // The host vectors above must outlive the copies.
