@@ -1010,10 +1010,37 @@ def run_spmv_general(a):
             row[key + "_frac"] = alg / (us * 1e-6) / 1e9 / peak
         out[name] = row
     G.variant(tuned)
+    G.close()
+    # The block product (s = 16) on the unpermuted operator, both kernels:
+    # algorithmic bytes = the format's matrix bytes + X once + Y once.
+    rp, c, v, n = P.convdiff3d(a.nx)
+    G = B.GpuMatrix(B.CsrMatrix(rp, c, v), B.FP32)
+    nd = len(G.diagonals())
+    spmm = {}
+    for f32, w, dt in ((False, 8, torch.float64), (True, 4, torch.float32)):
+        X = torch.rand(n * 16, dtype=dt, device="cuda")
+        Y = torch.empty_like(X)
+        for kern, name in ((0, "dia"), (1, "csr")):
+            for _ in range(3):
+                G.spmm(16, X.data_ptr(), Y.data_ptr(), f32, kern, sp_)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(20):
+                G.spmm(16, X.data_ptr(), Y.data_ptr(), f32, kern, sp_)
+            e1.record(stream)
+            e1.synchronize()
+            us = e0.elapsed_time(e1) / 20 * 1e3
+            mat = nd * w * n + n if name == "dia" else nnz * (w + 4) + 4 * (n + 1)
+            alg = mat + 2 * 16 * w * n
+            key = f"{name}_{'fp32' if f32 else 'fp64'}"
+            spmm[key + "_us"] = us
+            spmm[key + "_frac"] = alg / (us * 1e-6) / 1e9 / peak
     line = {"metric": "SpMV time on an operator without a diagonal form",
             "workload": f"permuted convdiff3d {a.nx}^3", "n": n, "nnz": nnz,
             "peak_gbs": peak, "autotuned": G.SPMV_VARIANTS[tuned],
-            "variants": out, "timing": "hot, CUDA events, 50 launches"}
+            "variants": out, "timing": "hot, CUDA events, 50 launches",
+            "spmm_s16_unpermuted": spmm}
     print(json.dumps(line), flush=True)
     G.close()
     return 0

@@ -130,6 +130,7 @@ def _load():
     L.bksp_gpu_solve.argtypes = [vp, i, i, vp, vp, d, i, vp, C.POINTER(Stats)]
     L.bksp_gpu_spmv.argtypes = [vp, i, vp, vp, vp]
     L.bksp_gpu_matrix_variant.argtypes = [vp, i]
+    L.bksp_gpu_spmm.argtypes = [vp, i, i, i, vp, vp, vp]
     L.bksp_gpu_matrix_diagonals.argtypes = [vp, C.POINTER(C.c_int)]
     L.bksp_gpu_read_matrix_market.argtypes = [C.c_char_p, i, C.POINTER(vp)]
     L.bksp_gpu_matrix_csr.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), _dp]
@@ -568,6 +569,14 @@ class GpuMatrix:
         rc = lib.bksp_gpu_spmv(self.h, int(bool(fp32)), x_ptr, y_ptr, stream)
         if rc != 0:
             raise RuntimeError("bksp_gpu_spmv failed")
+
+    def spmm(self, s, X_ptr, Y_ptr, fp32=False, kernel=-1, stream=None):
+        """Y = A X for row-major device blocks (n x s); kernel -1 autotuned,
+        0 diagonal form, 1 CSR."""
+        rc = lib.bksp_gpu_spmm(self.h, int(fp32), int(s), int(kernel), X_ptr,
+                               Y_ptr, stream)
+        if rc != 0:
+            raise RuntimeError(f"bksp_gpu_spmm failed ({rc})")
 
     def true_residual(self, b_ptr, x_ptr, stream=None):
         return lib.bksp_gpu_true_residual(self.h, b_ptr, x_ptr, stream)

@@ -626,6 +626,7 @@ extern "C" int bksp_gpu_dcsrmm(dspmat* A, char trans, int s, double alpha,
     a.alpha = alpha;
     a.mode = 1;
     a.s = s;
+    spmm_autotune(dA.h64(), s, 0, st);
     launch_spmm(dA.h64(), a, ss.red(kD, E_NONE), st);
     BK_CHECK(cudaGetLastError());
     launch_rm2cm(dC, tmp, n, s, st);

@@ -216,6 +216,39 @@ int bksp_gpu_spmv(bksp_gpu_matrix* m, int fp32, const void* x, void* y,
   }
 }
 
+int bksp_gpu_spmm(bksp_gpu_matrix* m, int fp32, int s, int kernel,
+                  const void* X, void* Y, void* stream) {
+  if (!m || !X || !Y || s < 1 || s > 16 || kernel < -1 || kernel > 1)
+    return INVALID_PARAMETERS;
+  if (fp32 && !m->A.v32) return INVALID_PARAMETERS;
+  try {
+    cudaStream_t st = pick(stream);
+    thread_local SolveState ss;
+    thread_local bool ready = false;
+    if (!ready) {
+      ss.create(0, st);
+      ss.start(0, 1, 0.0, st);
+      ready = true;
+    }
+    CsrH h = fp32 ? m->A.h32() : m->A.h64();
+    if (kernel == 1) h.dia.nd = 0;   // the CSR kernel
+    SpmmH a{};
+    a.X = static_cast<const double*>(X);
+    a.Y = static_cast<double*>(Y);
+    a.alpha = 1.0;
+    a.s = s;
+    a.prec = fp32 ? 1 : 0;
+    if (kernel == -1) spmm_autotune(h, s, a.prec, st);
+    spmm_force(kernel);
+    launch_spmm(h, a, ss.red(kD, E_NONE), st);
+    spmm_force(-1);
+    BK_CHECK(cudaGetLastError());
+    return 0;
+  } catch (const std::exception& e) {
+    return fail(e);
+  }
+}
+
 double bksp_gpu_true_residual(bksp_gpu_matrix* m, const double* b,
                               const double* x, void* stream) {
   if (!m || !b || !x) return NAN;

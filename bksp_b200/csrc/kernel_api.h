@@ -301,6 +301,12 @@ struct BlkH {
   int prec;
 };
 void launch_spmm(const CsrH& A, const SpmmH& a, const RedH& rd, cudaStream_t st);
+// Time the diagonal-form and CSR block products for A at width s once
+// (outside stream capture) and cache the faster for launch_spmm.
+void spmm_autotune(const CsrH& A, int s, int prec, cudaStream_t st);
+// This thread's next launch_spmm calls: 0 the diagonal form where usable,
+// 1 CSR, -1 the cached choice.
+void spmm_force(int kernel);
 void launch_block(const BlkH& a, const RedH& rd, cudaStream_t st);
 void launch_cm2rm(const double* cm, double* rm, int n, int s, cudaStream_t st);
 void launch_rm2cm(const double* rm, double* cm, int n, int s, cudaStream_t st);

@@ -1,10 +1,12 @@
 // Shifted-method and block-method kernels and their launch wrappers
 // (kernel_api.h).
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "dev_common.cuh"
 #include "epilogues.cuh"
@@ -50,15 +52,101 @@ static bool spmm_dia_off() {
   return off;
 }
 
+// SpMM autotuner: for an operator with a diagonal form, the faster of the
+// diagonal-form and CSR kernels per (rows, entries, s, precision, device),
+// timed once outside any stream capture (spmm_autotune) and cached; the two
+// give bit-identical results.  Until a choice exists, the diagonal form.
+namespace {
+struct SpmmKey {
+  int n, nnz, s, prec, dev;
+  bool operator==(const SpmmKey& o) const {
+    return n == o.n && nnz == o.nnz && s == o.s && prec == o.prec && dev == o.dev;
+  }
+};
+std::mutex g_spmm_mu;
+std::vector<std::pair<SpmmKey, int>> g_spmm_choice;   // 0 diagonal form, 1 CSR
+thread_local int g_spmm_force = -1;                     // set while timing
+
+int spmm_cached(const CsrH& A, int s, int prec) {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const SpmmKey key{A.n, A.nnz, s, prec, dev};
+  std::lock_guard<std::mutex> lk(g_spmm_mu);
+  for (const auto& kv : g_spmm_choice)
+    if (kv.first == key) return kv.second;
+  return -1;
+}
+}  // namespace
+
+void spmm_force(int kernel) { g_spmm_force = kernel; }
+
+void spmm_autotune(const CsrH& A, int s, int prec, cudaStream_t st) {
+  if (A.dia.nd == 0 || spmm_dia_off() || A.n < (1 << 14)) return;
+  const char* e = std::getenv("BKSP_GPU_AUTOTUNE");
+  if (e && std::strcmp(e, "0") == 0) return;
+  if (spmm_cached(A, s, prec) >= 0) return;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const size_t w = prec == 1 ? sizeof(float) : sizeof(double);
+  const size_t bytes = (size_t)A.n * (size_t)s * w;
+  void *X = nullptr, *Y = nullptr;
+  CtlH* ctl = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  float best[2] = {1e30f, 1e30f};
+  bool ok = cudaMallocAsync(&X, bytes, st) == cudaSuccess &&
+            cudaMallocAsync(&Y, bytes, st) == cudaSuccess &&
+            cudaMallocAsync(reinterpret_cast<void**>(&ctl), sizeof(CtlH), st) == cudaSuccess &&
+            cudaMemsetAsync(X, 0, bytes, st) == cudaSuccess &&
+            cudaMemsetAsync(ctl, 0, sizeof(CtlH), st) == cudaSuccess &&
+            cudaEventCreate(&e0) == cudaSuccess && cudaEventCreate(&e1) == cudaSuccess;
+  if (ok) {
+    SpmmH a{};
+    a.X = static_cast<const double*>(X);
+    a.Y = static_cast<double*>(Y);
+    a.alpha = 1.0;
+    a.s = s;
+    a.prec = prec;
+    const RedH rd{nullptr, nullptr, nullptr, ctl, 0, 0, 0, 0, 0};
+    const long long l0 = launch_count();
+    for (int round = 0; round < 2 && ok; ++round)
+      for (int v = 0; v < 2 && ok; ++v) {
+        g_spmm_force = v;
+        launch_spmm(A, a, rd, st);
+        ok = cudaEventRecord(e0, st) == cudaSuccess;
+        for (int r = 0; r < 5; ++r) launch_spmm(A, a, rd, st);
+        ok = ok && cudaEventRecord(e1, st) == cudaSuccess &&
+             cudaEventSynchronize(e1) == cudaSuccess;
+        float ms = 0.f;
+        if (ok && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess)
+          best[v] = std::min(best[v], ms);
+      }
+    g_spmm_force = -1;
+    launch_count() = l0;
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (X) cudaFreeAsync(X, st);
+  if (Y) cudaFreeAsync(Y, st);
+  if (ctl) cudaFreeAsync(ctl, st);
+  cudaGetLastError();
+  if (!ok) return;
+  const int choice = best[1] < 0.98f * best[0] ? 1 : 0;   // CSR only if clearly faster
+  std::lock_guard<std::mutex> lk(g_spmm_mu);
+  g_spmm_choice.push_back({SpmmKey{A.n, A.nnz, s, prec, dev}, choice});
+}
+
 void launch_spmm(const CsrH& A, const SpmmH& a, const RedH& rd, cudaStream_t st) {
   if (g_prog_rec) prog_unsupported("block / shifted kernel");
   ++launch_count();
   // Diagonal form: 16-byte row segments (s a multiple of the vector width,
-  // aligned blocks); else the CSR kernel.
+  // aligned blocks) unless the autotuner found the CSR kernel faster; else
+  // the CSR kernel.
   auto al = [](const void* p) { return ((uintptr_t)p & 15u) == 0; };
   const int vn = a.prec == 1 ? 4 : 2;
+  const int pick = g_spmm_force >= 0 ? g_spmm_force
+                                     : (A.dia.nd > 0 ? spmm_cached(A, a.s, a.prec) : 1);
   if (A.dia.nd > 0 && a.s % vn == 0 && al(a.X) && al(a.Y) && al(a.C) && al(a.W) &&
-      !spmm_dia_off()) {
+      !spmm_dia_off() && pick != 1) {
     const long long rows = A.n;
     const long long per = kThreads / (a.s / vn);
     const long long items = rows * (a.s / vn);

@@ -91,7 +91,15 @@ SpmmH spmm_args(const T* X, T* Y, int s, double alpha = 1.0, const T* C = nullpt
 
 void spmm(const DevCsr& A, const SpmmH& a, const RedH& rd, cudaStream_t st) {
   if (a.prec == 1 && !A.v32) throw CudaError("FP32 block product: FP32 values missing");
-  launch_spmm(a.prec == 1 ? A.h32() : A.h64(), a, rd, st);
+  const CsrH h = a.prec == 1 ? A.h32() : A.h64();
+  // The drivers' first products run before their loops are captured: the
+  // autotuner's one-time timing happens there.
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (!g_prog_rec && cudaStreamIsCapturing(st, &cs) == cudaSuccess &&
+      cs == cudaStreamCaptureStatusNone)
+    spmm_autotune(h, a.s, a.prec, st);
+  cudaGetLastError();
+  launch_spmm(h, a, rd, st);
 }
 
 }  // namespace

@@ -154,6 +154,14 @@ int bksp_gpu_matrix_diagonals(const bksp_gpu_matrix *A, int *offsets);
 int bksp_gpu_spmv(bksp_gpu_matrix *A, int fp32, const void *x, void *y,
                   void *stream);
 
+/* Y = A X for row-major device blocks of n x s (s <= 16), FP64 (fp32 = 0)
+ * or FP32 (fp32 = 1, needs BKSP_GPU_FP32): the block methods' product.
+ * kernel: -1 the autotuned choice, 0 the diagonal form (operators that
+ * have one, s a multiple of the 16-byte vector), 1 CSR.  Asynchronous on
+ * `stream`.  For kernel timing. */
+int bksp_gpu_spmm(bksp_gpu_matrix *A, int fp32, int s, int kernel,
+                  const void *X, void *Y, void *stream);
+
 /* FP64 ||b - A x||_2 / ||b||_2 of device vectors (synchronous). */
 double bksp_gpu_true_residual(bksp_gpu_matrix *A, const double *b,
                               const double *x, void *stream);
