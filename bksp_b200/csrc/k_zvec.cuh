@@ -351,7 +351,7 @@ __device__ __forceinline__ void zblk_finish(const double* g, int ng, int s,
                                             const double* dd, int nd,
                                             const short* gslot, const Red& rd);
 
-__global__ void __launch_bounds__(kThreads, 2)
+__global__ void __launch_bounds__(kThreads, 3)
 k_zblock(ZBlkH a, Red rd) {
   if (skip(rd)) return;
   __shared__ double2 tile[6][kZBlkRows][17];
@@ -382,12 +382,26 @@ k_zblock(ZBlkH a, Red rd) {
   double g[4] = {0.0, 0.0, 0.0, 0.0};
   double dd[4] = {0.0, 0.0, 0.0, 0.0};
   const long long ntiles = (a.n + kZBlkRows - 1) / kZBlkRows;
+  // The next tile's inputs are loaded into registers while the current
+  // tile is computed, so a tile's global loads overlap the previous one's
+  // work.
+  double2 pre[4];
+  auto fetch = [&](long long tl) {
+    const long long row = tl * kZBlkRows + r;
+    const bool ok = c < s && row < a.n && tl < ntiles;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+      pre[i] = (i < a.nin && ok) ? a.in[i][row * s + c] : make_double2(0.0, 0.0);
+  };
+  fetch(blockIdx.x);
   for (long long tl = blockIdx.x; tl < ntiles; tl += gridDim.x) {
     const long long row = tl * kZBlkRows + r;
     const bool valid = c < s && row < a.n;
-    for (int i = 0; i < a.nin; ++i)
-      tile[i][r][c] = valid ? a.in[i][row * s + c] : make_double2(0.0, 0.0);
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+      if (i < a.nin) tile[i][r][c] = pre[i];
     __syncthreads();
+    fetch(tl + gridDim.x);
     for (int o = 0; o < a.nout; ++o) {
       double2 y = make_double2(0.0, 0.0);
       bool first = true;
