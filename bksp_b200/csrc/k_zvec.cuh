@@ -106,47 +106,60 @@ k_zlc(ZLcH a, Red rd) {
   const int nin = a.nin, nout = a.nout, nd = a.nd;
   const unsigned irep = a.in_rep_mask, orep = a.out_rep_mask;
   const long long step = (long long)gridDim.x * kThreads;
+  // Up to two elements per thread and sweep (narrow combinations): all of
+  // both elements' input loads are in flight together.
+  constexpr int UN = MI <= 8 ? 2 : 1;
   for (int rep = 0; rep < a.reps; ++rep) {
     const long long ioff = rep * a.stride;
-    for (long long e = (long long)blockIdx.x * kThreads + t; e < n; e += step) {
-      double2 v[MI];
+    for (long long e0 = (long long)blockIdx.x * kThreads + t; e0 < n; e0 += step * UN) {
+      double2 v[UN][MI];
 #pragma unroll
-      for (int i = 0; i < MI; ++i)
-        v[i] = i < nin ? __ldg(ip[i] + (((irep >> i) & 1u) ? ioff : 0) + e)
-                       : make_double2(0.0, 0.0);
-      double2 y[MO];
+      for (int q = 0; q < UN; ++q) {
+        const long long e = e0 + q * step;
 #pragma unroll
-      for (int o = 0; o < MO; ++o) {
-        y[o] = make_double2(0.0, 0.0);
-        if (o < nout) {
-          const unsigned u = used[o];
-          bool any = false;
-#pragma unroll
-          for (int i = 0; i < MI; ++i) {
-            if ((u >> i) & 1u) {
-              y[o] = any ? zfma(cs[o][i], v[i], y[o]) : zmul_f(cs[o][i], v[i]);
-              any = true;
-            }
-          }
-          op[o][(((orep >> o) & 1u) ? ioff : 0) + e] = y[o];
-        }
+        for (int i = 0; i < MI; ++i)
+          v[q][i] = (i < nin && e < n)
+                        ? __ldg(ip[i] + (((irep >> i) & 1u) ? ioff : 0) + e)
+                        : make_double2(0.0, 0.0);
       }
 #pragma unroll
-      for (int d = 0; d < kZDots; ++d) {
-        if (d < nd) {
-          double2 du = make_double2(0.0, 0.0), dv = du;
-          const int c0 = dcode[d][0], c1 = dcode[d][1];
+      for (int q = 0; q < UN; ++q) {
+        const long long e = e0 + q * step;
+        if (e >= n) break;
+        double2 y[MO];
 #pragma unroll
-          for (int i = 0; i < MI; ++i) {
-            if (c0 == i) du = v[i];
-            if (c1 == i) dv = v[i];
-          }
+        for (int o = 0; o < MO; ++o) {
+          y[o] = make_double2(0.0, 0.0);
+          if (o < nout) {
+            const unsigned u = used[o];
+            bool any = false;
 #pragma unroll
-          for (int o = 0; o < MO; ++o) {
-            if (c0 == 100 + o) du = y[o];
-            if (c1 == 100 + o) dv = y[o];
+            for (int i = 0; i < MI; ++i) {
+              if ((u >> i) & 1u) {
+                y[o] = any ? zfma(cs[o][i], v[q][i], y[o]) : zmul_f(cs[o][i], v[q][i]);
+                any = true;
+              }
+            }
+            op[o][(((orep >> o) & 1u) ? ioff : 0) + e] = y[o];
           }
-          zdot_acc(du, dv, dconj[d] != 0, acc[2 * d], acc[2 * d + 1]);
+        }
+#pragma unroll
+        for (int d = 0; d < kZDots; ++d) {
+          if (d < nd) {
+            double2 du = make_double2(0.0, 0.0), dv = du;
+            const int c0 = dcode[d][0], c1 = dcode[d][1];
+#pragma unroll
+            for (int i = 0; i < MI; ++i) {
+              if (c0 == i) du = v[q][i];
+              if (c1 == i) dv = v[q][i];
+            }
+#pragma unroll
+            for (int o = 0; o < MO; ++o) {
+              if (c0 == 100 + o) du = y[o];
+              if (c1 == 100 + o) dv = y[o];
+            }
+            zdot_acc(du, dv, dconj[d] != 0, acc[2 * d], acc[2 * d + 1]);
+          }
         }
       }
     }
