@@ -70,3 +70,29 @@ def test_block_gram_update_through_qr(gpu, s, m):
     assert np.abs(Q @ R - V).max() <= 1e-12 * np.abs(V).max()
     assert np.allclose(np.tril(R, -1), 0.0)
     assert (np.diag(R) > 0).all()
+
+
+@pytest.mark.parametrize("fp32", [False, True])
+def test_spmm_kernels_bit_identical_and_autotuned(gpu, fp32):
+    """The diagonal-form and CSR block products add each row's entries in
+    the same order with the same rounding, so they agree bit for bit; the
+    autotuned launch (either of them) gives the same block."""
+    import torch
+    rp, c, v, n = P.convdiff3d(48)
+    G = gpu.GpuMatrix(gpu.CsrMatrix(rp, c, v), gpu.FP32)
+    assert len(G.diagonals()) == 7
+    dt = torch.float32 if fp32 else torch.float64
+    X = torch.rand(n * 16, dtype=dt, device="cuda") * 2 - 1
+    outs = []
+    for kern in (0, 1, -1):
+        Y = torch.full_like(X, float("nan"))
+        G.spmm(16, X.data_ptr(), Y.data_ptr(), fp32, kern)
+        torch.cuda.synchronize()
+        outs.append(Y.cpu().numpy())
+    assert np.array_equal(outs[0], outs[1])
+    assert np.array_equal(outs[0], outs[2])
+    A = sp.csr_matrix((v, c, rp), shape=(n, n))
+    ref = A @ X.cpu().numpy().astype(np.float64).reshape(n, 16)
+    np.testing.assert_allclose(outs[0].reshape(n, 16), ref,
+                               rtol=1e-4 if fp32 else 1e-12, atol=1e-4 if fp32 else 1e-12)
+    G.close()
