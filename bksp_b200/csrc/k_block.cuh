@@ -90,7 +90,7 @@ template <> struct Vec16<double> { using V = double2; static constexpr int N = 2
 template <> struct Vec16<float> { using V = float4; static constexpr int N = 4; };
 
 template <typename T, int ND>
-__global__ void __launch_bounds__(kThreads, 4)
+__global__ void __launch_bounds__(kThreads, 3)
 k_spmm_dia(CsrH A, SpmmArgs<T> a, Red rd) {
   if (skip(rd)) return;
   using PV = typename Vec16<T>::V;
@@ -112,15 +112,30 @@ k_spmm_dia(CsrH A, SpmmArgs<T> a, Red rd) {
     T y[VN];
 #pragma unroll
     for (int e = 0; e < VN; ++e) y[e] = T(0);
+    // Every diagonal's value and X segment are loaded before the first is
+    // used (a row index clamped into range where the row lacks the
+    // diagonal: a valid address whose value is then not used), so all of a
+    // row's loads are in flight together; the adds keep ascending diagonal
+    // order and only the stored entries enter.
+    T av[kDiaMax];
+    PV xp[kDiaMax];
+#pragma unroll
+    for (int d = 0; d < kDiaMax; ++d) {
+      if (d < nd) {
+        long long j = row + A.dia.off[d];
+        j = j < 0 ? 0 : (j >= n ? n - 1 : j);
+        av[d] = __ldg(V + d * stride + row);
+        xp[d] = __ldg(reinterpret_cast<const PV*>(a.X + j * s) + q);
+      }
+    }
 #pragma unroll
     for (int d = 0; d < kDiaMax; ++d) {
       if (d < nd && ((m >> d) & 1u)) {
-        const T av = mul_rn(alpha, __ldg(V + d * stride + row));
-        const long long j = row + A.dia.off[d];
+        const T avd = mul_rn(alpha, av[d]);
         T xv[VN];
-        unpack<T>(__ldg(reinterpret_cast<const PV*>(a.X + j * s) + q), xv);
+        unpack<T>(xp[d], xv);
 #pragma unroll
-        for (int e = 0; e < VN; ++e) y[e] = add_rn(y[e], mul_rn(av, xv[e]));
+        for (int e = 0; e < VN; ++e) y[e] = add_rn(y[e], mul_rn(avd, xv[e]));
       }
     }
     const long long o = row * s + q * VN;
