@@ -34,7 +34,7 @@ struct SpmmArgs {
 };
 
 template <typename T, int ND>
-__global__ void __launch_bounds__(kThreads, 4)
+__global__ void __launch_bounds__(kThreads, 8)
 k_spmm(CsrH A, SpmmArgs<T> a, Red rd) {
   if (skip(rd)) return;
   const T* __restrict__ val = static_cast<const T*>(A.val);
@@ -50,24 +50,9 @@ k_spmm(CsrH A, SpmmArgs<T> a, Red rd) {
     if (lane < s) {
       T y = T(0);
       const int k0 = __ldg(A.rowptr + row), k1 = __ldg(A.rowptr + row + 1);
-      // Rounds of eight entries: the round's column indices and values,
-      // then its X row segments, are all in flight before the first add
-      // (the entries are still added in CSR order).
-      for (int kb = k0; kb < k1; kb += 8) {
-        int cc[8];
-        T vv[8], xv[8];
-#pragma unroll
-        for (int u = 0; u < 8; ++u) {
-          const bool in = kb + u < k1;
-          cc[u] = in ? __ldg(A.col + kb + u) : 0;
-          vv[u] = in ? __ldg(val + kb + u) : T(0);
-        }
-#pragma unroll
-        for (int u = 0; u < 8; ++u)
-          xv[u] = kb + u < k1 ? __ldg(a.X + (long long)cc[u] * s + lane) : T(0);
-#pragma unroll
-        for (int u = 0; u < 8; ++u)
-          if (kb + u < k1) y = add_rn(y, mul_rn(mul_rn(alpha, vv[u]), xv[u]));
+      for (int k = k0; k < k1; ++k) {
+        const T av = mul_rn(alpha, __ldg(val + k));
+        y = add_rn(y, mul_rn(av, __ldg(a.X + (long long)__ldg(A.col + k) * s + lane)));
       }
       const long long o = (long long)row * s + lane;
       if (a.mode == 1) y = add_rn(a.C[o], y);
