@@ -196,26 +196,19 @@ void launch_block(const BlkH& a, const RedH& rd, cudaStream_t st) {
   static_assert(sizeof(BlkArgs<double>) == sizeof(BlkH), "BlkArgs layout");
   static_assert(sizeof(BlkArgs<float>) == sizeof(BlkH), "BlkArgs layout");
   const long long tiles = (a.n + kBlkTileRows - 1) / kBlkTileRows;
-  // A launch with Gram products or dots ends in the last CTA summing every
-  // CTA's partials (blk_finish): its grid is capped at two CTAs per SM so
-  // that serial tail stays short; the others run one full wave.
-  const bool reduces = a.ng > 0 || a.nd > 0;
-  auto grid_of = [&](int cap) {
-    if (reduces) cap = std::min(cap, 2 * kSMs);
-    const long long g = tiles < cap ? tiles : cap;
-    return (int)(g < 1 ? 1 : g);
-  };
   if (a.prec == 1) {
     BlkArgs<float> b;
     memcpy(&b, &a, sizeof(b));
-    const int g = grid_of(resident_grid(reinterpret_cast<const void*>(k_block<float>)));
-    launch_k(k_block<float>, g, kThreads, 0, st, b, rd);
+    const int cap = resident_grid(reinterpret_cast<const void*>(k_block<float>));
+    int g = (int)(tiles < cap ? tiles : cap);
+    launch_k(k_block<float>, g < 1 ? 1 : g, kThreads, 0, st, b, rd);
     return;
   }
   BlkArgs<double> b;
   memcpy(&b, &a, sizeof(b));
-  const int g = grid_of(resident_grid(reinterpret_cast<const void*>(k_block<double>)));
-  launch_k(k_block<double>, g, kThreads, 0, st, b, rd);
+  const int cap = resident_grid(reinterpret_cast<const void*>(k_block<double>));   // one wave
+  int g = (int)(tiles < cap ? tiles : cap);
+  launch_k(k_block<double>, g < 1 ? 1 : g, kThreads, 0, st, b, rd);
 }
 
 // Column-major n x s (leading dimension n) <-> row-major np x s.
