@@ -168,7 +168,28 @@ struct BlkArgs {
 
 __device__ __forceinline__ void blk_finish(const double* g, int ng, int s,
                                            const double* dd, int nd,
-                                           const short* gslot, const Red& rd);
+                                           const short* gslot, const Red& rd,
+                                           double* stage);
+
+// Scalar slots a block epilogue may touch: the common and recurrence
+// slots below the first s-by-s cell and the cells kBkG1 .. kBkScr2.  The
+// last CTA stages them in shared memory for the epilogue (its s-by-s
+// algebra is a long dependent chain of loads and stores; in shared memory
+// each costs tens of cycles instead of an L2 round trip) and writes them
+// back afterwards.
+constexpr int kBlkEpiSlots = bk_cell(19);
+
+template <typename T>
+struct BlkSmem {
+  T tile[6][kBlkTileRows][kBlkS + 1];
+  T mat[2][4][kBlkS * kBlkS];
+  T cs[2][4];
+};
+template <typename T>
+constexpr size_t blk_smem_bytes() {
+  return sizeof(BlkSmem<T>) > sizeof(double) * kBlkEpiSlots
+             ? sizeof(BlkSmem<T>) : sizeof(double) * kBlkEpiSlots;
+}
 
 // Terms are formed in T (the block's element type); Gram products and dots
 // accumulate in FP64 either way.
@@ -176,9 +197,13 @@ template <typename T>
 __global__ void __launch_bounds__(kThreads, 4)
 k_block(BlkArgs<T> a, Red rd) {
   if (skip(rd)) return;
-  __shared__ T tile[6][kBlkTileRows][kBlkS + 1];
-  __shared__ T mat[2][4][kBlkS * kBlkS];
-  __shared__ T cs[2][4];
+  // The tiles and matrices share their storage with the epilogue's staged
+  // slots (used only after the last tile).
+  __shared__ __align__(16) unsigned char raw[blk_smem_bytes<T>()];
+  BlkSmem<T>& sm = *reinterpret_cast<BlkSmem<T>*>(raw);
+  auto& tile = sm.tile;
+  auto& mat = sm.mat;
+  auto& cs = sm.cs;
   const int s = a.s;
   const int t = threadIdx.x;
   const int r = t / kBlkS, c = t % kBlkS;   // tile element of this thread
@@ -301,7 +326,8 @@ k_block(BlkArgs<T> a, Red rd) {
     }
     __syncthreads();
   }
-  if (a.ng > 0 || a.nd > 0 || rd.epi) blk_finish(gacc, a.ng, s, dacc, a.nd, a.gslot, rd);
+  if (a.ng > 0 || a.nd > 0 || rd.epi)
+    blk_finish(gacc, a.ng, s, dacc, a.nd, a.gslot, rd, reinterpret_cast<double*>(raw));
 }
 
 // Deterministic reduction of per-thread Gram entries (thread t owns entry t
@@ -310,7 +336,8 @@ k_block(BlkArgs<T> a, Red rd) {
 // part[(slot) * kMaxBlocks + block], slots 0..2*256-1 Grams, 512.. dots.
 __device__ __forceinline__ void blk_finish(const double* g, int ng, int s,
                                            const double* dd, int nd,
-                                           const short* gslot, const Red& rd) {
+                                           const short* gslot, const Red& rd,
+                                           double* stage) {
   __shared__ double wsum[2][kWarps];
   __shared__ int is_last;
   // Block-major partials (block b's kBlkPart values contiguous), so both
@@ -354,11 +381,19 @@ __device__ __forceinline__ void blk_finish(const double* g, int ng, int s,
     rd.S[rd.out + t] = v;
   }
   __syncthreads();
-  if (t == 0) {
-    *rd.ticket = 0u;
-    __threadfence();
-    if (rd.epi) run_epilogue(rd);
+  if (t == 0) *rd.ticket = 0u;
+  if (rd.epi) {
+    for (int q = t; q < kBlkEpiSlots; q += kThreads) stage[q] = __ldcg(rd.S + q);
+    __syncthreads();
+    if (t == 0) {
+      Red local = rd;
+      local.S = stage;
+      run_epilogue(local);
+    }
+    __syncthreads();
+    for (int q = t; q < kBlkEpiSlots; q += kThreads) rd.S[q] = stage[q];
   }
+  if (t == 0) __threadfence();
 }
 
 }  // namespace bk
