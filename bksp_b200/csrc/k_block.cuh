@@ -9,6 +9,7 @@
 // (row-major, M[b][c] at S[slot + b * s + c]).
 #pragma once
 #include "dev_common.cuh"
+#include "epi_block_cta.cuh"
 
 namespace bk {
 
@@ -385,11 +386,10 @@ __device__ __forceinline__ void blk_finish(const double* g, int ng, int s,
   if (rd.epi) {
     for (int q = t; q < kBlkEpiSlots; q += kThreads) stage[q] = __ldcg(rd.S + q);
     __syncthreads();
-    if (t == 0) {
-      Red local = rd;
-      local.S = stage;
-      run_epilogue(local);
-    }
+    Red local = rd;
+    local.S = stage;
+    // s-by-s algebra on all threads; the scalar epilogues on one
+    if (!run_block_epilogue_cta(local, t) && t == 0) run_epilogue(local);
     __syncthreads();
     for (int q = t; q < kBlkEpiSlots; q += kThreads) rd.S[q] = stage[q];
   }

@@ -15,6 +15,7 @@
 #include "dev_common.cuh"
 #include "solver_defs.h"
 #include "zkernel_api.h"
+#include "zepi_block_cta.cuh"
 
 namespace bk {
 
@@ -492,6 +493,7 @@ __device__ __forceinline__ void zblk_finish(const double* g, int ng, int s,
   const int r = t >> 4, c = t & 15;
   for (int q = 0; q < ng; ++q) {
     double re = 0.0, im = 0.0;
+#pragma unroll 8
     for (int b = 0; b < nb; ++b) {
       re += __ldcg(rd.part + (long long)b * kZBlkPart + q * 512 + 2 * t);
       im += __ldcg(rd.part + (long long)b * kZBlkPart + q * 512 + 2 * t + 1);
@@ -503,6 +505,7 @@ __device__ __forceinline__ void zblk_finish(const double* g, int ng, int s,
   }
   if (t < 2 * nd) {
     double v = 0.0;
+#pragma unroll 8
     for (int b = 0; b < nb; ++b) v += __ldcg(rd.part + (long long)b * kZBlkPart + 1024 + t);
     rd.S[rd.out + t] = v;
   }
@@ -510,8 +513,9 @@ __device__ __forceinline__ void zblk_finish(const double* g, int ng, int s,
   if (t == 0) {
     *rd.ticket = 0u;
     __threadfence();
-    if (rd.epi) run_epilogue(rd);
   }
+  // s-by-s algebra on all threads; the scalar epilogues on one
+  if (rd.epi && !run_zblock_epilogue_cta(rd, t) && t == 0) run_epilogue(rd);
 }
 
 // ---------------------------------------------------------- k_zshift
