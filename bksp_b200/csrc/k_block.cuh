@@ -16,6 +16,13 @@ namespace bk {
 constexpr int kBlkS = 16;           // max block width
 constexpr int kBlkTileRows = 32;    // rows per tile of the block kernel
 constexpr int kBlkSub = kBlkTileRows / (kThreads / kBlkS);   // rows per thread
+// Tile row stride: a multiple of two elements, so a row's entries can be
+// read two at a time (double2 / float2), and not of 16, so the two rows a
+// warp reads at once fall in different banks.
+constexpr int kBlkTileStride = kBlkS + 2;
+template <typename T> struct Pair;
+template <> struct Pair<double> { using V = double2; };
+template <> struct Pair<float> { using V = float2; };
 
 // ------------------------------------------------------------------ SpMM
 // Y = alpha * A X  (mode 0), Y = C + alpha * A X  (mode 1), with the
@@ -182,7 +189,7 @@ constexpr int kBlkEpiSlots = bk_cell(19);
 
 template <typename T>
 struct BlkSmem {
-  T tile[6][kBlkTileRows][kBlkS + 1];
+  T tile[6][kBlkTileRows][kBlkTileStride];
   T mat[2][4][kBlkS * kBlkS];
   T cs[2][4];
 };
@@ -193,9 +200,10 @@ constexpr size_t blk_smem_bytes() {
 }
 
 // Terms are formed in T (the block's element type); Gram products and dots
-// accumulate in FP64 either way.
+// accumulate in FP64 either way.  Three CTAs per SM (80 registers): at four
+// (64 registers) the tile loop spilled and ran ~10 % slower.
 template <typename T>
-__global__ void __launch_bounds__(kThreads, 4)
+__global__ void __launch_bounds__(kThreads, 3)
 k_block(BlkArgs<T> a, Red rd) {
   if (skip(rd)) return;
   // The tiles and matrices share their storage with the epilogue's staged
@@ -258,10 +266,16 @@ k_block(BlkArgs<T> a, Red rd) {
     // Outputs: for each term the s-by-s matrix column c is read once into
     // registers and serves all kBlkSub rows of this thread; every element's
     // terms are accumulated in input order, as before.
-    for (int o = 0; o < a.nout; ++o) {
+    // (Both loops are unrolled to their bounds so that every term's
+    // parameters and matrices are addressed statically.)
+#pragma unroll
+    for (int o = 0; o < 2; ++o) {
+      if (o >= a.nout) break;
       T y[kBlkSub];
       bool first = true;
-      for (int i = 0; i < a.nin; ++i) {
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        if (i >= a.nin) break;
         const CfH& cf = a.c[o][i];
         if (!cf.op) continue;
         if (a.mslot[o][i] >= 0) {
@@ -273,8 +287,12 @@ k_block(BlkArgs<T> a, Red rd) {
             const int rr = r + (kThreads / kBlkS) * k;
             T z = T(0);
 #pragma unroll
-            for (int b = 0; b < kBlkS; ++b)
-              if (b < s) z = fma_rn(tile[i][rr][b], mc[b], z);
+            for (int b = 0; b < kBlkS; b += 2) {
+              const typename Pair<T>::V x2 =
+                  *reinterpret_cast<const typename Pair<T>::V*>(&tile[i][rr][b]);
+              if (b < s) z = fma_rn(x2.x, mc[b], z);
+              if (b + 1 < s) z = fma_rn(x2.y, mc[b + 1], z);
+            }
             const T term = cs[o][i] * z;
             y[k] = first ? term : add_rn(y[k], term);
           }
@@ -302,7 +320,9 @@ k_block(BlkArgs<T> a, Red rd) {
       }
     }
     __syncthreads();
-    for (int g = 0; g < a.ng; ++g) {
+#pragma unroll
+    for (int g = 0; g < 2; ++g) {
+      if (g >= a.ng) break;
       // thread (r, c) accumulates G[r][c] = sum_rows U[row][r] V[row][c]
       const int u = a.gram[g][0], v = a.gram[g][1];
       const int tu = u < a.nin ? u : 4 + (u - a.nin);
@@ -315,7 +335,9 @@ k_block(BlkArgs<T> a, Red rd) {
         gacc[g] = z;
       }
     }
-    for (int d = 0; d < a.nd; ++d) {
+#pragma unroll
+    for (int d = 0; d < 2; ++d) {
+      if (d >= a.nd) break;
       const int u = a.dot[d][0], v = a.dot[d][1];
       const int tu = u < a.nin ? u : 4 + (u - a.nin);
       const int tv = v < a.nin ? v : 4 + (v - a.nin);
@@ -332,24 +354,36 @@ k_block(BlkArgs<T> a, Red rd) {
 }
 
 // Deterministic reduction of per-thread Gram entries (thread t owns entry t
-// of each Gram) and Frobenius dots across the grid; the last block writes
-// the sums to the scalar slots and runs the epilogue.  Partials layout:
-// part[(slot) * kMaxBlocks + block], slots 0..2*256-1 Grams, 512.. dots.
+// of each Gram) and Frobenius dots across the grid, in two levels: the
+// last block of each group of kRedGroup blocks sums its group's partials
+// in block order, the last such group block sums the group sums in group
+// order, writes them to the scalar slots and runs the epilogue.  (One
+// level over all ~600 blocks' partials was a chain of dependent batches
+// of L2 loads on one SM; two levels need a handful.)  Partials: block b's
+// kBlkPart values contiguous (Grams at q * 256, dots at 512), so writes
+// and reads are coalesced.
 __device__ __forceinline__ void blk_finish(const double* g, int ng, int s,
                                            const double* dd, int nd,
                                            const short* gslot, const Red& rd,
                                            double* stage) {
   __shared__ double wsum[2][kWarps];
   __shared__ int is_last;
-  // Block-major partials (block b's kBlkPart values contiguous), so both
-  // the writes here and the last block's reads are coalesced, and a
-  // thread's reads of consecutive blocks are independent loads the loop
-  // keeps in flight together.
   constexpr int kBlkPart = 514;
   const int t = threadIdx.x;
+  const int nb = gridDim.x;
+  const int grp = blockIdx.x / kRedGroup;
+  const int b0 = grp * kRedGroup;
+  const int gn = min(kRedGroup, nb - b0);
+  const int ngrp = (nb + kRedGroup - 1) / kRedGroup;
+  double* gpart = rd.part + (long long)kGridCap * kBlkPart;
+  unsigned* gticket = reinterpret_cast<unsigned*>(rd.part + red2_ticket_offset(kBlkPart));
   double* mine = rd.part + (long long)blockIdx.x * kBlkPart;
-  for (int q = 0; q < ng; ++q) mine[q * 256 + t] = g[q];
-  for (int d = 0; d < nd; ++d) {
+#pragma unroll
+  for (int q = 0; q < 2; ++q)
+    if (q < ng) mine[q * 256 + t] = g[q];
+#pragma unroll
+  for (int d = 0; d < 2; ++d) {
+    if (d >= nd) break;
     const double v = warp_sum(dd[d]);
     if ((t & 31) == 0) wsum[d][t >> 5] = v;
   }
@@ -361,24 +395,49 @@ __device__ __forceinline__ void blk_finish(const double* g, int ng, int s,
       mine[512 + d] = v;
     }
     __threadfence();
-    const unsigned tk = atomicAdd(rd.ticket, 1u);
-    is_last = (tk == gridDim.x - 1);
+    is_last = atomicAdd(gticket + grp, 1u) == (unsigned)gn - 1;
   }
   __syncthreads();
   if (!is_last) return;
   __threadfence();
-  const int nb = gridDim.x;
+  // Level 1: this group's blocks.
+  const double* gp = rd.part + (long long)b0 * kBlkPart;
+  double* gout = gpart + (long long)grp * kBlkPart;
+  for (int q = 0; q < ng; ++q) {
+    double v = 0.0;
+#pragma unroll
+    for (int b = 0; b < kRedGroup; ++b)
+      if (b < gn) v += __ldcg(gp + (long long)b * kBlkPart + q * 256 + t);
+    gout[q * 256 + t] = v;
+  }
+  if (t < nd) {
+    double v = 0.0;
+#pragma unroll
+    for (int b = 0; b < kRedGroup; ++b)
+      if (b < gn) v += __ldcg(gp + (long long)b * kBlkPart + 512 + t);
+    gout[512 + t] = v;
+  }
+  __syncthreads();
+  if (t == 0) {
+    gticket[grp] = 0u;
+    __threadfence();
+    is_last = atomicAdd(rd.ticket, 1u) == (unsigned)ngrp - 1;
+  }
+  __syncthreads();
+  if (!is_last) return;
+  __threadfence();
+  // Level 2: the groups.
   const int r = t / kBlkS, c = t % kBlkS;
   for (int q = 0; q < ng; ++q) {
     double v = 0.0;
 #pragma unroll 16
-    for (int b = 0; b < nb; ++b) v += __ldcg(rd.part + (long long)b * kBlkPart + q * 256 + t);
+    for (int k = 0; k < ngrp; ++k) v += __ldcg(gpart + (long long)k * kBlkPart + q * 256 + t);
     if (r < s && c < s) rd.S[gslot[q] + r * s + c] = v;
   }
   if (t < nd) {
     double v = 0.0;
 #pragma unroll 16
-    for (int b = 0; b < nb; ++b) v += __ldcg(rd.part + (long long)b * kBlkPart + 512 + t);
+    for (int k = 0; k < ngrp; ++k) v += __ldcg(gpart + (long long)k * kBlkPart + 512 + t);
     rd.S[rd.out + t] = v;
   }
   __syncthreads();

@@ -457,15 +457,24 @@ k_zblock(ZBlkH a, Red rd) {
 }
 
 // Deterministic grid reduction of the Gram entries (thread t owns entry t
-// of each Gram) and the Frobenius dots: block-major partials of kZBlkPart
-// doubles per block; the last block writes the sums to the slots and runs
-// the epilogue.
+// of each Gram) and the Frobenius dots, in two levels as blk_finish does
+// (the last block of each group of kRedGroup blocks sums its group in
+// block order, the last group block the group sums in group order):
+// block-major partials of kZBlkPart doubles per block; the last block
+// writes the sums to the slots and runs the epilogue.
 __device__ __forceinline__ void zblk_finish(const double* g, int ng, int s,
                                             const double* dd, int nd,
                                             const short* gslot, const Red& rd) {
   __shared__ double wsum[4][kWarps];
   __shared__ int is_last;
   const int t = threadIdx.x;
+  const int nb = gridDim.x;
+  const int grp = blockIdx.x / kRedGroup;
+  const int b0 = grp * kRedGroup;
+  const int gn = min(kRedGroup, nb - b0);
+  const int ngrp = (nb + kRedGroup - 1) / kRedGroup;
+  double* gpart = rd.part + (long long)kGridCap * kZBlkPart;
+  unsigned* gticket = reinterpret_cast<unsigned*>(rd.part + red2_ticket_offset(kZBlkPart));
   double* mine = rd.part + (long long)blockIdx.x * kZBlkPart;
   for (int q = 0; q < ng; ++q) {
     mine[q * 512 + 2 * t] = g[2 * q];
@@ -483,20 +492,49 @@ __device__ __forceinline__ void zblk_finish(const double* g, int ng, int s,
       mine[1024 + d] = v;
     }
     __threadfence();
-    const unsigned tk = atomicAdd(rd.ticket, 1u);
-    is_last = (tk == gridDim.x - 1);
+    is_last = atomicAdd(gticket + grp, 1u) == (unsigned)gn - 1;
   }
   __syncthreads();
   if (!is_last) return;
   __threadfence();
-  const int nb = gridDim.x;
+  // Level 1: this group's blocks.
+  const double* gp = rd.part + (long long)b0 * kZBlkPart;
+  double* gout = gpart + (long long)grp * kZBlkPart;
+  for (int q = 0; q < ng; ++q) {
+    double re = 0.0, im = 0.0;
+#pragma unroll
+    for (int b = 0; b < kRedGroup; ++b)
+      if (b < gn) {
+        re += __ldcg(gp + (long long)b * kZBlkPart + q * 512 + 2 * t);
+        im += __ldcg(gp + (long long)b * kZBlkPart + q * 512 + 2 * t + 1);
+      }
+    gout[q * 512 + 2 * t] = re;
+    gout[q * 512 + 2 * t + 1] = im;
+  }
+  if (t < 2 * nd) {
+    double v = 0.0;
+#pragma unroll
+    for (int b = 0; b < kRedGroup; ++b)
+      if (b < gn) v += __ldcg(gp + (long long)b * kZBlkPart + 1024 + t);
+    gout[1024 + t] = v;
+  }
+  __syncthreads();
+  if (t == 0) {
+    gticket[grp] = 0u;
+    __threadfence();
+    is_last = atomicAdd(rd.ticket, 1u) == (unsigned)ngrp - 1;
+  }
+  __syncthreads();
+  if (!is_last) return;
+  __threadfence();
+  // Level 2: the groups.
   const int r = t >> 4, c = t & 15;
   for (int q = 0; q < ng; ++q) {
     double re = 0.0, im = 0.0;
 #pragma unroll 8
-    for (int b = 0; b < nb; ++b) {
-      re += __ldcg(rd.part + (long long)b * kZBlkPart + q * 512 + 2 * t);
-      im += __ldcg(rd.part + (long long)b * kZBlkPart + q * 512 + 2 * t + 1);
+    for (int k = 0; k < ngrp; ++k) {
+      re += __ldcg(gpart + (long long)k * kZBlkPart + q * 512 + 2 * t);
+      im += __ldcg(gpart + (long long)k * kZBlkPart + q * 512 + 2 * t + 1);
     }
     if (r < s && c < s) {
       rd.S[gslot[q] + 2 * (r * s + c)] = re;
@@ -506,7 +544,7 @@ __device__ __forceinline__ void zblk_finish(const double* g, int ng, int s,
   if (t < 2 * nd) {
     double v = 0.0;
 #pragma unroll 8
-    for (int b = 0; b < nb; ++b) v += __ldcg(rd.part + (long long)b * kZBlkPart + 1024 + t);
+    for (int k = 0; k < ngrp; ++k) v += __ldcg(gpart + (long long)k * kZBlkPart + 1024 + t);
     rd.S[rd.out + t] = v;
   }
   __syncthreads();

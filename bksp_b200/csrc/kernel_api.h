@@ -16,6 +16,19 @@ constexpr int kLcMaxIn = 24;   // widest linear combination (inputs)
 constexpr int kLcMaxOut = 6;   // widest linear combination (outputs)
 constexpr int kMaxDotsApi = 8;
 constexpr int kPartRows = 64;  // rows of the per-block partials buffer
+// Block-kernel reductions run in two levels: the last block of each group
+// of kRedGroup blocks sums the group's partials, the last group the
+// groups' sums.  Buffer of `per` doubles per block: kGridCap block rows,
+// kRedGroups group rows, then kRedGroups unsigned group tickets (zeroed
+// once; each group's last block resets its ticket).
+constexpr int kRedGroup = 16;
+constexpr int kRedGroups = kGridCap / kRedGroup;
+constexpr long long red2_doubles(int per) {
+  return (long long)per * (kGridCap + kRedGroups) + kRedGroups;
+}
+constexpr long long red2_ticket_offset(int per) {
+  return (long long)per * (kGridCap + kRedGroups);
+}
 constexpr int kTileNnz = 2048;  // SpMV row block: max stored entries
 constexpr int kTileRows = 256;  // SpMV row block: max rows (= threads)
 

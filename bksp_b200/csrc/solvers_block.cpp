@@ -107,7 +107,9 @@ void spmm(const DevCsr& A, const SpmmH& a, const RedH& rd, cudaStream_t st) {
 BlockCtx::BlockCtx(int n_, int s_, SolveState& ss_, cudaStream_t st_)
     : n(n_), s(s_), np(pad64(n_)), ss(ss_), st(st_) {
   if (s < 1 || s > kBlockMaxS) throw CudaError("block width out of range");
-  bpart = dalloc_n<double>((long long)514 * kGridCap, st);
+  bpart = dalloc_n<double>(red2_doubles(514), st);
+  BK_CHECK(cudaMemsetAsync(bpart + red2_ticket_offset(514), 0,
+                           kRedGroups * sizeof(double), st));
 }
 
 BlockCtx::~BlockCtx() { dfree(bpart, st); }

@@ -629,7 +629,9 @@ struct ZBlockCtx {
   ZBlockCtx(int n_, int s_, SolveState& ss_, cudaStream_t st_)
       : n(n_), s(s_), np(pad64(n_)), ss(ss_), st(st_) {
     if (s < 1 || s > 16) throw CudaError("complex block width out of range");
-    bpart = dalloc_n<double>((long long)kZBlkPart * kGridCap, st);
+    bpart = dalloc_n<double>(red2_doubles(kZBlkPart), st);
+    BK_CHECK(cudaMemsetAsync(bpart + red2_ticket_offset(kZBlkPart), 0,
+                             kRedGroups * sizeof(double), st));
   }
   ~ZBlockCtx() {
     for (void* p : owned) dfree(p, st);

@@ -4,6 +4,7 @@ that has the reference sources; the outputs are committed).
     make -C oracle && OPENBLAS_NUM_THREADS=1 python tests/golden/make_golden.py
     OPENBLAS_NUM_THREADS=8 OMP_NUM_THREADS=8 python tests/golden/make_golden.py --full
     OPENBLAS_NUM_THREADS=1 python tests/golden/make_golden.py --complex
+    python tests/golden/make_golden.py --thread-spread
 
 * ``testmats.npz`` -- the reference's two test matrices (testmat/bfwb398.mtx,
   symmetric, one triangle; testmat/pde2961.mtx, general) as read by the
@@ -18,6 +19,11 @@ that has the reference sources; the outputs are committed).
 * ``reference_full.json`` (``--full``) -- the same records at the full sizes
   of the block and shifted benchmark configurations (3D Poisson 64^3 with 16
   right-hand sides; 2D convection-diffusion 1024^2 with 32 shifts).
+* ``--thread-spread`` adds to ``reference_full.json`` the return value of
+  the block configurations' reference solves under OpenBLAS at 1, 2, 3, 4,
+  6 and 8 threads (each in a child process): the reference's own spread of
+  iteration counts, which comes from the order its threaded dgemm sums the
+  Gram products in.
 * ``reference_z.json`` (``--complex``) -- the complex solvers zbicg,
   zshbicgstabl and zblbicgstabl on seeded complex problems
   (bksp_b200.problems.complex_*).  zbicgstabl is not recorded: its unit
@@ -247,8 +253,48 @@ def main_complex():
         json.dump(out, f, indent=1)
 
 
+SPREAD_THREADS = (1, 2, 3, 4, 6, 8)
+
+
+def spread_child(which):
+    """One block solve at 64^3 in this process; prints its return value."""
+    rp, c, v, n = P.poisson3d(64)
+    Bm = np.random.default_rng(2).standard_normal((n, 16))
+    if which == "blcg":
+        lrp, lc, lv, _ = P.lower_triangle(rp, c, v, n)
+        ret = R.call("dblcg", R.Matrix(lrp, lc, lv, n, symmetric=True),
+                     Bm, 1e-8, 5000, np.zeros((n, 16)))[0]
+    else:
+        ret = R.call("dblbicgstabl", R.Matrix(rp, c, v, n),
+                     Bm, 2, 1e-8, 5000, np.zeros((n, 16)))[0]
+    print(json.dumps({"ret": int(ret)}))
+
+
+def main_spread():
+    import subprocess
+    path = os.path.join(HERE, "reference_full.json")
+    with open(path) as f:
+        out = json.load(f)
+    for key, which in (("cfg3/blcg_p64", "blcg"), ("cfg3/blbicgstabl2_p64", "blbicgstabl2")):
+        spread = {}
+        for th in SPREAD_THREADS:
+            env = dict(os.environ, OPENBLAS_NUM_THREADS=str(th), OMP_NUM_THREADS=str(th))
+            r = subprocess.run([sys.executable, os.path.abspath(__file__),
+                                "--spread-child", which], env=env,
+                               capture_output=True, text=True, check=True)
+            spread[str(th)] = json.loads(r.stdout.strip().splitlines()[-1])["ret"]
+            print(key, th, spread[str(th)], flush=True)
+        out[key]["ret_by_threads"] = spread
+    with open(path, "w") as f:
+        json.dump(out, f, indent=1)
+
+
 if __name__ == "__main__":
-    if "--full" in sys.argv[1:]:
+    if "--spread-child" in sys.argv[1:]:
+        spread_child(sys.argv[sys.argv.index("--spread-child") + 1])
+    elif "--thread-spread" in sys.argv[1:]:
+        main_spread()
+    elif "--full" in sys.argv[1:]:
         main_full()
     elif "--complex" in sys.argv[1:]:
         main_complex()

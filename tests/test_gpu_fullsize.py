@@ -7,9 +7,12 @@ configurations, against the compiled reference's outputs at those sizes
 * shifted BiCGSTAB(4), 2D convection-diffusion 1024^2 (n = 1,048,576), 32
   log-spaced shifts 1e-3..1, b ~ U[-1,1] (seed 3), tol 1e-8.
 
-Criteria: return index within max(2, 5 %) (Block BiCGSTAB(l): 10 %, its QR
-is a Cholesky QR with a non-negative R diagonal where the reference calls
-LAPACK's Householder QR, which changes the rounding of every block step);
+Criteria: return index within max(2, 5 %) of the 8-thread reference, or,
+for the block methods, within the range of return indices the reference
+itself gives under OpenBLAS at 1 to 8 threads (``ret_by_threads``; at 64^3
+Block BiCGSTAB(2) ends anywhere in 56..70 depending on how the threaded
+dgemm orders the Gram sums, and every change of summation order moves the
+GPU's index the same way);
 convergence-test history within 1e-6 relative over the first 20 tests while
 the reference value is above 1e-8 (block: 1e-5); the worst column's / the
 worst shift's FP64 true residual within 10x the reference's."""
@@ -46,6 +49,16 @@ def poisson64():
     return rp, c, v, lrp, lc, lv, n, A, Bm
 
 
+def _ret_ok(ret, g, rel=0.05):
+    """Within max(2, rel) of the 8-thread reference, or inside the
+    reference's own spread over OpenBLAS thread counts (2 iterations of
+    slack at either end)."""
+    if iters_close(ret, g["ret"], rel=rel):
+        return True
+    spread = list(g.get("ret_by_threads", {}).values())
+    return bool(spread) and min(spread) - 2 <= ret <= max(spread) + 2
+
+
 def test_block_cg_poisson64(gpu, full, poisson64):
     B = gpu
     rp, c, v, lrp, lc, lv, n, A, Bm = poisson64
@@ -53,7 +66,7 @@ def test_block_cg_poisson64(gpu, full, poisson64):
     with B.record(hist_cap=6000) as st:
         ret = B.dblcg(B.CsrMatrix(lrp, lc, lv, symmetric=True), Bm, 1e-8, 5000, X)
     g = full["cfg3/blcg_p64"]
-    assert iters_close(ret, g["ret"]), (ret, g["ret"])
+    assert _ret_ok(ret, g), (ret, g["ret"], g.get("ret_by_threads"))
     hist_close(st["hist"], g["hist"], k=20, rtol=1e-5, floor=1e-8)
     assert max(_col_res(A, Bm, X)) <= 10 * max(g["true_res_cols"])
 
@@ -65,7 +78,7 @@ def test_block_bicgstabl2_poisson64(gpu, full, poisson64):
     with B.record(hist_cap=6000) as st:
         ret = B.dblbicgstabl(B.CsrMatrix(rp, c, v), Bm, 2, 1e-8, 5000, X)
     g = full["cfg3/blbicgstabl2_p64"]
-    assert iters_close(ret, g["ret"], rel=0.1), (ret, g["ret"])
+    assert _ret_ok(ret, g), (ret, g["ret"], g.get("ret_by_threads"))
     hist_close(st["hist"], g["hist"], k=20, rtol=1e-5, floor=1e-8)
     assert max(_col_res(A, Bm, X)) <= 10 * max(g["true_res_cols"])
 
