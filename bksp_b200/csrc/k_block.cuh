@@ -200,10 +200,11 @@ constexpr size_t blk_smem_bytes() {
 }
 
 // Terms are formed in T (the block's element type); Gram products and dots
-// accumulate in FP64 either way.  Three CTAs per SM (80 registers): at four
-// (64 registers) the tile loop spilled and ran ~10 % slower.
+// accumulate in FP64 either way.  Two CTAs per SM (128 registers, no
+// spills): measured ~10 % faster than three (80 registers) and ~20 % faster
+// than four (64 registers, the tile loop spilling).
 template <typename T>
-__global__ void __launch_bounds__(kThreads, 3)
+__global__ void __launch_bounds__(kThreads, 2)
 k_block(BlkArgs<T> a, Red rd) {
   if (skip(rd)) return;
   // The tiles and matrices share their storage with the epilogue's staged
