@@ -817,6 +817,8 @@ def run_configs(a):
     * cfg 3: Block CG and Block BiCGSTAB(2), 16 Gaussian right-hand sides
       (seed 2), 3D Poisson 64^3 and 128^3, through dblcg / dblbicgstabl and
       their mixed counterparts (FP64 refinement around FP32 inner solves);
+      the second of two calls is timed (the first includes the one-time
+      block-product autotuning and the loop's graph capture);
     * cfg 4: shifted BiCGSTAB(4), 32 shifts 1e-3..1, 2D convection-diffusion
       1024^2, dshbicgstabl against bksp_dshbicgstabl_mixed (FP32 shift
       vectors, per-shift FP64 polishing).
@@ -931,7 +933,7 @@ def run_configs(a):
             res[name] = {}
             for mode, fn in (("plain_fp64", plain), ("mixed", mixed)):
                 X = np.zeros((n, 16))
-                r, dt, st = host_run(lambda: (X.fill(0.0), fn(X))[1], reps=1)
+                r, dt, st = host_run(lambda: (X.fill(0.0), fn(X))[1], reps=2)
                 res[name][mode] = {"ret": r, "solve_s": st["solve_ms"] / 1e3, "e2e_s": dt,
                                    "worst_true_residual": worst(X)}
             pair(name, None, None)
