@@ -186,7 +186,9 @@ def workload_config(nx, n, nnz):
     return {"workload": f"bicgstabl{L_DEG}_convdiff3d_{nx}^3",
             "n": n, "nnz": nnz, "l": L_DEG, "tol_true_residual": TOL_TRUE,
             "rhs": "b = A x_true, x_true ~ U[-1,1] seed 1",
-            "l2": "inputs larger than L2 (FP64 CSR %.0f MB)" % ((nnz * 12 + 4 * n) / 1e6),
+            "l2": ("solve inputs larger than L2 (FP64 CSR %.0f MB); kernel timings "
+                   "after a 384 MB write + read of a flush buffer before each launch")
+                  % ((nnz * 12 + 4 * n) / 1e6),
             "parallelism": "replicas"}
 
 
@@ -428,20 +430,30 @@ def run_ours(a):
     ys64 = torch.empty(n, dtype=torch.float64, device=dev)
     xs32 = xs64.float()
     ys32 = torch.empty(n, dtype=torch.float32, device=dev)
-    reps = 50
+    reps = 30
     tuned = G.variant()
+    # The FP32 diagonal form with its vectors (78 MB) fits in L2: every
+    # timed launch follows a 384 MB write and a read of the same buffer
+    # (the read leaves L2 holding clean lines of that buffer, so the timed
+    # launch neither hits its own data nor pays for writing back the
+    # flush's dirty lines), and only the launch is inside the events.
+    l2_flush = torch.empty(384 << 20, dtype=torch.uint8, device=dev)
 
     def time_spmv(xx, yy, f32):
         for _ in range(5):
             G.spmv(xx.data_ptr(), yy.data_ptr(), f32, sp)
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(reps):
+        tot = 0.0
+        for k in range(reps):
+            l2_flush.fill_(k & 255)
+            l2_flush.max()
+            e0.record(stream)
             G.spmv(xx.data_ptr(), yy.data_ptr(), f32, sp)
-        e1.record(stream)
-        e1.synchronize()
-        return e0.elapsed_time(e1) / reps
+            e1.record(stream)
+            e1.synchronize()
+            tot += e0.elapsed_time(e1)
+        return tot / reps
 
     variants = {}
     for var_id, vname in G.SPMV_VARIANTS.items():
