@@ -221,13 +221,17 @@ k_block(BlkArgs<T> a, Red rd) {
     const int o = q / 4, i = q % 4;
     cs[o][i] = (o < a.nout && i < a.nin) ? (T)eval_cf(a.c[o][i], rd.S) : T(0);
   }
+  // s-by-s matrices zero-padded to kBlkS x kBlkS (row stride kBlkS): with
+  // the tile's columns >= s zero as well, the products below run over all
+  // kBlkS terms without a per-term predicate (the padded terms add
+  // fma(0, 0, z) = z).
   for (int o = 0; o < a.nout; ++o)
     for (int i = 0; i < a.nin; ++i)
       if (a.mslot[o][i] >= 0)
-        for (int q = t; q < s * s; q += kThreads) {
-          const int b = q / s, cc = q % s;
+        for (int q = t; q < kBlkS * kBlkS; q += kThreads) {
+          const int b = q / kBlkS, cc = q % kBlkS;
           const int src = a.trans[o][i] ? cc * s + b : b * s + cc;
-          mat[o][i][q] = (T)rd.S[a.mslot[o][i] + src];
+          mat[o][i][q] = (b < s && cc < s) ? (T)rd.S[a.mslot[o][i] + src] : T(0);
         }
   __syncthreads();
   double gacc[2] = {0.0, 0.0};
@@ -282,7 +286,7 @@ k_block(BlkArgs<T> a, Red rd) {
         if (a.mslot[o][i] >= 0) {
           T mc[kBlkS];
 #pragma unroll
-          for (int b = 0; b < kBlkS; ++b) mc[b] = b < s ? mat[o][i][b * s + c] : T(0);
+          for (int b = 0; b < kBlkS; ++b) mc[b] = mat[o][i][b * kBlkS + c];
 #pragma unroll
           for (int k = 0; k < kBlkSub; ++k) {
             const int rr = r + (kThreads / kBlkS) * k;
@@ -291,8 +295,8 @@ k_block(BlkArgs<T> a, Red rd) {
             for (int b = 0; b < kBlkS; b += 2) {
               const typename Pair<T>::V x2 =
                   *reinterpret_cast<const typename Pair<T>::V*>(&tile[i][rr][b]);
-              if (b < s) z = fma_rn(x2.x, mc[b], z);
-              if (b + 1 < s) z = fma_rn(x2.y, mc[b + 1], z);
+              z = fma_rn(x2.x, mc[b], z);
+              z = fma_rn(x2.y, mc[b + 1], z);
             }
             const T term = cs[o][i] * z;
             y[k] = first ? term : add_rn(y[k], term);
