@@ -363,8 +363,8 @@ k_block(BlkArgs<T> a, Red rd) {
 // last block of each group of kRedGroup blocks sums its group's partials
 // in block order, the last such group block sums the group sums in group
 // order, writes them to the scalar slots and runs the epilogue.  (One
-// level over all ~600 blocks' partials was a chain of dependent batches
-// of L2 loads on one SM; two levels need a handful.)  Partials: block b's
+// level over all the grid's partials was a long chain of dependent
+// batches of L2 loads on one SM; two levels need a handful.)  Partials: block b's
 // kBlkPart values contiguous (Grams at q * 256, dots at 512), so writes
 // and reads are coalesced.
 __device__ __forceinline__ void blk_finish(const double* g, int ng, int s,
