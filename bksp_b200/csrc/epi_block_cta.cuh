@@ -58,9 +58,11 @@ __device__ __forceinline__ void cm_mul(const double* A, const double* B,
 
 // dm_lu by the block.  At step k every thread finds the pivot itself (the
 // same scan, so the same row), then row k and the pivot row are swapped,
-// the trailing entries updated (thread (i, j) with i, j > k) and last the
-// multipliers stored in column k.
+// the multipliers f_i = a_ik / a_kk formed once (thread i, into shared
+// memory) and the trailing entries updated (thread (i, j), i > k, j >= k;
+// j = k stores f_i).
 __device__ __forceinline__ bool cm_lu(double* A, double* piv, int s, int t) {
+  __shared__ double fcol[16];
   bool ok = true;
   for (int k = 0; k < s; ++k) {
     int p = k;
@@ -77,15 +79,13 @@ __device__ __forceinline__ bool cm_lu(double* A, double* piv, int s, int t) {
     __syncthreads();
     const double d = A[k * s + k];
     if (d == 0.0) { ok = false; continue; }
+    if (t > k && t < s) fcol[t] = A[t * s + k] / d;
+    __syncthreads();
     if (t < s * s) {
       const int i = t / s, j = t % s;
-      if (i > k && j > k) {
-        const double f = A[i * s + k] / d;
-        A[i * s + j] = fma(-f, A[k * s + j], A[i * s + j]);
-      }
+      if (i > k && j > k) A[i * s + j] = fma(-fcol[i], A[k * s + j], A[i * s + j]);
+      else if (i > k && j == k) A[i * s + k] = fcol[i];
     }
-    __syncthreads();
-    if (t > k && t < s) A[t * s + k] = A[t * s + k] / d;
     __syncthreads();
   }
   __syncthreads();
